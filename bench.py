@@ -1,0 +1,281 @@
+"""Benchmark: FP64 upwind DG advection operator apply (GenDiL's matrix-free path) on B200.
+
+Workload (one "step" = one operator apply over the whole mesh): 3D upwind DG advection, cell
+term + interior faces + boundary faces with inflow value 0, 64^3 Cartesian hexahedra on the unit
+cube, order p = 3 GLL basis (16,777,216 DoFs), 4-point Gauss-Legendre quadrature, velocity
+beta(x) = (1 + 0.5 sin 2 pi y, 0.5 + 0.25 cos 2 pi z, 0.25); input u ~ U[-1,1] from
+FillRandom(seed 1).  x and y are 134 MB each (> 126 MB L2), so no L2 flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  ``value`` = GDoF/s of the device-resident apply (all ranks);
+``e2e`` = the same apply through the C ABI with the input copied from pinned host memory and
+the result copied back inside the timed region; ``roofline`` = algorithmic bytes (read x +
+write y, 16 B/DoF) per launch over the measured launch time, against the measured HBM copy
+bandwidth; ``cpu_baseline`` = the GenDiL reference operator (compiled from its own headers,
+OpenMP) timed on this host.  ``--impl reference`` times that reference alone.
+For N > 1 each rank runs an independent replica (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_AXIS, ORDER, NQ = 64, 3, 4
+METRIC = "GDoF/s per operator apply vs HBM roofline; mixed vs FP64 solve time @1e-10"
+WORKLOAD = "fp64 upwind DG advection apply, 3D 64^3 hex, p=3 GLL, q=4 GL, sin/cos velocity, inflow 0"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def case_dict(n=N_AXIS):
+    return {"D": 3, "P": ORDER, "Q": NQ, "basis": 0, "sizes": [n] * 3, "h": [1.0 / n] * 3, "origin": [0.0] * 3,
+            "periodic": [0] * 3, "beta_kind": 2, "g": 0.0}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [v.strip() for v in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(x_np, seconds_target=12.0):
+    """The GenDiL reference operator (oracle/_ref, OpenMP) on this host's cores."""
+    from oracle.bindings import Reference, have_reference
+    if not have_reference():
+        return None
+    ref = Reference()
+    case = case_dict()
+    t1 = ref.time_advection(case, x_np, 1)
+    pairs = max(1, min(20, int(seconds_target / max(2 * t1, 1e-3))))
+    t = ref.time_advection(case, x_np, pairs)
+    ndofs = len(x_np)
+    return {"value": ndofs / t / 1e9, "unit": "GDoF/s", "cores": ref.num_threads(), "kind": "reference",
+            "sample": f"full 64^3 p=3 mesh, {2 * pairs} applies (op(x,y); op(y,x) pairs) after 2 warm-up applies, "
+                      f"GenDiL AdvectionOperator WithBC, SerialKernelConfiguration + OpenMP, mean {t * 1e3:.1f} ms/apply"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+    from oracle.bindings import have_reference
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgendil_ref.so was not built"}))
+        return 0
+    import gendil_b200 as g
+    x = g.fill_random((N_AXIS ** 3) * (ORDER + 1) ** 3, 1)
+    from oracle.bindings import Reference
+    ref = Reference()
+    case = case_dict()
+    ref.time_advection(case, x, max(1, args.warmup // 2))
+    t = ref.time_advection(case, x, max(1, args.steps // 2))
+    v = len(x) / t / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "GDoF/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "dofs": len(x), "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": ref.num_threads(), "kind": "reference",
+                             "sample": f"full 64^3 mesh, {2 * max(1, args.steps // 2)} applies, OpenMP"},
+            "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import gendil_b200 as g
+    from gendil_b200 import coefficients as C
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    space = g.Space(3, [N_AXIS] * 3, order=ORDER)
+    op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
+    nd = space.num_dofs
+    x_np = g.fill_random(nd, 1)
+    x = torch.from_numpy(x_np).to(dev)
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        op(x, y)
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            op(x, y)
+        stop.record(stream)
+        barrier()
+    ms = start.elapsed_time(stop)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * nd * args.steps / (ms * 1e-3) / 1e9
+
+    # end to end through the C ABI: pinned host input -> device -> apply -> host result
+    xh = torch.from_numpy(x_np).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    for _ in range(2):
+        x.copy_(xh, non_blocking=True)
+        op(x, y)
+        yh.copy_(y, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(3, min(args.steps, 20))
+    e0.record(stream)
+    for _ in range(e_steps):
+        x.copy_(xh, non_blocking=True)
+        op(x, y)
+        yh.copy_(y, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    ems = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ems], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e_value = world * nd * e_steps / (ems * 1e-3) / 1e9
+
+    hbm, peak_kind = peaks()
+    alg_bytes = 16.0 * nd
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("advection_fp64_64cubed_p3")
+        except (OSError, ValueError):
+            traffic = None
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)",
+                "config": {"workload": WORKLOAD, "dofs": nd, "elements": space.num_elements,
+                           "parallelism": f"replicas{world}" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (x, y 134 MB each)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_launch": alg_bytes},
+                "e2e": {"value": e2e_value, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * nd,
+                        "d2h_bytes_per_step": 8 * nd, "steps": e_steps},
+                "gpu_launches": args.steps,
+                "clocks": clocks.summary()}
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(x_np)
+            except Exception as exc:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"unavailable": str(exc)}
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

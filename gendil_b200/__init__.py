@@ -1,0 +1,283 @@
+"""gendil_b200 -- B200-native matrix-free DG mass / upwind-advection operators.
+
+Python host binding over the C ABI of ``libdgop.so`` (``include/dgop.h``).  Device memory and
+streams come from PyTorch; every operator apply runs the library's own sm_100a kernels.  There
+is no CPU fallback: importing this package on a machine without the built library raises.
+
+The objects mirror GenDiL's operator API for this path:
+
+* :class:`Space`  -- ``CartesianMesh<D>`` + ``MakeLobattoFiniteElement`` / ``MakeLegendreFiniteElement``
+  + ``MakeFiniteElementSpace`` (Meshes/MeshDataStructures/CartesianMesh/cartesianndmesh.hpp:44,
+  FiniteElementMethod/finiteelement.hpp:103,109, finiteelementspace.hpp:84);
+* :class:`MassOperator`, :class:`AdvectionOperator`, :class:`MassAdvectionOperator`,
+  :class:`SystemOperator` -- ``MakeMassFiniteElementOperator`` (massoperator.hpp:270),
+  ``MakeAdvectionOperator`` (advectionoperator.hpp:1416,1481), ``MassAdvectionOperator``
+  (massadvectionoperator.hpp:329); calling ``op(x, y)`` overwrites ``y`` like the reference's
+  ``operator()(const Vector&, Vector&)``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .coefficients import Coefficient, as_coefficient
+
+__all__ = ["Space", "MassOperator", "AdvectionOperator", "MassAdvectionOperator", "SystemOperator",
+           "Coefficient", "DGOPError", "lib", "GLL", "GL", "BC_NONE", "BC_INFLOW"]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libdgop.so")
+
+GLL, GL = 0, 1
+BC_NONE, BC_INFLOW = 0, 1
+MAX_TERMS, MAX_DIM = 4, 6
+
+
+class DGOPError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dgop error {code}: {msg}")
+        self.code = code
+
+
+class _Coef(ctypes.Structure):
+    _fields_ = [("constant", ctypes.c_double), ("nterms", ctypes.c_int),
+                ("tables", (ctypes.c_void_p * MAX_DIM) * MAX_TERMS), ("element_factor", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded ``libdgop.so`` (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m gendil_b200.build` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i64, d, i = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int
+        L.dgop_last_error.restype = ctypes.c_char_p
+        L.dgop_version.restype = ctypes.c_char_p
+        L.dgop_space_create.argtypes = [i, vp, vp, vp, vp, i, i, ctypes.POINTER(vp)]
+        L.dgop_space_destroy.argtypes = [vp]
+        L.dgop_space_num_dofs.argtypes = [vp]
+        L.dgop_space_num_dofs.restype = i64
+        L.dgop_space_num_elements.argtypes = [vp]
+        L.dgop_space_num_elements.restype = i64
+        L.dgop_space_coordinates.argtypes = [vp, i, i, vp]
+        L.dgop_mass_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
+        L.dgop_advection_create.argtypes = [vp, i, vp, i, d, ctypes.POINTER(vp)]
+        L.dgop_mass_advection_create.argtypes = [vp, i, vp, vp, ctypes.POINTER(vp)]
+        L.dgop_system_create.argtypes = [vp, i, vp, vp, i, d, ctypes.POINTER(vp)]
+        L.dgop_operator_destroy.argtypes = [vp]
+        L.dgop_apply.argtypes = [vp, vp, vp, vp]
+        L.dgop_apply_ex.argtypes = [vp, d, vp, d, vp, vp]
+        L.dgop_apply_transpose.argtypes = [vp, vp, vp, vp]
+        L.dgop_apply_f32.argtypes = [vp, vp, vp, vp]
+        L.dgop_fill_random.argtypes = [vp, i64, ctypes.c_uint, d, d]
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise DGOPError(rc, lib().dgop_last_error().decode())
+    return rc
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        try:
+            import torch
+            return torch.cuda.current_stream().cuda_stream
+        except Exception:  # pragma: no cover - torch always present in this package's use
+            return 0
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class Space:
+    """A DG L2 space on a Cartesian hypercube mesh of dimension 1..6, order 0..7."""
+
+    def __init__(self, dim, n_elem, h=None, origin=None, periodic=None, order=1, basis=GLL):
+        n_elem = [int(v) for v in (n_elem if np.ndim(n_elem) else [n_elem] * dim)]
+        if h is None:
+            h = [1.0 / v for v in n_elem]
+        h = [float(v) for v in (h if np.ndim(h) else [h] * dim)]
+        origin = [0.0] * dim if origin is None else [float(v) for v in origin]
+        periodic = [0] * dim if periodic is None else [int(bool(v)) for v in periodic]
+        self.dim, self.order, self.basis = dim, order, basis
+        self.n_elem, self.h, self.origin, self.periodic = n_elem, h, origin, periodic
+        self._a = [np.ascontiguousarray(n_elem + [1] * (MAX_DIM - dim), dtype=np.int64),
+                   np.ascontiguousarray(h + [1.0] * (MAX_DIM - dim), dtype=np.float64),
+                   np.ascontiguousarray(origin + [0.0] * (MAX_DIM - dim), dtype=np.float64),
+                   np.ascontiguousarray(periodic + [0] * (MAX_DIM - dim), dtype=np.int32)]
+        handle = ctypes.c_void_p()
+        check(lib().dgop_space_create(dim, *(a.ctypes.data for a in self._a), order, basis, ctypes.byref(handle)))
+        self.handle = handle
+
+    @property
+    def num_dofs(self):
+        return int(lib().dgop_space_num_dofs(self.handle))
+
+    @property
+    def num_elements(self):
+        return int(lib().dgop_space_num_elements(self.handle))
+
+    @property
+    def dofs_per_element(self):
+        return (self.order + 1) ** self.dim
+
+    def coordinates(self, q, axis):
+        """Coordinates at which coefficient tables are sampled along ``axis`` (n_elem x (q+2))."""
+        out = np.empty(self.n_elem[axis] * (q + 2), dtype=np.float64)
+        check(lib().dgop_space_coordinates(self.handle, q, axis, out.ctypes.data))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().dgop_space_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Operator:
+    def __init__(self, space, q):
+        self.space, self.q = space, q
+        self.handle = None
+        self._keep = []
+
+    def _coef(self, c):
+        """Tabulate a coefficient into the ctypes struct (tables kept alive on self)."""
+        if c is None:
+            return None
+        c = as_coefficient(c, self.space.dim)
+        st = _Coef()
+        st.constant = float(c.constant)
+        st.nterms = len(c.terms)
+        for t, term in enumerate(c.terms):
+            for axis, fn in term.items():
+                tab = np.ascontiguousarray(c.tabulate(fn, self.space.coordinates(self.q, axis)), dtype=np.float64)
+                self._keep.append(tab)
+                st.tables[t][axis] = tab.ctypes.data
+        if c.element_factor is not None:
+            self._keep.append(c.element_factor)
+            st.element_factor = _ptr(c.element_factor)
+        self._keep.append(st)
+        return st
+
+    def _vec(self, coefs):
+        arr = (_Coef * self.space.dim)(*coefs)
+        self._keep.append(arr)
+        return arr
+
+    def __call__(self, x, y, stream=None):
+        """y = A x (overwrites y), FP64 device tensors."""
+        check(lib().dgop_apply(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        return y
+
+    def apply(self, x, y, alpha=1.0, beta=0.0, stream=None):
+        """y = alpha A x + beta y."""
+        check(lib().dgop_apply_ex(self.handle, float(alpha), _ptr(x), float(beta), _ptr(y), _stream(stream)))
+        return y
+
+    def apply_transpose(self, x, y, stream=None):
+        check(lib().dgop_apply_transpose(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        return y
+
+    def apply_f32(self, x, y, stream=None):
+        check(lib().dgop_apply_f32(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        return y
+
+    @property
+    def num_dofs(self):
+        return self.space.num_dofs
+
+    def close(self):
+        if self.handle:
+            lib().dgop_operator_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MassOperator(_Operator):
+    """y = M_sigma x (MassFiniteElementOperator, massoperator.hpp:169)."""
+
+    def __init__(self, space, q, sigma=1.0):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        check(lib().dgop_mass_create(space.handle, q, ctypes.byref(self._coef(sigma)), ctypes.byref(h)))
+        self.handle = h
+
+
+class AdvectionOperator(_Operator):
+    """y = A x, upwind DG advection (AdvectionOperator, advectionoperator.hpp:1005).
+
+    ``bc=BC_NONE`` skips boundary faces (WithoutBC, :106); ``BC_INFLOW`` uses the constant inflow
+    value ``g`` (WithBC, :269)."""
+
+    def __init__(self, space, q, beta, bc=BC_INFLOW, g=0.0):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        coefs = [self._coef(c) for c in _components(beta, space.dim)]
+        check(lib().dgop_advection_create(space.handle, q, self._vec(coefs), bc, float(g), ctypes.byref(h)))
+        self.handle = h
+
+
+class MassAdvectionOperator(_Operator):
+    """y = (M_sigma + A_interior) x (MassAdvectionOperator, massadvectionoperator.hpp:329)."""
+
+    def __init__(self, space, q, beta, sigma=1.0):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        coefs = [self._coef(c) for c in _components(beta, space.dim)]
+        check(lib().dgop_mass_advection_create(space.handle, q, ctypes.byref(self._coef(sigma)), self._vec(coefs),
+                                               ctypes.byref(h)))
+        self.handle = h
+
+
+class SystemOperator(_Operator):
+    """y = (M_sigma + A) x in one launch: the implicit-Euler operator M/dt + A."""
+
+    def __init__(self, space, q, beta, sigma=1.0, bc=BC_INFLOW, g=0.0):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        coefs = [self._coef(c) for c in _components(beta, space.dim)]
+        check(lib().dgop_system_create(space.handle, q, ctypes.byref(self._coef(sigma)), self._vec(coefs), bc,
+                                       float(g), ctypes.byref(h)))
+        self.handle = h
+
+
+def fill_random(n, seed=12345, lo=-1.0, hi=1.0):
+    """FillRandom (Algebra/vector.hpp:632) into a new float64 numpy array."""
+    out = np.empty(int(n), dtype=np.float64)
+    check(lib().dgop_fill_random(out.ctypes.data, int(n), int(seed), float(lo), float(hi)))
+    return out
+
+
+def _components(beta, dim):
+    if isinstance(beta, (list, tuple)) and len(beta) == dim:
+        return list(beta)
+    if np.ndim(beta) == 1 and len(beta) == dim:
+        return [float(b) for b in beta]
+    raise ValueError(f"velocity must have {dim} components")

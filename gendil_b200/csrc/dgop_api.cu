@@ -1,0 +1,499 @@
+// C-ABI implementation: spaces, operators, coefficient tables, launch configuration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "basis.h"
+#include "dgop_internal.h"
+
+namespace dgop {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return DGOP_ERR_CUDA;
+}
+
+#define DGOP_CUDA(call)                               \
+  do {                                                \
+    cudaError_t _e = (call);                          \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+namespace {
+
+// Per-space 1D tables for quadrature size q.
+struct Tables1D {
+  double xq[kMaxQ], wq[kMaxQ], xn[kMaxN], wn[kMaxN];
+  double B[kMaxQ * kMaxN], Dq[kMaxQ * kMaxQ], Bf[2][kMaxN];
+};
+
+bool make_tables(const dgop_space& s, int q, Tables1D& t) {
+  if (!gauss_points(1, q, t.xq, t.wq)) return false;
+  if (!gauss_points(s.basis == DGOP_BASIS_GLL ? 0 : 1, s.n, t.xn, t.wn)) return false;
+  for (int i = 0; i < q; ++i)
+    for (int j = 0; j < s.n; ++j) t.B[i * s.n + j] = lagrange_value(t.xn, s.n, j, t.xq[i]);
+  // collocated derivative on the Gauss points (doftoquad.hpp:142-150): Dq[i][j] = l_j'(x_i)
+  for (int i = 0; i < q; ++i)
+    for (int j = 0; j < q; ++j) t.Dq[i * q + j] = lagrange_grad(t.xq, q, j, t.xq[i]);
+  for (int j = 0; j < s.n; ++j) {
+    t.Bf[0][j] = lagrange_value(t.xn, s.n, j, 0.0);
+    t.Bf[1][j] = lagrange_value(t.xn, s.n, j, 1.0);
+  }
+  return true;
+}
+
+struct PackedCoef {
+  double constant = 0.0;
+  int nterms = 0;
+  int64_t off[kMaxTerms][kMaxDim];
+  const double* elem = nullptr;
+};
+
+// Appends the host tables of `c` to `pack` and records their offsets.
+int pack_coef(const dgop_space& s, int q, const dgop_coef* c, std::vector<double>& pack, PackedCoef& out) {
+  for (auto& row : out.off)
+    for (auto& v : row) v = -1;
+  if (!c) {
+    out.constant = 0.0;
+    out.nterms = 0;
+    return DGOP_OK;
+  }
+  if (c->nterms < 0 || c->nterms > DGOP_MAX_TERMS) {
+    set_error("coefficient: nterms must be in [0, 4]");
+    return DGOP_ERR_ARG;
+  }
+  out.constant = c->constant;
+  out.nterms = c->nterms;
+  out.elem = c->element_factor;
+  for (int t = 0; t < c->nterms; ++t) {
+    for (int k = 0; k < s.D; ++k) {
+      const double* tab = c->tables[t][k];
+      if (!tab) continue;
+      const int64_t len = s.sizes[k] * (q + 2);
+      out.off[t][k] = (int64_t)pack.size();
+      pack.insert(pack.end(), tab, tab + len);
+    }
+  }
+  return DGOP_OK;
+}
+
+int device_sm_count(int dev) {
+  static int cache[64] = {};
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cache[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cache[dev] = v;
+  }
+  return cache[dev];
+}
+
+template <typename Real>
+__global__ void convert_kernel(const double* in, Real* out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (Real)in[i];
+}
+
+template <typename Real>
+int setup_launch(dgop_operator* op, LaunchCfg<Real>& L, const Tables1D& t, const std::vector<double>& pack,
+                 const PackedCoef& sig, const PackedCoef* beta) {
+  const dgop_space& s = op->sp;
+  const int D = s.D, N = s.n, Q = op->q;
+  const GenericEntry<Real>* e = nullptr;
+  if constexpr (sizeof(Real) == 8) e = find_generic_f64(D, N, Q);
+  else e = find_generic_f32(D, N, Q);
+  if (!e || !e->launch) {
+    set_error("no kernel compiled for dim=" + std::to_string(D) + " order=" + std::to_string(N - 1) +
+              " q=" + std::to_string(Q) + (sizeof(Real) == 8 ? " (fp64)" : " (fp32)"));
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  L.entry = e;
+  OpParams<Real>& p = L.params;
+  std::memset(&p, 0, sizeof(p));
+  p.nelem = s.nelem;
+  int64_t stride = 1;
+  double detJ = 1.0;
+  for (int k = 0; k < D; ++k) {
+    p.sizes[k] = s.sizes[k];
+    p.estride[k] = stride;
+    stride *= s.sizes[k];
+    p.periodic[k] = s.periodic[k];
+    p.invh[k] = (Real)(1.0 / s.h[k]);
+    detJ *= s.h[k];
+  }
+  p.detJ = (Real)detJ;
+  for (int i = 0; i < Q * N; ++i) p.B[i] = (Real)t.B[i];
+  for (int i = 0; i < Q * Q; ++i) p.Dq[i] = (Real)t.Dq[i];
+  for (int j = 0; j < N; ++j) {
+    p.Bf[0][j] = (Real)t.Bf[0][j];
+    p.Bf[1][j] = (Real)t.Bf[1][j];
+  }
+  for (int i = 0; i < Q; ++i) p.wq[i] = (Real)t.wq[i];
+  p.tab_ld = Q + 2;
+  p.gll = s.basis == DGOP_BASIS_GLL ? 1 : 0;
+  p.g = (Real)op->g;
+  p.flags = op->flags;
+  // tables
+  if (!pack.empty()) {
+    std::vector<Real> packed(pack.begin(), pack.end());
+    DGOP_CUDA(cudaMalloc(&L.d_tab, sizeof(Real) * packed.size()));
+    DGOP_CUDA(cudaMemcpy(L.d_tab, packed.data(), sizeof(Real) * packed.size(), cudaMemcpyHostToDevice));
+  }
+  p.tab = L.d_tab;
+  auto fill = [&](CoefDev<Real>& d, const PackedCoef& c, int slot) -> int {
+    d.constant = (Real)c.constant;
+    d.nterms = c.nterms;
+    std::memcpy(d.off, c.off, sizeof(d.off));
+    d.elem = nullptr;
+    if (c.elem) {
+      if constexpr (sizeof(Real) == 8) {
+        d.elem = reinterpret_cast<const Real*>(c.elem);
+      } else {
+        DGOP_CUDA(cudaMalloc(&L.d_elem[slot], sizeof(Real) * s.nelem));
+        convert_kernel<Real><<<256, 256>>>(c.elem, L.d_elem[slot], s.nelem);
+        DGOP_CUDA(cudaGetLastError());
+        d.elem = L.d_elem[slot];
+      }
+    }
+    return DGOP_OK;
+  };
+  int rc = fill(p.sigma, sig, 0);
+  if (rc) return rc;
+  for (int k = 0; k < D; ++k) {
+    rc = fill(p.beta[k], beta[k], k + 1);
+    if (rc) return rc;
+  }
+  // launch shape
+  int max_smem = 0;
+  DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+  const int sms = device_sm_count(op->device);
+  const int64_t per_elem_bytes = (int64_t)e->per_elem * sizeof(Real);
+  const int threads = 256;
+  int eb;
+  bool use_scratch = false;
+  const int64_t budget = 100 * 1024;
+  if (per_elem_bytes + generic_fixed_bytes_rt(D, e->mats, 1, sizeof(Real)) > max_smem - 1024) {
+    use_scratch = true;
+    eb = 1;
+  } else {
+    eb = (int)std::max<int64_t>(1, std::min<int64_t>(64, budget / per_elem_bytes));
+    const int64_t want_ctas = 2LL * sms;
+    while (eb > 1 && (s.nelem + eb - 1) / eb < want_ctas) eb /= 2;
+  }
+  L.eb = eb;
+  p.eb = eb;
+  size_t smem = generic_fixed_bytes_rt(D, e->mats, eb, sizeof(Real));
+  if (!use_scratch) smem += (size_t)eb * per_elem_bytes;
+  smem = (smem + 15) & ~size_t(15);
+  // the attribute is per kernel: allow the device maximum so operators sharing a kernel never
+  // lower each other's limit; occupancy below uses this launch's actual size.
+  DGOP_CUDA(cudaFuncSetAttribute(e->func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  if ((int)smem > max_smem) {
+    set_error("shared memory request exceeds the device limit");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  int per_sm = 0;
+  DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, e->func, threads, smem));
+  if (per_sm < 1) per_sm = 1;
+  const int64_t need = (s.nelem + eb - 1) / eb;
+  int64_t grid = std::min<int64_t>(need, (int64_t)sms * per_sm);
+  if (use_scratch) {
+    grid = std::min<int64_t>(grid, (int64_t)sms * 2);
+    p.scratch_per_cta = e->per_elem;
+    DGOP_CUDA(cudaMalloc(&L.d_scratch, sizeof(Real) * (size_t)grid * e->per_elem));
+    p.scratch = L.d_scratch;
+  }
+  L.grid = dim3((unsigned)std::max<int64_t>(grid, 1));
+  L.block = dim3(threads);
+  L.smem = smem;
+  L.ready = true;
+  return DGOP_OK;
+}
+
+template <typename Real>
+void free_launch(LaunchCfg<Real>& L) {
+  if (L.d_tab) cudaFree(L.d_tab);
+  if (L.d_scratch) cudaFree(L.d_scratch);
+  for (auto* p : L.d_elem)
+    if (p) cudaFree(p);
+  L = LaunchCfg<Real>{};
+}
+
+int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta, int flags,
+                    double g, dgop_operator** out) {
+  if (!space || !out) {
+    set_error("null space or output handle");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  if (q < 1 || q > kMaxQ) {
+    set_error("q must be in [1, 8]");
+    return DGOP_ERR_ARG;
+  }
+  if ((flags & (kAdvCell | kFaceInt | kFaceBnd)) && !beta) {
+    set_error("advection needs a velocity coefficient (dim entries)");
+    return DGOP_ERR_ARG;
+  }
+  ensure_registry();
+  auto* op = new (std::nothrow) dgop_operator();
+  if (!op) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  op->sp = *space;
+  op->q = q;
+  op->flags = flags;
+  op->g = g;
+  cudaGetDevice(&op->device);
+  Tables1D t;
+  if (!make_tables(op->sp, q, t)) {
+    delete op;
+    set_error("basis tables");
+    return DGOP_ERR_ARG;
+  }
+  std::vector<double> pack;
+  PackedCoef sig, bet[kMaxDim];
+  dgop_coef one{};
+  one.constant = 1.0;
+  int rc = pack_coef(op->sp, q, (flags & kMass) ? (sigma ? sigma : &one) : nullptr, pack, sig);
+  for (int k = 0; rc == DGOP_OK && k < op->sp.D; ++k)
+    rc = pack_coef(op->sp, q, (flags & (kAdvCell | kFaceInt | kFaceBnd)) ? &beta[k] : nullptr, pack, bet[k]);
+  if (rc == DGOP_OK) rc = setup_launch<double>(op, op->f64, t, pack, sig, bet);
+  if (rc == DGOP_OK) {
+    // FP32 path is optional: absent instantiations only disable dgop_apply_f32.
+    const int rc32 = setup_launch<float>(op, op->f32, t, pack, sig, bet);
+    if (rc32 != DGOP_OK) {
+      free_launch(op->f32);
+      set_error("");
+    }
+  }
+  if (rc != DGOP_OK) {
+    free_launch(op->f64);
+    free_launch(op->f32);
+    delete op;
+    return rc;
+  }
+  *out = op;
+  return DGOP_OK;
+}
+
+}  // namespace
+
+template <typename Real>
+static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, Real alpha, const Real* x, Real beta_y, Real* y,
+                       int extra_flags, cudaStream_t s) {
+  if (!L.ready) {
+    set_error("operator has no kernel for this precision");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (!x || !y) {
+    set_error("null vector");
+    return DGOP_ERR_ARG;
+  }
+  if (x == y) {
+    set_error("in-place apply is not supported (x and y alias)");
+    return DGOP_ERR_ARG;
+  }
+  OpParams<Real> p = L.params;
+  p.x = x;
+  p.y = y;
+  p.alpha = alpha;
+  p.beta_y = beta_y;
+  p.flags = op->flags | extra_flags;
+  L.entry->launch(p, L.grid, L.block, L.smem, s);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
+  return DGOP_OK;
+}
+
+int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
+               cudaStream_t s) {
+  return launch_impl<double>(op, op->f64, alpha, x, beta_y, y, extra_flags, s);
+}
+
+int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
+               cudaStream_t s) {
+  return launch_impl<float>(op, op->f32, alpha, x, beta_y, y, extra_flags, s);
+}
+
+}  // namespace dgop
+
+using namespace dgop;
+
+extern "C" {
+
+const char* dgop_last_error(void) { return dgop::g_last_error.c_str(); }
+
+const char* dgop_version(void) { return "dgop-b200 0.1 (sm_100a)"; }
+
+int dgop_fill_random(double* out, int64_t n, unsigned seed, double lo, double hi) {
+  if (!out || n < 0) {
+    set_error("dgop_fill_random: bad arguments");
+    return DGOP_ERR_ARG;
+  }
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<double> dist(lo, hi);
+  for (int64_t i = 0; i < n; ++i) out[i] = dist(rng);
+  return DGOP_OK;
+}
+
+int dgop_space_create(int dim, const int64_t* n_elem, const double* h, const double* origin, const int* periodic,
+                      int order, int basis, dgop_space** out) {
+  if (!out) {
+    set_error("null output handle");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  if (dim < 1 || dim > DGOP_MAX_DIM || !n_elem || !h) {
+    set_error("dim must be in [1, 6] and n_elem, h non-null");
+    return DGOP_ERR_ARG;
+  }
+  if (order < 0 || order + 1 > kMaxN) {
+    set_error("order must be in [0, 7]");
+    return DGOP_ERR_ARG;
+  }
+  if (basis != DGOP_BASIS_GLL && basis != DGOP_BASIS_GL) {
+    set_error("basis must be DGOP_BASIS_GLL or DGOP_BASIS_GL");
+    return DGOP_ERR_ARG;
+  }
+  auto* s = new (std::nothrow) dgop_space();
+  if (!s) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  s->D = dim;
+  s->P = order;
+  s->n = order + 1;
+  s->basis = basis;
+  s->nelem = 1;
+  int64_t nd = 1;
+  for (int k = 0; k < dim; ++k) {
+    if (n_elem[k] < 1 || !(h[k] > 0.0) || !std::isfinite(h[k])) {
+      delete s;
+      set_error("n_elem must be >= 1 and h > 0 on every axis");
+      return DGOP_ERR_ARG;
+    }
+    s->sizes[k] = n_elem[k];
+    s->h[k] = h[k];
+    s->origin[k] = origin ? origin[k] : 0.0;
+    s->periodic[k] = periodic ? (periodic[k] != 0) : 0;
+    s->nelem *= n_elem[k];
+    nd *= s->n;
+  }
+  s->ndofs = s->nelem * nd;
+  *out = s;
+  return DGOP_OK;
+}
+
+int dgop_space_destroy(dgop_space* space) {
+  delete space;
+  return DGOP_OK;
+}
+
+int64_t dgop_space_num_dofs(const dgop_space* space) { return space ? space->ndofs : -1; }
+
+int64_t dgop_space_num_elements(const dgop_space* space) { return space ? space->nelem : -1; }
+
+int dgop_space_coordinates(const dgop_space* space, int q, int axis, double* coords) {
+  if (!space || !coords || axis < 0 || axis >= space->D || q < 1 || q > kMaxQ) {
+    set_error("dgop_space_coordinates: bad arguments");
+    return DGOP_ERR_ARG;
+  }
+  double xq[kMaxQ], wq[kMaxQ];
+  gauss_points(1, q, xq, wq);
+  const double h = space->h[axis], o = space->origin[axis];
+  for (int64_t e = 0; e < space->sizes[axis]; ++e) {
+    // X = cell origin + h * xhat (hypercubecell.hpp:41-52, cartesianndmesh.hpp:95-105)
+    const double cell = o + h * (double)e;
+    for (int j = 0; j < q; ++j) coords[e * (q + 2) + j] = cell + h * xq[j];
+    coords[e * (q + 2) + q] = cell + h * 0.0;
+    coords[e * (q + 2) + q + 1] = cell + h * 1.0;
+  }
+  return DGOP_OK;
+}
+
+int dgop_mass_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out) {
+  return create_operator(space, q, sigma, nullptr, kMass, 0.0, out);
+}
+
+int dgop_advection_create(const dgop_space* space, int q, const dgop_coef* beta, int bc, double bc_value,
+                          dgop_operator** out) {
+  if (bc != DGOP_BC_NONE && bc != DGOP_BC_INFLOW) {
+    set_error("bc must be DGOP_BC_NONE or DGOP_BC_INFLOW");
+    return DGOP_ERR_ARG;
+  }
+  const int flags = kAdvCell | kFaceInt | (bc == DGOP_BC_INFLOW ? kFaceBnd : 0);
+  return create_operator(space, q, nullptr, beta, flags, bc_value, out);
+}
+
+int dgop_mass_advection_create(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta,
+                               dgop_operator** out) {
+  return create_operator(space, q, sigma, beta, kMass | kAdvCell | kFaceInt, 0.0, out);
+}
+
+int dgop_system_create(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta, int bc,
+                       double bc_value, dgop_operator** out) {
+  if (bc != DGOP_BC_NONE && bc != DGOP_BC_INFLOW) {
+    set_error("bc must be DGOP_BC_NONE or DGOP_BC_INFLOW");
+    return DGOP_ERR_ARG;
+  }
+  const int flags = kMass | kAdvCell | kFaceInt | (bc == DGOP_BC_INFLOW ? kFaceBnd : 0);
+  return create_operator(space, q, sigma, beta, flags, bc_value, out);
+}
+
+int dgop_operator_destroy(dgop_operator* op) {
+  if (!op) return DGOP_OK;
+  free_launch(op->f64);
+  free_launch(op->f32);
+  delete op;
+  return DGOP_OK;
+}
+
+int64_t dgop_operator_num_dofs(const dgop_operator* op) { return op ? op->sp.ndofs : -1; }
+
+int dgop_apply(dgop_operator* op, const double* x, double* y, void* stream) {
+  if (!op) {
+    set_error("null operator");
+    return DGOP_ERR_ARG;
+  }
+  return launch_f64(op, 1.0, x, 0.0, y, 0, (cudaStream_t)stream);
+}
+
+int dgop_apply_ex(dgop_operator* op, double alpha, const double* x, double beta, double* y, void* stream) {
+  if (!op) {
+    set_error("null operator");
+    return DGOP_ERR_ARG;
+  }
+  return launch_f64(op, alpha, x, beta, y, 0, (cudaStream_t)stream);
+}
+
+int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* stream) {
+  if (!op) {
+    set_error("null operator");
+    return DGOP_ERR_ARG;
+  }
+  return launch_f64(op, 1.0, x, 0.0, y, kTranspose, (cudaStream_t)stream);
+}
+
+int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream) {
+  if (!op) {
+    set_error("null operator");
+    return DGOP_ERR_ARG;
+  }
+  return launch_f32(op, 1.0f, x, 0.0f, y, 0, (cudaStream_t)stream);
+}
+
+}  // extern "C"

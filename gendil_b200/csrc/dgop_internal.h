@@ -1,0 +1,57 @@
+// Internal definitions shared by the C-ABI implementation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "dgop.h"
+#include "dgop_params.h"
+#include "registry.h"
+
+struct dgop_space {
+  int D = 0, P = 0, n = 0, basis = 0;
+  int64_t sizes[DGOP_MAX_DIM] = {};
+  double h[DGOP_MAX_DIM] = {}, origin[DGOP_MAX_DIM] = {};
+  int periodic[DGOP_MAX_DIM] = {};
+  int64_t nelem = 0, ndofs = 0;
+};
+
+namespace dgop {
+
+template <typename Real>
+struct LaunchCfg {
+  const GenericEntry<Real>* entry = nullptr;
+  OpParams<Real> params{};  // x, y, alpha, beta_y and flags are set per call
+  int eb = 1;
+  dim3 grid, block;
+  size_t smem = 0;
+  Real* d_tab = nullptr;
+  Real* d_scratch = nullptr;
+  Real* d_elem[kMaxDim + 1] = {};  // converted per-element factors (FP32 only)
+  bool ready = false;
+};
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+}  // namespace dgop
+
+struct dgop_operator {
+  dgop_space sp;
+  int q = 0;
+  int flags = 0;
+  double g = 0.0;
+  int device = 0;
+  dgop::LaunchCfg<double> f64;
+  dgop::LaunchCfg<float> f32;
+};
+
+namespace dgop {
+// Launch the operator kernel: y = alpha * Op(x) + beta_y * y, with `extra_flags` or-ed in.
+int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
+               cudaStream_t s);
+int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
+               cudaStream_t s);
+}  // namespace dgop

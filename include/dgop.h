@@ -1,0 +1,102 @@
+/* dgop -- B200-native matrix-free DG operators (mass, upwind advection) behind a C ABI.
+ *
+ * All vectors are caller-owned DEVICE pointers in the reference's L2 layout: element-major,
+ * elements numbered x-fastest, each element block FIFO with axis 0 fastest
+ * (GenDiL FiniteElementMethod/MatrixFreeOperators/KernelOperators/DoFIO/elementtensorview.hpp:42-48).
+ * Every entry point returns DGOP_OK (0) or a negative error code and never aborts; the message
+ * of the last error on the calling thread is returned by dgop_last_error().  Applies take an
+ * explicit cudaStream_t (passed as void*), allocate nothing and do not synchronize.
+ */
+#ifndef DGOP_H
+#define DGOP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dgop_status {
+  DGOP_OK = 0,
+  DGOP_ERR_ARG = -1,         /* invalid argument (sizes, null pointers, unsupported order) */
+  DGOP_ERR_CUDA = -2,        /* a CUDA call failed */
+  DGOP_ERR_ALLOC = -3,       /* device or host allocation failed */
+  DGOP_ERR_UNSUPPORTED = -4, /* no kernel for this (dimension, order, quadrature) */
+  DGOP_ERR_NOT_CONVERGED = -5,
+  DGOP_ERR_TIMEOUT = -6
+};
+
+enum dgop_basis { DGOP_BASIS_GLL = 0, DGOP_BASIS_GL = 1 };
+enum dgop_bc { DGOP_BC_NONE = 0, DGOP_BC_INFLOW = 1 };
+enum dgop_precision { DGOP_FP64 = 0, DGOP_FP32 = 1 };
+
+typedef struct dgop_space dgop_space;
+typedef struct dgop_operator dgop_operator;
+
+/* A scalar coefficient c(X) = constant + sum_{t < nterms} prod_k T_{t,k}(X_k), times an optional
+ * per-element factor.  tables[t][k] is a HOST array of n_elem[k] * (q + 2) samples of T_{t,k}
+ * at the coordinates returned by dgop_space_coordinates (NULL = factor 1);
+ * element_factor is a DEVICE array of num_elements values (NULL = 1).  This is the closed set of
+ * coefficients the reference's user lambdas reduce to on Cartesian meshes: constants, functions
+ * of one coordinate per factor (massoperator.hpp:78, advectionoperator.hpp:317), sums of such
+ * products, and piecewise-constant element fields. */
+#define DGOP_MAX_TERMS 4
+#define DGOP_MAX_DIM 6
+typedef struct {
+  double constant;
+  int nterms;
+  const double* tables[DGOP_MAX_TERMS][DGOP_MAX_DIM];
+  const double* element_factor;
+} dgop_coef;
+
+/* ---- spaces (CartesianMesh<D> + MakeLobatto/LegendreFiniteElement + MakeFiniteElementSpace:
+ *      Meshes/MeshDataStructures/CartesianMesh/cartesianndmesh.hpp:44, finiteelement.hpp:103,109,
+ *      finiteelementspace.hpp:84) */
+int dgop_space_create(int dim, const int64_t* n_elem, const double* h, const double* origin,
+                      const int* periodic, int order, int basis, dgop_space** out);
+int dgop_space_destroy(dgop_space* space);
+int64_t dgop_space_num_dofs(const dgop_space* space);
+int64_t dgop_space_num_elements(const dgop_space* space);
+/* The n_elem[axis] * (q + 2) coordinates at which coefficient tables are sampled: element e,
+ * point j < q is Gauss point j, j = q is the element's lower face, j = q + 1 its upper face. */
+int dgop_space_coordinates(const dgop_space* space, int q, int axis, double* coords);
+
+/* ---- operators
+ * mass:            y = M_sigma x                   (MakeMassFiniteElementOperator, massoperator.hpp:270)
+ * advection:       y = A x, bc NONE skips boundary faces (advectionoperator.hpp:1416),
+ *                  INFLOW uses the constant inflow value bc_value (advectionoperator.hpp:1481)
+ * mass_advection:  y = (M_sigma + A_interior) x   (MassAdvectionOperator, massadvectionoperator.hpp:329)
+ * system:          y = (M_sigma + A) x with the given boundary treatment, one fused launch
+ *                  (the (M/dt + A) implicit-Euler operator the reference composes from the two). */
+int dgop_mass_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out);
+int dgop_advection_create(const dgop_space* space, int q, const dgop_coef* beta, int bc, double bc_value,
+                          dgop_operator** out);
+int dgop_mass_advection_create(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta,
+                               dgop_operator** out);
+int dgop_system_create(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta, int bc,
+                       double bc_value, dgop_operator** out);
+int dgop_operator_destroy(dgop_operator* op);
+int64_t dgop_operator_num_dofs(const dgop_operator* op);
+
+/* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers.
+ * (MassFiniteElementOperator::operator() massoperator.hpp:209, AdvectionOperator::operator()
+ * advectionoperator.hpp:1070: both overwrite y.) */
+int dgop_apply(dgop_operator* op, const double* x, double* y, void* stream);
+int dgop_apply_ex(dgop_operator* op, double alpha, const double* x, double beta, double* y, void* stream);
+/* y = A^T x: the adjoint of the linear part (inflow value treated as 0); no reference counterpart. */
+int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* stream);
+/* FP32 apply of the same operator (tables rounded to FP32); no reference counterpart. */
+int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
+
+/* FillRandom (Algebra/vector.hpp:632): out[i] = std::uniform_real_distribution<double>(lo, hi)
+ * draws from std::mt19937(seed), in order, into a HOST buffer of n values. */
+int dgop_fill_random(double* out, int64_t n, unsigned seed, double lo, double hi);
+
+const char* dgop_last_error(void);
+const char* dgop_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGOP_H */

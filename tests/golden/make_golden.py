@@ -1,0 +1,143 @@
+"""Generate the golden fixtures from the GenDiL reference itself.
+
+Run in a container that holds the reference source (it builds ``oracle/_ref`` first with
+``make -C oracle ref``):
+
+    python tests/golden/make_golden.py
+
+It writes ``tests/golden/cases.json`` (case descriptions) and ``tests/golden/golden.npz``
+(reference outputs).  Inputs are not stored: they are ``FillRandom(seed)`` draws
+(Algebra/vector.hpp:632), which the fixtures also pin (``rng_seed<k>`` prefixes), so the
+tests regenerate them bit-exactly.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.bindings import Reference, num_dofs  # noqa: E402
+
+
+def cube(D, n, P, Q, basis=0, h=None, origin=None, periodic=None, sizes=None):
+    sizes = list(sizes) if sizes is not None else [n] * D
+    h = list(h) if h is not None else [1.0 / s for s in sizes]
+    return {"D": D, "P": P, "Q": Q, "basis": basis, "sizes": sizes, "h": h,
+            "origin": list(origin) if origin is not None else [0.0] * D,
+            "periodic": list(periodic) if periodic is not None else [0] * D}
+
+
+def mass_cases():
+    c = []
+    c.append(("m1", dict(cube(1, 5, 0, 1), sigma_kind=0, sigma_c=1.0)))
+    c.append(("m2", dict(cube(1, 7, 3, 5, origin=[0.5]), sigma_kind=1)))
+    c.append(("m3", dict(cube(1, 4, 7, 8), sigma_kind=1)))
+    c.append(("m4", dict(cube(2, 0, 0, 1, sizes=[3, 4]), sigma_kind=0, sigma_c=2.5)))
+    c.append(("m5", dict(cube(2, 0, 2, 4, sizes=[4, 3], h=[0.25, 1 / 3], origin=[-1.0, 0.5]), sigma_kind=1)))
+    c.append(("m6", dict(cube(2, 3, 4, 3), sigma_kind=1)))
+    c.append(("m7", dict(cube(2, 0, 2, 3, basis=1, sizes=[3, 2]), sigma_kind=1)))
+    c.append(("m8", dict(cube(3, 0, 1, 4, sizes=[3, 2, 2]), sigma_kind=1)))
+    c.append(("m9", dict(cube(3, 4, 3, 4), sigma_kind=0, sigma_c=1.0)))
+    c.append(("m10", dict(cube(3, 3, 3, 6), sigma_kind=1)))
+    c.append(("m11", dict(cube(3, 0, 2, 2, basis=1, sizes=[2, 3, 2]), sigma_kind=1)))
+    c.append(("m12", dict(cube(3, 2, 7, 8), sigma_kind=1)))
+    c.append(("m13", dict(cube(4, 2, 2, 3), sigma_kind=1)))
+    c.append(("m14", dict(cube(5, 2, 1, 2), sigma_kind=1)))
+    c.append(("m15", dict(cube(6, 2, 1, 2), sigma_kind=1)))
+    c.append(("m16", dict(cube(6, 0, 2, 3, sizes=[2, 1, 2, 1, 2, 1]), sigma_kind=1)))
+    return c
+
+
+def adv_cases():
+    c = []
+    c.append(("a1", dict(cube(1, 6, 0, 1), beta_kind=0, beta_c=[0.7], g=0.3, sigma_kind=0, sigma_c=2.0)))
+    c.append(("a2", dict(cube(1, 5, 2, 4), beta_kind=1, g=0.3, sigma_kind=1)))
+    c.append(("a2s", dict(cube(1, 5, 2, 4), beta_kind=2, g=0.0, sigma_kind=1)))
+    c.append(("a2p", dict(cube(1, 5, 2, 4, periodic=[1]), beta_kind=2, g=0.0, sigma_kind=0, sigma_c=1.0)))
+    c.append(("a3", dict(cube(2, 3, 1, 2, basis=1), beta_kind=0, beta_c=[0.7, -0.3], g=0.3, sigma_kind=0, sigma_c=3.0)))
+    c.append(("a4", dict(cube(2, 0, 2, 3, sizes=[4, 3], h=[0.25, 1 / 3], origin=[-1.0, 0.5]), beta_kind=2, g=0.3,
+                         sigma_kind=1)))
+    c.append(("a4b", dict(cube(2, 0, 2, 3, sizes=[4, 3]), beta_kind=1, g=0.0, sigma_kind=1)))
+    c.append(("a4p", dict(cube(2, 0, 2, 3, sizes=[4, 3], origin=[-0.5, -0.5]), beta_kind=3, g=0.2, sigma_kind=0,
+                          sigma_c=1.0)))
+    c.append(("a4per", dict(cube(2, 0, 2, 3, sizes=[4, 3], periodic=[1, 0]), beta_kind=2, g=0.1, sigma_kind=0,
+                            sigma_c=1.0)))
+    c.append(("a5", dict(cube(2, 3, 4, 3), beta_kind=0, beta_c=[-0.4, 0.9], g=0.5, sigma_kind=0, sigma_c=1.0)))
+    c.append(("a6", dict(cube(3, 3, 0, 2), beta_kind=0, beta_c=[0.7, -0.3, 0.4], g=0.3, sigma_kind=0, sigma_c=1.0)))
+    c.append(("a7", dict(cube(3, 0, 1, 3, sizes=[3, 2, 4]), beta_kind=1, g=0.0, sigma_kind=1)))
+    c.append(("a8", dict(cube(3, 4, 3, 4), beta_kind=2, g=0.0, sigma_kind=0, sigma_c=1000.0)))
+    c.append(("a8g", dict(cube(3, 4, 3, 4), beta_kind=2, g=0.3, sigma_kind=1)))
+    c.append(("a8per", dict(cube(3, 4, 3, 4, periodic=[1, 0, 1]), beta_kind=2, g=0.0, sigma_kind=0, sigma_c=1.0)))
+    c.append(("a9", dict(cube(3, 0, 2, 2, basis=1, sizes=[2, 2, 3]), beta_kind=0, beta_c=[-0.5, 0.25, 0.8], g=0.3,
+                         sigma_kind=0, sigma_c=1.0)))
+    c.append(("a10", dict(cube(3, 2, 5, 6), beta_kind=2, g=0.0, sigma_kind=1)))
+    c.append(("a11", dict(cube(3, 0, 7, 8, sizes=[2, 2, 1]), beta_kind=0, beta_c=[0.3, -0.6, 0.2], g=0.1,
+                          sigma_kind=0, sigma_c=1.0)))
+    c.append(("a12", dict(cube(4, 0, 1, 2, sizes=[2, 3, 2, 2], origin=[0, 0, -1, -1], h=[0.5, 1 / 3, 1, 1]),
+                          beta_kind=3, g=0.0, sigma_kind=1)))
+    c.append(("a13", dict(cube(5, 2, 1, 2), beta_kind=0, beta_c=[0.5, -0.5, 0.3, -0.2, 0.1], g=0.2, sigma_kind=0,
+                          sigma_c=1.0)))
+    c.append(("a14", dict(cube(6, 0, 2, 3, sizes=[2, 2, 1, 2, 1, 2], h=[0.5, 0.5, 1.0, 1.0, 2.0, 1.0],
+                          origin=[0, 0, 0, -1, -1, -1]),
+                          beta_kind=3, g=0.0, sigma_kind=0, sigma_c=200.0)))
+    return c
+
+
+def main():
+    ref = Reference()
+    cases = {"mass": [], "advection": [], "cg": [], "gmres": []}
+    arrays = {}
+    for seed in (0, 1, 2, 3, 12345):
+        arrays[f"rng_seed{seed}"] = ref.fill_random(256, seed)
+    for kind in (0, 1):
+        for n in range(1, 9):
+            c, w = ref.points(kind, n)
+            arrays[f"points_{kind}_{n}_x"] = c
+            arrays[f"points_{kind}_{n}_w"] = w
+    for cid, case in mass_cases():
+        case = dict(case, seed=0)
+        x = ref.fill_random(num_dofs(case), case["seed"])
+        arrays[f"{cid}_y"] = ref.mass_apply(case, x)
+        cases["mass"].append({"id": cid, **case})
+    for cid, case in adv_cases():
+        case = dict(case, seed=1)
+        x = ref.fill_random(num_dofs(case), case["seed"])
+        for mode in (0, 1, 2):
+            arrays[f"{cid}_mode{mode}_y"] = ref.advection_apply(case, x, mode)
+        cases["advection"].append({"id": cid, **case})
+    # CG on the mass operator: b = M u (u from seed 0), x0 = 0 (conjugategradient.hpp:125)
+    for cid, case, iters, tol in (("cg1", dict(cube(3, 4, 3, 4), sigma_kind=0, sigma_c=1.0), 20, 1e-6),
+                                  ("cg2", dict(cube(3, 4, 3, 4), sigma_kind=1), 500, 1e-12),
+                                  ("cg3", dict(cube(1, 10, 3, 5), sigma_kind=0, sigma_c=1.0), 500, 1e-12)):
+        u = ref.fill_random(num_dofs(case), 0)
+        try:
+            b = ref.mass_apply(case, u)
+            x, info = ref.mass_cg(case, b, np.zeros_like(b), iters, tol)
+        except NotImplementedError:
+            continue
+        arrays[f"{cid}_x"] = x
+        cases["cg"].append({"id": cid, **case, "max_iters": iters, "tol": tol, **info})
+    # GMRES(30) on sigma M + A, b from seed 2 (gmres.hpp:74)
+    for cid, case, dt in (("gm1", dict(cube(3, 4, 3, 4), beta_kind=2, g=0.0), 1e-3),
+                          ("gm2", dict(cube(2, 8, 2, 3), beta_kind=2, g=0.0), 1e-3),
+                          ("gm3", dict(cube(1, 16, 2, 4), beta_kind=1, g=0.0), 1e-2)):
+        case = dict(case, sigma_c=1.0 / dt)
+        b = ref.fill_random(num_dofs(case), 2)
+        x, info = ref.system_gmres(case, b, np.zeros_like(b), 5000, 30, 1e-10)
+        arrays[f"{cid}_x"] = x
+        cases["gmres"].append({"id": cid, **case, "restart": 30, "tol": 1e-10, "max_iters": 5000, **info})
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(cases, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **arrays)
+    total = sum(a.nbytes for a in arrays.values())
+    print(f"wrote {len(arrays)} arrays ({total / 1e6:.2f} MB raw)")
+
+
+if __name__ == "__main__":
+    main()
