@@ -171,7 +171,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    space = g.Space(3, [N_AXIS] * 3, order=ORDER)
+    space = g.Space(3, [args.size] * 3, order=ORDER)
     op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
     nd = space.num_dofs
     x_np = g.fill_random(nd, 1)
@@ -251,7 +251,10 @@ def run_ours(args):
                         "d2h_bytes_per_step": 8 * nd, "steps": e_steps},
                 "gpu_launches": args.steps,
                 "clocks": clocks.summary()}
-        if world == 1 and not args.no_cpu_baseline:
+        line["config"]["kernel"] = op.kernel
+        if args.size != N_AXIS:
+            line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
+        if world == 1 and not args.no_cpu_baseline and args.size == N_AXIS:
             try:
                 line["cpu_baseline"] = cpu_baseline(x_np)
             except Exception as exc:  # the baseline is reported, never required
@@ -269,6 +272,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=N_AXIS, help="elements per axis (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -76,6 +76,10 @@ def lib():
         L.dgop_apply_transpose.argtypes = [vp, vp, vp, vp]
         L.dgop_apply_f32.argtypes = [vp, vp, vp, vp]
         L.dgop_fill_random.argtypes = [vp, i64, ctypes.c_uint, d, d]
+        L.dgop_operator_kernel.argtypes = [vp]
+        L.dgop_operator_kernel_note.argtypes = [vp]
+        L.dgop_operator_kernel_note.restype = ctypes.c_char_p
+        L.dgop_operator_select_kernel.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -207,6 +211,19 @@ class _Operator:
     @property
     def num_dofs(self):
         return self.space.num_dofs
+
+    @property
+    def kernel(self):
+        """'generic' (sum-factorized) or 'kron' (register-resident Kronecker form)."""
+        return ("generic", "kron")[lib().dgop_operator_kernel(self.handle)]
+
+    @property
+    def kernel_note(self):
+        return lib().dgop_operator_kernel_note(self.handle).decode()
+
+    def select_kernel(self, name):
+        check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1}[name]))
+        return self
 
     def close(self):
         if self.handle:

@@ -27,7 +27,7 @@ BASE_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 # Non-instantiation sources; gen_generic.cu is compiled once per (dimension, N).
-SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "blas.cu", "krylov.cu"]
+SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "kron_plan.cpp", "gen_kron3d.cu", "blas.cu", "krylov.cu"]
 
 
 def nvcc():

@@ -92,9 +92,18 @@ def velocity_phase_space(dim):
     return out
 
 
+def density_separable(dim):
+    """(1 + 0.5 x0) (1 + x1^2) (2 - x2): one separable product (dim >= 3)."""
+    if dim < 3:
+        raise ValueError("density_separable needs dim >= 3")
+    return Coefficient(terms=[{0: lambda x: 1.0 + 0.5 * x, 1: lambda x: 1.0 + x * x, 2: lambda x: 2.0 - x}])
+
+
 def sigma_preset(kind, dim, c=1.0):
-    """The oracle's sigma presets: 0 constant c, 1 density_poly."""
-    return constant(c) if kind == 0 else density_poly(dim)
+    """The oracle's sigma presets: 0 constant c, 1 density_poly, 2 density_separable."""
+    if kind == 0:
+        return constant(c)
+    return density_poly(dim) if kind == 1 else density_separable(dim)
 
 
 def beta_preset(kind, dim, c=None):

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "basis.h"
+#include "kron_plan.h"
 #include "dgop_internal.h"
 
 namespace dgop {
@@ -223,6 +224,171 @@ int setup_launch(dgop_operator* op, LaunchCfg<Real>& L, const Tables1D& t, const
   return DGOP_OK;
 }
 
+// A coefficient in the Kronecker planner's form: a constant, or one product term (no constant).
+SepCoef sep_of(const dgop_coef* c) {
+  SepCoef s;
+  if (!c) {
+    s.separable = true;
+    s.c = 1.0;
+    return s;
+  }
+  s.has_elem = c->element_factor != nullptr;
+  if (c->nterms == 0) {
+    s.separable = true;
+    s.c = c->constant;
+  } else if (c->nterms == 1 && c->constant == 0.0) {
+    s.separable = true;
+    s.c = 1.0;
+    for (int k = 0; k < DGOP_MAX_DIM; ++k) s.tab[k] = c->tables[0][k];
+  }
+  return s;
+}
+
+template <typename Real>
+int upload(Real** dst, const double* src, size_t n) {
+  std::vector<Real> tmp(src, src + n);
+  DGOP_CUDA(cudaMalloc(dst, sizeof(Real) * (n ? n : 1)));
+  if (n) DGOP_CUDA(cudaMemcpy(*dst, tmp.data(), sizeof(Real) * n, cudaMemcpyHostToDevice));
+  return DGOP_OK;
+}
+
+template <typename Real>
+int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, const double* elem_sigma,
+               const double* const* elem_beta) {
+  const dgop_space& s = op->sp;
+  KronEntry<Real>* entry = nullptr;
+  if constexpr (sizeof(Real) == 8) entry = &kron3d_slot_f64(s.n);
+  else entry = &kron3d_slot_f32(s.n);
+  if (!entry->launch) {
+    set_error("no Kronecker kernel for this order");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  K.entry = entry;
+  KronParams<Real>& p = K.params;
+  std::memset(&p, 0, sizeof(p));
+  p.nelem = s.nelem;
+  p.fdx = FastDiv((uint32_t)s.sizes[0]);
+  p.fdy = FastDiv((uint32_t)s.sizes[1]);
+  for (int k = 0; k < 3; ++k) {
+    p.sizes[k] = s.sizes[k];
+    p.periodic[k] = s.periodic[k];
+  }
+  p.flags = op->flags;
+  p.has_adv = plan.has_adv;
+  p.has_mass = plan.has_mass;
+  p.mass_merged = plan.mass_merged;
+  p.g = (Real)op->g;
+  int rc = upload<Real>(&K.d_mats, plan.mats.data(), plan.mats.size());
+  if (rc) return rc;
+  p.mats = K.d_mats;
+  // slot -> matrix table; constant tables go to kernel-parameter space
+  const int N = s.n;
+  auto put = [&](KronParams<Real>& q, int slot, const KronMat& m) {
+    q.vary[slot] = 0;
+    q.vm[slot] = m;
+    if (m.off < 0) return;  // slot unused by this operator
+    if (m.stride == 0) {
+      for (int i = 0; i < N * N; ++i) q.cm[slot][i] = (Real)plan.mats[m.off + i];
+    } else {
+      q.vary[slot] = 1;
+    }
+  };
+  if (plan.has_adv) {
+    put(p, kSlotDX, plan.D[0]);
+    put(p, kSlotDY, plan.D[1]);
+    put(p, kSlotDZ, plan.D[2]);
+    put(p, kSlotTXY, plan.T[0][1]);
+    put(p, kSlotTXZ, plan.T[0][2]);
+    put(p, kSlotTYZ, plan.T[1][2]);
+    put(p, kSlotTYX, plan.T[1][0]);
+    put(p, kSlotTZX, plan.T[2][0]);
+    put(p, kSlotTZY, plan.T[2][1]);
+    if (plan.has_mass && !plan.mass_merged) {
+      put(p, kSlotMD, plan.MD);
+      put(p, kSlotMX, plan.MT[0]);
+      put(p, kSlotMY, plan.MT[1]);
+    }
+    std::vector<double> phi;
+    std::vector<signed char> sg;
+    size_t phi_off[3], sg_off[3][3];
+    for (int a = 0; a < 3; ++a) {
+      phi_off[a] = phi.size();
+      phi.insert(phi.end(), plan.phi[a].begin(), plan.phi[a].end());
+      for (int k = 0; k < 3; ++k) {
+        sg_off[a][k] = sg.size();
+        sg.insert(sg.end(), plan.sgn[a][k].begin(), plan.sgn[a][k].end());
+      }
+    }
+    rc = upload<Real>(&K.d_phi, phi.data(), phi.size());
+    if (rc) return rc;
+    DGOP_CUDA(cudaMalloc(&K.d_sgn, sg.size() ? sg.size() : 1));
+    if (!sg.empty()) DGOP_CUDA(cudaMemcpy(K.d_sgn, sg.data(), sg.size(), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; ++a) {
+      p.phi[a] = K.d_phi + phi_off[a];
+      for (int k = 0; k < 3; ++k) p.sgn[a][k] = (k == a) ? nullptr : K.d_sgn + sg_off[a][k];
+    }
+  } else {
+    put(p, kSlotDZ, plan.MD);
+    put(p, kSlotTZX, plan.MT[0]);
+    put(p, kSlotTZY, plan.MT[1]);
+  }
+  auto elem_ptr = [&](const double* src, int slot, const Real** dst) -> int {
+    *dst = nullptr;
+    if (!src) return DGOP_OK;
+    if constexpr (sizeof(Real) == 8) {
+      *dst = src;
+    } else {
+      DGOP_CUDA(cudaMalloc(&K.d_elem[slot], sizeof(Real) * s.nelem));
+      convert_kernel<Real><<<256, 256>>>(src, K.d_elem[slot], s.nelem);
+      DGOP_CUDA(cudaGetLastError());
+      *dst = K.d_elem[slot];
+    }
+    return DGOP_OK;
+  };
+  for (int a = 0; a < 3; ++a)
+    if ((rc = elem_ptr(plan.has_adv ? elem_beta[a] : nullptr, a, &p.elem[a]))) return rc;
+  if ((rc = elem_ptr(plan.has_mass ? elem_sigma : nullptr, 3, &p.elem_mass))) return rc;
+  // transposed operator: the same blocks with the transposed D matrices
+  K.params_t = p;
+  if (plan.has_adv) {
+    put(K.params_t, kSlotDX, plan.Dt[0]);
+    put(K.params_t, kSlotDY, plan.Dt[1]);
+    put(K.params_t, kSlotDZ, plan.Dt[2]);
+  }
+  // persistent grid: every warp walks groups of entry->epw consecutive elements
+  const int threads = kKronThreads, warps = threads / 32;
+  K.block = dim3(threads);
+  K.smem = (size_t)warps * entry->warp_smem * sizeof(Real);
+  int max_smem = 0;
+  DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+  if ((int)K.smem > max_smem) {
+    set_error("Kronecker kernel shared memory exceeds the device limit");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  DGOP_CUDA(cudaFuncSetAttribute(entry->func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  DGOP_CUDA(cudaFuncSetAttribute(entry->func_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  const bool sep = plan.has_adv && plan.has_mass && !plan.mass_merged;
+  int per_sm = 0;
+  DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? entry->func_sep : entry->func, threads,
+                                                          K.smem));
+  if (per_sm < 1) per_sm = 1;
+  const int64_t groups = (s.nelem + entry->epw - 1) / entry->epw;
+  const int64_t ctas = std::min<int64_t>((groups + warps - 1) / warps, (int64_t)device_sm_count(op->device) * per_sm);
+  K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+  K.ready = true;
+  return DGOP_OK;
+}
+
+template <typename Real>
+void free_kron(KronCfg<Real>& K) {
+  if (K.d_mats) cudaFree(K.d_mats);
+  if (K.d_phi) cudaFree(K.d_phi);
+  if (K.d_sgn) cudaFree(K.d_sgn);
+  for (auto* p : K.d_elem)
+    if (p) cudaFree(p);
+  K = KronCfg<Real>{};
+}
+
 template <typename Real>
 void free_launch(LaunchCfg<Real>& L) {
   if (L.d_tab) cudaFree(L.d_tab);
@@ -271,13 +437,21 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
   int rc = pack_coef(op->sp, q, (flags & kMass) ? (sigma ? sigma : &one) : nullptr, pack, sig);
   for (int k = 0; rc == DGOP_OK && k < op->sp.D; ++k)
     rc = pack_coef(op->sp, q, (flags & (kAdvCell | kFaceInt | kFaceBnd)) ? &beta[k] : nullptr, pack, bet[k]);
-  if (rc == DGOP_OK) rc = setup_launch<double>(op, op->f64, t, pack, sig, bet);
+  std::string generic_err;
   if (rc == DGOP_OK) {
-    // FP32 path is optional: absent instantiations only disable dgop_apply_f32.
-    const int rc32 = setup_launch<float>(op, op->f32, t, pack, sig, bet);
-    if (rc32 != DGOP_OK) {
-      free_launch(op->f32);
-      set_error("");
+    rc = setup_launch<double>(op, op->f64, t, pack, sig, bet);
+    if (rc == DGOP_ERR_UNSUPPORTED) {
+      // no generic instantiation for this shape: acceptable when the Kronecker kernel covers it
+      generic_err = g_last_error;
+      free_launch(op->f64);
+      rc = DGOP_OK;
+    } else if (rc == DGOP_OK) {
+      // FP32 path is optional: absent instantiations only disable dgop_apply_f32.
+      const int rc32 = setup_launch<float>(op, op->f32, t, pack, sig, bet);
+      if (rc32 != DGOP_OK) {
+        free_launch(op->f32);
+        set_error("");
+      }
     }
   }
   if (rc != DGOP_OK) {
@@ -286,6 +460,50 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
     delete op;
     return rc;
   }
+  // Kronecker form, when the coefficients and basis allow it (see kron.h)
+  {
+    KronInputs in;
+    in.D = op->sp.D;
+    in.N = op->sp.n;
+    in.Q = q;
+    in.gll = op->sp.basis == DGOP_BASIS_GLL;
+    in.flags = flags;
+    in.sizes = op->sp.sizes;
+    in.h = op->sp.h;
+    in.B = t.B;
+    in.Dq = t.Dq;
+    in.wq = t.wq;
+    const dgop_coef* sg = (flags & kMass) ? (sigma ? sigma : &one) : nullptr;
+    in.sigma = sep_of(sg);
+    const bool adv = (flags & (kAdvCell | kFaceInt | kFaceBnd)) != 0;
+    const double* elem_beta[kMaxDim] = {};
+    for (int k = 0; k < op->sp.D; ++k) {
+      in.beta[k] = sep_of(adv ? &beta[k] : nullptr);
+      elem_beta[k] = adv ? beta[k].element_factor : nullptr;
+    }
+    KronPlanHost plan = plan_kron3d(in);
+    if (plan.ok) {
+      const double* es = sg ? sg->element_factor : nullptr;
+      const int krc = setup_kron<double>(op, op->k64, plan, es, elem_beta);
+      if (krc == DGOP_OK) {
+        if (setup_kron<float>(op, op->k32, plan, es, elem_beta) != DGOP_OK) free_kron(op->k32);
+        op->kernel = DGOP_KERNEL_KRON;
+      } else {
+        free_kron(op->k64);
+        op->kron_why = "Kronecker setup failed";
+      }
+      set_error("");
+    } else {
+      op->kron_why = plan.why;
+    }
+  }
+  if (!op->f64.ready && !op->k64.ready) {
+    free_launch(op->f32);
+    free_kron(op->k32);
+    delete op;
+    set_error(generic_err.empty() ? std::string("no kernel for this operator") : generic_err);
+    return DGOP_ERR_UNSUPPORTED;
+  }
   *out = op;
   return DGOP_OK;
 }
@@ -293,12 +511,8 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 }  // namespace
 
 template <typename Real>
-static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, Real alpha, const Real* x, Real beta_y, Real* y,
-                       int extra_flags, cudaStream_t s) {
-  if (!L.ready) {
-    set_error("operator has no kernel for this precision");
-    return DGOP_ERR_UNSUPPORTED;
-  }
+static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, Real alpha, const Real* x, Real beta_y,
+                       Real* y, int extra_flags, cudaStream_t s) {
   if (!x || !y) {
     set_error("null vector");
     return DGOP_ERR_ARG;
@@ -306,6 +520,22 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, Real alpha, const 
   if (x == y) {
     set_error("in-place apply is not supported (x and y alias)");
     return DGOP_ERR_ARG;
+  }
+  if (op->kernel == DGOP_KERNEL_KRON && K.ready) {
+    KronParams<Real> p = (extra_flags & kTranspose) ? K.params_t : K.params;
+    p.x = x;
+    p.y = y;
+    p.alpha = alpha;
+    p.beta_y = beta_y;
+    p.flags = op->flags | extra_flags;
+    K.entry->launch(p, K.grid, K.block, K.smem, s);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
+    return DGOP_OK;
+  }
+  if (!L.ready) {
+    set_error("operator has no kernel for this precision");
+    return DGOP_ERR_UNSUPPORTED;
   }
   OpParams<Real> p = L.params;
   p.x = x;
@@ -321,12 +551,12 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, Real alpha, const 
 
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
                cudaStream_t s) {
-  return launch_impl<double>(op, op->f64, alpha, x, beta_y, y, extra_flags, s);
+  return launch_impl<double>(op, op->f64, op->k64, alpha, x, beta_y, y, extra_flags, s);
 }
 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s) {
-  return launch_impl<float>(op, op->f32, alpha, x, beta_y, y, extra_flags, s);
+  return launch_impl<float>(op, op->f32, op->k32, alpha, x, beta_y, y, extra_flags, s);
 }
 
 }  // namespace dgop
@@ -458,11 +688,34 @@ int dgop_operator_destroy(dgop_operator* op) {
   if (!op) return DGOP_OK;
   free_launch(op->f64);
   free_launch(op->f32);
+  free_kron(op->k64);
+  free_kron(op->k32);
   delete op;
   return DGOP_OK;
 }
 
 int64_t dgop_operator_num_dofs(const dgop_operator* op) { return op ? op->sp.ndofs : -1; }
+
+int dgop_operator_kernel(const dgop_operator* op) { return op ? op->kernel : -1; }
+
+const char* dgop_operator_kernel_note(const dgop_operator* op) { return op ? op->kron_why : ""; }
+
+int dgop_operator_select_kernel(dgop_operator* op, int kernel) {
+  if (!op || (kernel != DGOP_KERNEL_GENERIC && kernel != DGOP_KERNEL_KRON)) {
+    set_error("dgop_operator_select_kernel: bad arguments");
+    return DGOP_ERR_ARG;
+  }
+  if (kernel == DGOP_KERNEL_KRON && !op->k64.ready) {
+    set_error(std::string("Kronecker kernel unavailable: ") + op->kron_why);
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (kernel == DGOP_KERNEL_GENERIC && !op->f64.ready) {
+    set_error("generic kernel not built for this shape");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  op->kernel = kernel;
+  return DGOP_OK;
+}
 
 int dgop_apply(dgop_operator* op, const double* x, double* y, void* stream) {
   if (!op) {

@@ -8,6 +8,8 @@
 
 #include "dgop.h"
 #include "dgop_params.h"
+#include "kron.h"
+#include "kron_registry.h"
 #include "registry.h"
 
 struct dgop_space {
@@ -33,6 +35,20 @@ struct LaunchCfg {
   bool ready = false;
 };
 
+template <typename Real>
+struct KronCfg {
+  bool ready = false;
+  const KronEntry<Real>* entry = nullptr;
+  KronParams<Real> params{};    // forward operator
+  KronParams<Real> params_t{};  // transposed operator
+  dim3 grid, block;
+  size_t smem = 0;
+  Real* d_mats = nullptr;
+  Real* d_phi = nullptr;
+  signed char* d_sgn = nullptr;
+  Real* d_elem[4] = {};  // converted per-element factors (FP32 only)
+};
+
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
@@ -44,8 +60,12 @@ struct dgop_operator {
   int flags = 0;
   double g = 0.0;
   int device = 0;
+  int kernel = 0;             // DGOP_KERNEL_GENERIC or DGOP_KERNEL_KRON
+  const char* kron_why = "";  // why the Kronecker form is unavailable
   dgop::LaunchCfg<double> f64;
   dgop::LaunchCfg<float> f32;
+  dgop::KronCfg<double> k64;
+  dgop::KronCfg<float> k32;
 };
 
 namespace dgop {

@@ -1,0 +1,99 @@
+// Kronecker ("1D matrix") form of the DG operators on Cartesian meshes.
+//
+// With every coefficient separable per axis -- beta_a(X) = c_a * prod_k f_ak(X_k) and
+// sigma(X) = c_s * prod_k g_k(X_k) -- and GLL nodes (face trace = face slice), each term of the
+// reference's sum-factorized operator (advectionoperator.hpp:269-441, massoperator.hpp:39-89)
+// collapses to a tensor product of per-axis n x n matrices that depend only on the element's
+// coordinate along that axis:
+//
+//   M_k^f[e]  = B^T W f B            (mass-type, symmetric)
+//   G_k^f[e]  = B^T Dq^T W f B       (collocated gradient along the component's own axis)
+//
+//   y_e = sum_a  T_a [ D_a u_e + sum_{inflow faces s} phi_s(e) e_s (x) trace_{1-s}(u_nb) ]
+//   T_a = (x)_{k != a} M_k^{f_ak}[e_k],   D_a = s_a G_a^{f_aa}[e_a] + sum_{outflow s} phi_s e_s e_s^T
+//
+// s_a = -c_a detJ / h_a, phi_s(e_a) = detJ c_a f_aa(face s) (+-1/h_a).  The upwind choice needs
+// the sign of beta . n to be uniform over each face, i.e. each tangential factor keeps one sign
+// on each element's Gauss points; the planner checks this and otherwise leaves the operator on
+// the generic sum-factorized kernel.  The mass term merges into the z term when its x and y
+// factors equal the z velocity's.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "dgop_params.h"
+#include "fastdiv.h"
+
+namespace dgop {
+
+constexpr int kKronMaxN = 5;
+
+// A per-axis matrix table: matrix for element coordinate e at off + e * stride (stride 0: one
+// matrix for all elements).  Offsets are into the plan's matrix buffer.
+struct KronMat {
+  int64_t off = -1;
+  int64_t stride = 0;
+};
+
+// Matrix slots of the 3D kernel (see kron3d_kernel.cuh); the axis each slot acts along is fixed.
+enum KronSlot : int {
+  kSlotDX = 0,   // x term, along x (forward or transposed D)
+  kSlotDY = 1,   // y term, along y
+  kSlotDZ = 2,   // z term (mass merged) or the mass term alone, along z
+  kSlotTXY = 3,  // x term, y tangential
+  kSlotTXZ = 4,  // x term, z tangential
+  kSlotTYZ = 5,  // y term, z tangential
+  kSlotTYX = 6,  // y term, x tangential
+  kSlotTZX = 7,  // z term, x tangential
+  kSlotTZY = 8,  // z term, y tangential
+  kSlotMD = 9,   // separate mass term, along z
+  kSlotMX = 10,  // separate mass term, x tangential
+  kSlotMY = 11,  // separate mass term, y tangential
+  kNumSlots = 12
+};
+
+template <typename Real>
+struct KronParams {
+  int64_t nelem;      // < 2^32 (checked by the planner)
+  FastDiv fdx, fdy;   // element index -> (x, y, z) coordinates
+  int64_t sizes[3];
+  int periodic[3];
+  int flags;          // kAdvCell / kFaceInt / kFaceBnd / kMass / kTranspose as in OpFlags
+  int has_adv;        // advection terms present
+  int has_mass;       // mass term present
+  int mass_merged;    // mass folded into the z term's D matrix
+  Real g;             // inflow value
+  Real alpha, beta_y;
+  const Real* x;
+  Real* y;
+  const Real* mats;                          // element-dependent matrix tables (device)
+  int vary[kNumSlots];                       // slot depends on the element coordinate
+  KronMat vm[kNumSlots];                     // table of a varying slot
+  Real cm[kNumSlots][kKronMaxN * kKronMaxN]; // matrix of a constant slot (kernel-parameter space)
+  const Real* phi[3];            // phi[a][e_a * 2 + s]
+  const signed char* sgn[3][3];  // sgn[a][k][e_k] in {-1, 0, 1} (k != a)
+  const Real* elem[3];           // per-element beta_a factor or nullptr
+  const Real* elem_mass;         // per-element sigma factor or nullptr
+};
+
+struct KronPlanHost {
+  bool ok = false;
+  const char* why = "";
+  int N = 0;
+  std::vector<double> mats;               // all matrices, row-major N x N each
+  std::vector<double> phi[3];             // per axis, e * 2 + s
+  std::vector<signed char> sgn[3][3];
+  KronMat D[3], Dt[3], T[3][3], MD, MT[3];
+  int has_adv = 0, has_mass = 0, mass_merged = 0;
+};
+
+// Host-side description of one scalar coefficient: c * prod_k table_k (table_k may be null).
+struct SepCoef {
+  bool separable = false;   // constant, or one product term with no constant
+  double c = 1.0;
+  const double* tab[kMaxDim] = {};  // host tables, n_k * (q + 2)
+  bool has_elem = false;
+};
+
+}  // namespace dgop

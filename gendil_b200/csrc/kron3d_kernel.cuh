@@ -1,0 +1,582 @@
+// Register-resident Kronecker-form DG operator kernel for 3D hexahedra, N = p + 1 <= 5.
+//
+// N consecutive lanes own one element; lane t holds an N x N plane of it in registers:
+//   layout Z: plane z = t, values [x][y]      layout Y: plane y = t, values [x][z]
+// Operators along x and y run in layout Z, along x and z in layout Y.  Schedule per element
+// (9 n x n passes, 4 layout exchanges):
+//
+//   Z: px = Dx u + x-faces ; qx = Txy px ; py = Dy u + y-faces             exchange qx, py -> Y
+//   Y: out = Txz qx + Tyx Tyz py ; pz = Dz u + z-faces (mass merged) ; qz = Tzx pz
+//                                                                           exchange qz, out -> Z
+//   Z: out += Tzy qz ; y = alpha out + beta y
+//
+// The upwind neighbour trace of every inflow face is added to the face slice of the D-pass
+// output, so the tangential passes that follow apply the face's tangential operator to it.
+//
+// Memory: each warp loops over groups of 32/N consecutive elements (persistent grid).  The
+// group's DoFs, the neighbour traces its inflow faces need and a per-element record of its face
+// decisions are staged into padded shared memory one group ahead (double buffered, coalesced
+// cp.async copies), so loads of the next group overlap the arithmetic of this one; results leave
+// through the same buffer with coalesced stores.  Constant 1D matrices are read from
+// kernel-parameter space, only element-dependent ones from global memory.  For even N the layout
+// exchanges are register butterflies (shfl_xor within the element's lanes); odd N exchange
+// through a shared tile.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dgop_params.h"
+#include "kron.h"
+
+namespace dgop {
+
+template <int N, typename Real>
+struct Kron3DShape {
+  static constexpr int EPW = 32 / N;  // elements per warp group
+  static constexpr int NN = N * N, NNN = N * N * N;
+  // staging copy granule (bytes): 16 when a plane is a whole number of 16-byte chunks
+  static constexpr int CB = (NN * (int)sizeof(Real)) % 16 == 0 ? 16 : ((NN * (int)sizeof(Real)) % 8 == 0 ? 8 : 4);
+  static constexpr int CR = CB / (int)sizeof(Real);  // Reals per chunk
+  static constexpr int pad_for(int p) { return ((NN + p) * (int)sizeof(Real)) % CB == 0 ? p : pad_for(p + 1); }
+  static constexpr int SP = NN + pad_for(1);  // staged plane stride (Reals)
+  static constexpr int SE = N * SP;           // staged element stride
+  // neighbour traces: one slot per axis (N rows of N), used by the first face of that axis that
+  // needs a neighbour trace; a second one on the same axis (rare) is read from global memory
+  static constexpr int RB = (N * (int)sizeof(Real)) % 16 == 0 ? 16 : ((N * (int)sizeof(Real)) % 8 == 0 ? 8 : 4);
+  static constexpr int TR = N;                // trace row stride
+  static constexpr int TS = N * TR;           // trace slot stride
+  static constexpr int TE = 3 * TS;           // traces per element
+  // face record per element: 12 coefficients (axis, side, {corner, neighbour/inflow}) + flag word
+  static constexpr int RE = 12 + (16 / (int)sizeof(Real));
+  static constexpr int STAGE = EPW * (SE + TE + RE);  // one pipeline stage: DoFs, traces, records
+  static constexpr bool BUTTERFLY = (N == 2 || N == 4);
+  static constexpr int SI = N * (N + 1);      // exchange tile (odd N)
+  static constexpr int TSE = SI * N + 4;
+  static constexpr int TILE = EPW * TSE;
+  __host__ __device__ static constexpr int tidx(int i, int j, int k) { return k + (N + 1) * j + SI * i; }
+  // shared memory per warp (Reals): 2 pipeline stages + 3 exchange tiles for odd N
+  static constexpr int WARP_SMEM = 2 * STAGE + (BUTTERFLY ? 0 : 3 * TILE);
+};
+
+// Y[i][j] = sum_r A(i, r) X[r][j]      (operator along the first plane index)
+template <int N, typename Real, typename Mat>
+__device__ __forceinline__ void apply_first(const Mat& A, const Real (&X)[N][N], Real (&Y)[N][N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      Real s = A(i, 0) * X[0][j];
+#pragma unroll
+      for (int r = 1; r < N; ++r) s += A(i, r) * X[r][j];
+      Y[i][j] = s;
+    }
+}
+
+// Y[i][j] = sum_r A(j, r) X[i][r]      (operator along the second plane index)
+template <int N, typename Real, typename Mat>
+__device__ __forceinline__ void apply_second(const Mat& A, const Real (&X)[N][N], Real (&Y)[N][N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      Real s = A(j, 0) * X[i][0];
+#pragma unroll
+      for (int r = 1; r < N; ++r) s += A(j, r) * X[i][r];
+      Y[i][j] = s;
+    }
+}
+
+template <int N, typename Real>
+struct RegMat {
+  Real a[N][N];
+  __device__ __forceinline__ Real operator()(int i, int j) const { return a[i][j]; }
+};
+
+template <int N, typename Real, int SLOT>
+struct ParamMat {
+  const KronParams<Real>& P;
+  __device__ __forceinline__ Real operator()(int i, int j) const { return P.cm[SLOT][i * N + j]; }
+};
+
+// Apply slot SLOT's matrix (for element coordinate `coord` along its axis) along the first or
+// second plane index: constant matrices come from kernel-parameter space.
+template <int N, typename Real, int SLOT, bool FIRST>
+__device__ __forceinline__ void kron_apply(const KronParams<Real>& P, uint32_t coord, const Real (&X)[N][N],
+                                           Real (&Y)[N][N]) {
+  if (P.vary[SLOT]) {
+    RegMat<N, Real> A;
+    const Real* p = P.mats + P.vm[SLOT].off + (int64_t)coord * P.vm[SLOT].stride;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) A.a[i][j] = __ldg(p + i * N + j);
+    if (FIRST) apply_first<N>(A, X, Y);
+    else apply_second<N>(A, X, Y);
+  } else {
+    ParamMat<N, Real, SLOT> A{P};
+    if (FIRST) apply_first<N>(A, X, Y);
+    else apply_second<N>(A, X, Y);
+  }
+}
+
+// Layout exchange between the N lanes of an element: X[i][j] held by lane t (plane index t of
+// the third axis) becomes Y[i][k] = X_k[i][t].  Even N: shfl_xor butterflies on the lane bits;
+// at the stage on bit b each lane keeps the column of each pair (j, j|m) whose bit b matches its
+// own and trades the other with lane t ^ m.
+template <int N, typename Real>
+__device__ __forceinline__ void exchange_butterfly(int t, Real (&X)[N][N]) {
+#pragma unroll
+  for (int b = 0; (1 << b) < N; ++b) {
+    const int m = 1 << b;
+    const bool hi = (t & m) != 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        if (j & m) continue;
+        const Real send = hi ? X[i][j] : X[i][j | m];
+        const Real recv = __shfl_xor_sync(0xffffffffu, send, m);
+        if (hi) X[i][j] = recv;
+        else X[i][j | m] = recv;
+      }
+  }
+}
+
+template <int N, typename Real>
+__device__ __forceinline__ void tile_put(Real* tile, int le, int t, bool from_z, const Real (&X)[N][N]) {
+  using S = Kron3DShape<N, Real>;
+  Real* b = tile + le * S::TSE;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) b[from_z ? S::tidx(i, j, t) : S::tidx(i, t, j)] = X[i][j];
+}
+
+template <int N, typename Real>
+__device__ __forceinline__ void tile_get(const Real* tile, int le, int t, bool to_z, Real (&X)[N][N]) {
+  using S = Kron3DShape<N, Real>;
+  const Real* b = tile + le * S::TSE;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) X[i][j] = b[to_z ? S::tidx(i, j, t) : S::tidx(i, t, j)];
+}
+
+template <int N, typename Real>
+__device__ __forceinline__ void exchange(int le, int t, bool slot, Real* tile, bool z_to_y, Real (&X)[N][N]) {
+  if constexpr (Kron3DShape<N, Real>::BUTTERFLY) {
+    exchange_butterfly<N>(t, X);
+  } else {
+    if (slot) tile_put<N>(tile, le, t, z_to_y, X);
+    __syncwarp();
+    if (slot) tile_get<N>(tile, le, t, !z_to_y, X);
+  }
+}
+
+// Element coordinates (x fastest).
+template <typename Real>
+__device__ __forceinline__ void kron_coords(const KronParams<Real>& P, uint32_t e, uint32_t (&c)[3]) {
+  uint32_t q;
+  P.fdx.divmod(e, q, c[0]);
+  P.fdy.divmod(q, c[2], c[1]);
+}
+
+// Upwind decision for face (a, s) of element e (cartesianndmesh.hpp:109-198 for the neighbour,
+// advectionoperator.hpp:379-386 / 422-428 for the flux):
+//   corner: add phi * el * u[slice]              (outflow face, own trace)
+//   use_nb: add coef * neighbour trace            (inflow face, or the transposed coupling)
+//   use_g:  add coef * g                          (inflow boundary face with inflow value g)
+struct FaceDecision {
+  bool corner, use_nb, use_g;
+  int64_t d;  // neighbour offset
+};
+
+template <typename Real>
+__device__ __forceinline__ FaceDecision face_decide(const KronParams<Real>& P, int a, int s, const uint32_t (&c)[3],
+                                                    int64_t e, Real tsign, Real el_self, Real& phi, Real& coef) {
+  FaceDecision f{false, false, false, 0};
+  const int64_t n = P.sizes[a];
+  const int64_t st = a == 0 ? 1 : (a == 1 ? P.sizes[0] : P.sizes[0] * P.sizes[1]);
+  bool interior;
+  if (s == 0) {
+    interior = c[a] > 0 || P.periodic[a];
+    f.d = c[a] > 0 ? -st : (n - 1) * st;
+  } else {
+    interior = (int64_t)c[a] + 1 < n || P.periodic[a];
+    f.d = (int64_t)c[a] + 1 < n ? st : -(n - 1) * st;
+  }
+  const bool active = interior ? (P.flags & kFaceInt) : (P.flags & kFaceBnd);
+  phi = P.phi[a][c[a] * 2 + s];
+  coef = Real(0);
+  if (!active) return f;
+  const bool outflow = phi * tsign * el_self > Real(0);
+  f.corner = outflow;
+  if (!(P.flags & kTranspose)) {
+    if (!outflow) {
+      coef = phi * el_self;
+      f.use_nb = interior;
+      f.use_g = !interior;
+    }
+  } else if (interior) {
+    // transposed coupling: the neighbour's row, taken when its face (1-s) is inflow for it
+    const uint32_t cn = s ? ((int64_t)c[a] + 1 == n ? 0 : c[a] + 1) : (c[a] == 0 ? (uint32_t)(n - 1) : c[a] - 1);
+    const Real phin = P.phi[a][cn * 2 + (1 - s)];
+    const Real eln = P.elem[a] ? P.elem[a][e + f.d] : Real(1);
+    if (!(phin * tsign * eln > Real(0))) {
+      coef = phin * eln;
+      f.use_nb = true;
+    }
+  }
+  return f;
+}
+
+template <typename Real>
+__device__ __forceinline__ Real tan_sign(const KronParams<Real>& P, int a, const uint32_t (&c)[3]) {
+  Real s = Real(1);
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (k != a) s *= (Real)P.sgn[a][k][c[k]];
+  return s;
+}
+
+// Is the x neighbour on side s the adjacent element of the same staged group?
+__device__ __forceinline__ bool x_in_group(int s, int le, int ne, uint32_t cx, int64_t nx) {
+  const int rl = le + (s ? 1 : -1);
+  return rl >= 0 && rl < ne && (s ? (int64_t)cx + 1 < nx : cx > 0);
+}
+
+enum TraceSrc { kTraceLocal = 0, kTraceSlot = 1, kTraceGlobal = 2 };
+// Face record bits (5 per face f = axis * 2 + side): corner, neighbour trace, inflow value g,
+// and the trace source (TraceSrc) in bits 3-4.
+enum : uint32_t { kRecCorner = 1u, kRecNb = 2u, kRecG = 4u };
+
+template <typename Real>
+__device__ __forceinline__ int64_t neighbour_offset(const KronParams<Real>& P, int a, int s, uint32_t ca) {
+  const int64_t n = P.sizes[a];
+  const int64_t st = a == 0 ? 1 : (a == 1 ? P.sizes[0] : P.sizes[0] * P.sizes[1]);
+  if (s == 0) return ca > 0 ? -st : (n - 1) * st;
+  return (int64_t)ca + 1 < n ? st : -(n - 1) * st;
+}
+
+// Face terms of axis a added to a D-pass output Pm (plane [first][second]; the face slice is along
+// the first index when FIRST), from the element's face record (see stage_group).  nbval(side, r,
+// src, e_nb) reads the neighbour trace of that side from the group's staged DoFs (x only), the
+// axis' staged trace slot, or global memory.
+template <int N, typename Real, bool FIRST, typename NbVal>
+__device__ __forceinline__ void kron_faces(const KronParams<Real>& P, int a, const uint32_t (&c)[3], int64_t e,
+                                           uint32_t flags, const Real* rec, const Real (&U)[N][N], Real (&Pm)[N][N],
+                                           NbVal nbval) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int sl = s ? N - 1 : 0;
+    const uint32_t f = (flags >> (5 * (a * 2 + s))) & 31u;
+    if (f & kRecCorner) {
+      const Real k = rec[(a * 2 + s) * 2];
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        if (FIRST) Pm[sl][r] += k * U[sl][r];
+        else Pm[r][sl] += k * U[r][sl];
+      }
+    }
+    if (f & (kRecNb | kRecG)) {
+      const Real k = rec[(a * 2 + s) * 2 + 1];
+      if (f & kRecNb) {
+        const int src = (int)(f >> 3);
+        const int64_t en = src == kTraceGlobal ? e + neighbour_offset(P, a, s, c[a]) : e;
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          const Real v = nbval(s, r, src, en);
+          if (FIRST) Pm[sl][r] += k * v;
+          else Pm[r][sl] += k * v;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          if (FIRST) Pm[sl][r] += k * P.g;
+          else Pm[r][sl] += k * P.g;
+        }
+      }
+    }
+  }
+}
+
+template <int CB>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if constexpr (CB == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(CB));
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K)); }
+
+__device__ __forceinline__ int group_size(int epw, int64_t remaining) {
+  return remaining < epw ? (int)remaining : epw;
+}
+
+// Copy N contiguous Reals (a trace row) from global to shared memory.
+template <int N, typename Real>
+__device__ __forceinline__ void copy_row(Real* dst, const Real* src) {
+  using S = Kron3DShape<N, Real>;
+  constexpr int R = S::RB / (int)sizeof(Real);
+#pragma unroll
+  for (int i = 0; i < N; i += R) cp_async<S::RB>(dst + i, src + i);
+}
+
+// Stage the DoFs of elements [e0, e0 + ne) into `buf` (padded layout, coalesced); for advection,
+// also each element's face record and the neighbour traces its faces will read (lane t copies
+// row t of each trace).
+template <int N, typename Real>
+__device__ __forceinline__ void stage_group(const KronParams<Real>& P, int64_t e0, int ne, Real* buf, int lane,
+                                            int le, int t, bool adv) {
+  using S = Kron3DShape<N, Real>;
+  const int nchunks = ne * S::NNN / S::CR;
+  const Real* src = P.x + e0 * S::NNN;
+  for (int ch = lane; ch < nchunks; ch += 32) {
+    const int d = ch * S::CR;
+    const int r = d / S::NNN, o = d - r * S::NNN;
+    const int z = o / S::NN, w = o - z * S::NN;
+    cp_async<S::CB>(buf + r * S::SE + z * S::SP + w, src + d);
+  }
+  if (!adv || le >= ne) return;
+  const int64_t e = e0 + le;
+  uint32_t c[3];
+  kron_coords(P, (uint32_t)e, c);
+  Real* tb = buf + S::EPW * S::SE + le * S::TE;
+  Real* rb = buf + S::EPW * (S::SE + S::TE) + le * S::RE;
+  uint32_t flags = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const Real tsign = tan_sign(P, a, c);
+    const Real el = P.elem[a] ? P.elem[a][e] : Real(1);
+    bool slot_taken = false;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      Real phi, coef;
+      const FaceDecision f = face_decide(P, a, s, c, e, tsign, el, phi, coef);
+      uint32_t bits = 0;
+      if (f.corner) bits |= kRecCorner;
+      if (f.use_g) bits |= kRecG;
+      int src = kTraceLocal;
+      if (f.use_nb) {
+        bits |= kRecNb;
+        if (!(a == 0 && x_in_group(s, le, ne, c[0], P.sizes[0]))) src = slot_taken ? kTraceGlobal : kTraceSlot;
+      }
+      bits |= (uint32_t)src << 3;
+      flags |= bits << (5 * (a * 2 + s));
+      if (t == 0) {
+        rb[(a * 2 + s) * 2] = phi * el;
+        rb[(a * 2 + s) * 2 + 1] = coef;
+      }
+      if (src != kTraceSlot) continue;  // staged DoFs (x neighbours in the group) or global memory
+      slot_taken = true;
+      const Real* un = P.x + (e + f.d) * S::NNN;
+      const int sl = s ? 0 : N - 1;  // the neighbour's opposite slice
+      Real* dst = tb + a * S::TS + t * S::TR;
+      if (a == 0) {
+#pragma unroll
+        for (int r = 0; r < N; ++r) cp_async<(int)sizeof(Real)>(dst + r, un + sl + N * r + S::NN * t);
+      } else if (a == 1) {
+        copy_row<N>(dst, un + N * sl + S::NN * t);
+      } else {
+        copy_row<N>(dst, un + N * t + S::NN * sl);
+      }
+    }
+  }
+  if (t == 0) *reinterpret_cast<uint32_t*>(rb + 12) = flags;
+}
+
+template <int N, typename Real, bool SEP>
+__global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ KronParams<Real> P) {
+  using S = Kron3DShape<N, Real>;
+  constexpr int NN = S::NN, NNN = S::NNN, EPW = S::EPW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int le = lane / N, t = lane - le * N;
+  Real* wbase = reinterpret_cast<Real*>(smem_raw) + (size_t)warp * S::WARP_SMEM;
+  Real* tiles = wbase + 2 * S::STAGE;  // odd N only
+  const int64_t ngroups = (P.nelem + EPW - 1) / EPW;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const bool adv = P.has_adv != 0;
+  const bool slot = le < EPW;
+
+  int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  if (g < ngroups) stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), wbase, lane, le, t, adv);
+  cp_async_commit();
+  for (int it = 0; g < ngroups; g += nwarps, ++it) {
+    Real* buf = wbase + (it & 1) * S::STAGE;
+    {
+      const int64_t gn = g + nwarps;
+      if (gn < ngroups)
+        stage_group<N>(P, gn * EPW, group_size(EPW, P.nelem - gn * EPW), wbase + ((it + 1) & 1) * S::STAGE, lane, le,
+                       t, adv);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncwarp();
+    }
+    const int64_t e0 = g * EPW;
+    const int ne = group_size(EPW, P.nelem - e0);
+    const int64_t e = e0 + le;
+    const bool active = slot && le < ne;
+    uint32_t c[3] = {0, 0, 0};
+    if (active) kron_coords(P, (uint32_t)e, c);
+    const Real* ub = buf + (slot ? le : 0) * S::SE;
+    const Real* tb = buf + EPW * S::SE + (slot ? le : 0) * S::TE;
+    const Real* rec = buf + EPW * (S::SE + S::TE) + (slot ? le : 0) * S::RE;
+    const uint32_t fflags = (adv && active) ? *reinterpret_cast<const uint32_t*>(rec + 12) : 0u;
+    Real qx[N][N], py[N][N];
+
+    // ------------------------------------------------------------ layout Z (plane z = t)
+    if (adv) {
+      Real u[N][N];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) u[i][j] = active ? ub[t * S::SP + i + N * j] : Real(0);
+      {
+        Real px[N][N];
+        kron_apply<N, Real, kSlotDX, true>(P, c[0], u, px);
+        if (P.elem[0]) {
+          const Real elx = active ? P.elem[0][e] : Real(1);
+#pragma unroll
+          for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int j = 0; j < N; ++j) px[i][j] *= elx;
+        }
+        if (active)
+          kron_faces<N, Real, true>(P, 0, c, e, fflags, rec, u, px, [&](int s, int r, int src, int64_t en) {
+            const int sl = s ? 0 : N - 1;  // the neighbour's opposite slice
+            if (src == kTraceLocal) return ub[(s ? 1 : -1) * S::SE + t * S::SP + sl + N * r];
+            if (src == kTraceSlot) return tb[0 * S::TS + t * S::TR + r];
+            return P.x[en * NNN + sl + N * r + NN * t];
+          });
+        kron_apply<N, Real, kSlotTXY, false>(P, c[1], px, qx);
+      }
+      kron_apply<N, Real, kSlotDY, false>(P, c[1], u, py);
+      if (P.elem[1]) {
+        const Real ely = active ? P.elem[1][e] : Real(1);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int j = 0; j < N; ++j) py[i][j] *= ely;
+      }
+      if (active)
+        kron_faces<N, Real, false>(P, 1, c, e, fflags, rec, u, py, [&](int s, int r, int src, int64_t en) {
+          if (src == kTraceSlot) return tb[1 * S::TS + t * S::TR + r];
+          return P.x[en * NNN + r + N * (s ? 0 : N - 1) + NN * t];
+        });
+      exchange<N>(le, t, slot, tiles, true, qx);
+      exchange<N>(le, t, slot, tiles + S::TILE, true, py);
+    }
+
+    // ------------------------------------------------------------ layout Y (plane y = t)
+    Real out[N][N], qz[N][N];
+    [[maybe_unused]] Real qm[N][N];
+    {
+      // x and y terms first, so their inputs die before u is loaded
+      if (adv) {
+        kron_apply<N, Real, kSlotTXZ, false>(P, c[2], qx, out);
+        kron_apply<N, Real, kSlotTYZ, false>(P, c[2], py, qx);  // qx reused as scratch
+        kron_apply<N, Real, kSlotTYX, true>(P, c[0], qx, py);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int k = 0; k < N; ++k) out[i][k] += py[i][k];
+      } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int k = 0; k < N; ++k) out[i][k] = Real(0);
+      }
+      Real u[N][N], pz[N][N];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int k = 0; k < N; ++k) u[i][k] = active ? ub[k * S::SP + i + N * t] : Real(0);
+      kron_apply<N, Real, kSlotDZ, false>(P, c[2], u, pz);
+      if (adv) {
+        if (P.elem[2]) {
+          const Real elz = active ? P.elem[2][e] : Real(1);
+#pragma unroll
+          for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int k = 0; k < N; ++k) pz[i][k] *= elz;
+        }
+        if (active)
+          kron_faces<N, Real, false>(P, 2, c, e, fflags, rec, u, pz, [&](int s, int r, int src, int64_t en) {
+            if (src == kTraceSlot) return tb[2 * S::TS + t * S::TR + r];
+            return P.x[en * NNN + r + N * t + NN * (s ? 0 : N - 1)];
+          });
+      } else if (P.elem_mass) {
+        const Real em = active ? P.elem_mass[e] : Real(1);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int k = 0; k < N; ++k) pz[i][k] *= em;
+      }
+      kron_apply<N, Real, kSlotTZX, true>(P, c[0], pz, qz);
+      if constexpr (SEP) {
+        kron_apply<N, Real, kSlotMD, false>(P, c[2], u, pz);
+        if (P.elem_mass) {
+          const Real em = active ? P.elem_mass[e] : Real(1);
+#pragma unroll
+          for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int k = 0; k < N; ++k) pz[i][k] *= em;
+        }
+        kron_apply<N, Real, kSlotMX, true>(P, c[0], pz, qm);
+      }
+    }
+    if constexpr (!S::BUTTERFLY) __syncwarp();  // the tiles are reused
+    exchange<N>(le, t, slot, tiles, false, qz);
+    exchange<N>(le, t, slot, tiles + S::TILE, false, out);
+    if constexpr (SEP) exchange<N>(le, t, slot, tiles + 2 * S::TILE, false, qm);
+
+    // ------------------------------------------------------------ layout Z, output
+    kron_apply<N, Real, kSlotTZY, false>(P, c[1], qz, py);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) out[i][j] += py[i][j];
+    if constexpr (SEP) {
+      kron_apply<N, Real, kSlotMY, false>(P, c[1], qm, py);
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) out[i][j] += py[i][j];
+    }
+    __syncwarp();  // every lane is done reading the staged input of this group
+    if (slot) {
+      Real* ob = buf + le * S::SE + t * S::SP;
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) ob[i + N * j] = out[i][j];
+    }
+    __syncwarp();
+    {
+      // coalesced store, in the staging granule
+      const int nchunks = ne * NNN / S::CR;
+      Real* dst = P.y + e0 * NNN;
+      const Real alpha = P.alpha, by = P.beta_y;
+      for (int ch = lane; ch < nchunks; ch += 32) {
+        const int d = ch * S::CR;
+        const int r = d / NNN, o = d - r * NNN;
+        const int z = o / NN, w = o - z * NN;
+        const Real* sp = buf + r * S::SE + z * S::SP + w;
+#pragma unroll
+        for (int q = 0; q < S::CR; ++q) {
+          const Real v = sp[q];
+          dst[d + q] = (by == Real(0)) ? alpha * v : alpha * v + by * dst[d + q];
+        }
+      }
+    }
+    __syncwarp();  // the buffer is refilled by the prefetch of the next-but-one group
+  }
+  cp_async_wait<0>();
+}
+
+}  // namespace dgop

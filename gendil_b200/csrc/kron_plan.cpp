@@ -1,0 +1,165 @@
+// Host planner for the Kronecker form (see kron.h): eligibility and per-axis matrix tables.
+#include "kron_plan.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace dgop {
+
+namespace {
+
+// f(e, point j): table value or 1.
+inline double fval(const double* tab, int ld, int64_t e, int j) { return tab ? tab[e * ld + j] : 1.0; }
+
+// Append one N x N mass-type matrix per element coordinate (a single one when tab == nullptr).
+KronMat add_mass(std::vector<double>& mats, const KronInputs& in, int axis, const double* tab, double scale) {
+  const int N = in.N, Q = in.Q, ld = Q + 2;
+  const int64_t count = tab ? in.sizes[axis] : 1;
+  KronMat m;
+  m.off = (int64_t)mats.size();
+  m.stride = tab ? N * N : 0;
+  for (int64_t e = 0; e < count; ++e)
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double s = 0.0;
+        for (int q = 0; q < Q; ++q) s += in.B[q * N + i] * (in.wq[q] * fval(tab, ld, e, q)) * in.B[q * N + j];
+        mats.push_back(scale * s);
+      }
+  return m;
+}
+
+// G[j][m] = sum_p (sum_q B[q][j] Dq[p][q]) w_p f_p B[p][m], scaled; optionally plus a scaled
+// mass-type matrix (the merged mass term), optionally transposed.
+KronMat add_grad(std::vector<double>& mats, const KronInputs& in, int axis, const double* tab, double scale,
+                 bool transpose, const double* mtab, double mscale, bool with_mass) {
+  const int N = in.N, Q = in.Q, ld = Q + 2;
+  const bool varies = tab || (with_mass && mtab);
+  const int64_t count = varies ? in.sizes[axis] : 1;
+  KronMat m;
+  m.off = (int64_t)mats.size();
+  m.stride = varies ? N * N : 0;
+  for (int64_t e = 0; e < count; ++e) {
+    double G[kKronMaxN][kKronMaxN];
+    for (int j = 0; j < N; ++j)
+      for (int c = 0; c < N; ++c) {
+        double s = 0.0;
+        for (int p = 0; p < Q; ++p) {
+          double bd = 0.0;
+          for (int q = 0; q < Q; ++q) bd += in.B[q * N + j] * in.Dq[p * Q + q];
+          s += bd * (in.wq[p] * fval(tab, ld, e, p)) * in.B[p * N + c];
+        }
+        G[j][c] = scale * s;
+        if (with_mass) {
+          double ms = 0.0;
+          for (int q = 0; q < Q; ++q) ms += in.B[q * N + j] * (in.wq[q] * fval(mtab, ld, e, q)) * in.B[q * N + c];
+          G[j][c] += mscale * ms;
+        }
+      }
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) mats.push_back(transpose ? G[j][i] : G[i][j]);
+  }
+  return m;
+}
+
+// Sign of f over each element's Gauss points: +1 / -1 / 0 (all zero); false if mixed.
+bool sign_table(const KronInputs& in, int axis, const double* tab, std::vector<signed char>& out) {
+  const int Q = in.Q, ld = Q + 2;
+  out.assign(in.sizes[axis], 1);
+  if (!tab) return true;
+  for (int64_t e = 0; e < in.sizes[axis]; ++e) {
+    bool pos = false, neg = false;
+    for (int q = 0; q < Q; ++q) {
+      const double v = tab[e * ld + q];
+      if (!std::isfinite(v)) return false;
+      if (v > 0) pos = true;
+      if (v < 0) neg = true;
+    }
+    if (pos && neg) return false;
+    out[e] = pos ? 1 : (neg ? -1 : 0);
+  }
+  return true;
+}
+
+}  // namespace
+
+KronPlanHost plan_kron3d(const KronInputs& in) {
+  KronPlanHost p;
+  p.N = in.N;
+  if (in.D != 3) {
+    p.why = "dimension != 3";
+    return p;
+  }
+  if (!in.gll) {
+    p.why = "basis is not GLL";
+    return p;
+  }
+  if (in.N > 4) {  // the FP64 register kernel spills above N = 4
+    p.why = "order above 3 (register kernel limit)";
+    return p;
+  }
+  if ((uint64_t)in.sizes[0] * in.sizes[1] * in.sizes[2] >= (uint64_t(1) << 32)) {
+    p.why = "more than 2^32 elements";
+    return p;
+  }
+  const bool adv = (in.flags & kAdvCell) != 0;
+  const bool mass = (in.flags & kMass) != 0;
+  if (!adv && !mass) {
+    p.why = "empty operator";
+    return p;
+  }
+  if (adv)
+    for (int a = 0; a < 3; ++a)
+      if (!in.beta[a].separable) {
+        p.why = "velocity component is not a single separable product";
+        return p;
+      }
+  if (mass && !in.sigma.separable) {
+    p.why = "density is not a single separable product";
+    return p;
+  }
+  double detJ = 1.0;
+  for (int k = 0; k < 3; ++k) detJ *= in.h[k];
+  p.has_adv = adv;
+  p.has_mass = mass;
+  auto& M = p.mats;
+  if (adv) {
+    const SepCoef& bz = in.beta[2];
+    p.mass_merged = mass && !in.sigma.has_elem && !bz.has_elem && in.sigma.tab[0] == bz.tab[0] &&
+                    in.sigma.tab[1] == bz.tab[1];
+    for (int a = 0; a < 3; ++a) {
+      const SepCoef& b = in.beta[a];
+      const double invh = 1.0 / in.h[a];
+      const double s_a = -b.c * detJ * invh;
+      const bool merge = p.mass_merged && a == 2;
+      const double s_m = in.sigma.c * detJ;
+      p.D[a] = add_grad(M, in, a, b.tab[a], s_a, false, in.sigma.tab[2], s_m, merge);
+      p.Dt[a] = add_grad(M, in, a, b.tab[a], s_a, true, in.sigma.tab[2], s_m, merge);
+      for (int k = 0; k < 3; ++k) {
+        if (k == a) continue;
+        p.T[a][k] = add_mass(M, in, k, b.tab[k], 1.0);
+        if (!sign_table(in, k, b.tab[k], p.sgn[a][k])) {
+          p.why = "upwind direction changes sign inside an element face";
+          return p;
+        }
+      }
+      // phi_s(e_a) = detJ c_a f_aa(face s) (+-1/h_a); face s = 0 at xhat = 0 (index Q), 1 at xhat = 1
+      const int ld = in.Q + 2;
+      p.phi[a].resize(2 * in.sizes[a]);
+      for (int64_t e = 0; e < in.sizes[a]; ++e)
+        for (int s = 0; s < 2; ++s) {
+          const double f = b.tab[a] ? b.tab[a][e * ld + in.Q + s] : 1.0;
+          p.phi[a][2 * e + s] = detJ * b.c * f * (s ? invh : -invh);
+        }
+    }
+  }
+  if (mass && !p.mass_merged) {
+    const double s_m = in.sigma.c * detJ;
+    p.MD = add_mass(M, in, 2, in.sigma.tab[2], s_m);
+    p.MT[0] = add_mass(M, in, 0, in.sigma.tab[0], 1.0);
+    p.MT[1] = add_mass(M, in, 1, in.sigma.tab[1], 1.0);
+  }
+  p.ok = true;
+  return p;
+}
+
+}  // namespace dgop

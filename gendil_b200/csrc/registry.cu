@@ -1,6 +1,7 @@
 // Kernel registry storage and the one-time registration of all instantiation units.
 #include <mutex>
 
+#include "kron_registry.h"
 #include "registry.h"
 
 namespace dgop {
@@ -9,7 +10,12 @@ namespace {
 GenericEntry<double> g_f64[kMaxDim][kMaxN][kMaxQ];
 GenericEntry<float> g_f32[kMaxDim][kMaxN][kMaxQ];
 std::once_flag g_once;
+KronEntry<double> g_k64[kKronMaxN + 1];
+KronEntry<float> g_k32[kKronMaxN + 1];
 }  // namespace
+
+KronEntry<double>& kron3d_slot_f64(int N) { return g_k64[N]; }
+KronEntry<float>& kron3d_slot_f32(int N) { return g_k32[N]; }
 
 GenericEntry<double>& generic_slot_f64(int D, int N, int Q) { return g_f64[D - 1][N - 1][Q - 1]; }
 GenericEntry<float>& generic_slot_f32(int D, int N, int Q) { return g_f32[D - 1][N - 1][Q - 1]; }
@@ -29,6 +35,7 @@ void ensure_registry() {
   DGOP_CALL_N(D, 1) DGOP_CALL_N(D, 2) DGOP_CALL_N(D, 3) DGOP_CALL_N(D, 4) \
   DGOP_CALL_N(D, 5) DGOP_CALL_N(D, 6) DGOP_CALL_N(D, 7) DGOP_CALL_N(D, 8)
     DGOP_CALL_D(1) DGOP_CALL_D(2) DGOP_CALL_D(3) DGOP_CALL_D(4) DGOP_CALL_D(5) DGOP_CALL_D(6)
+    register_kron3d();
 #undef DGOP_CALL_D
 #undef DGOP_CALL_N
   });

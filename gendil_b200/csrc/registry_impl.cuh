@@ -14,6 +14,7 @@ constexpr bool generic_enabled(int D, int N, int Q) {
   constexpr int list[][3] = {
       {1, 1, 1}, {1, 4, 5}, {1, 8, 8}, {1, 3, 4}, {2, 1, 1}, {2, 3, 4}, {2, 5, 3}, {2, 3, 3}, {2, 2, 2},
       {3, 2, 4}, {3, 4, 4}, {3, 4, 6}, {3, 3, 2}, {3, 8, 8}, {3, 1, 2}, {3, 2, 3}, {3, 6, 6}, {3, 3, 3},
+      {3, 2, 2}, {3, 5, 5}, {3, 4, 3},
       {4, 3, 3}, {4, 2, 2}, {5, 2, 2}, {6, 2, 2}, {6, 3, 3}};
   for (const auto& c : list)
     if (c[0] == D && c[1] == N && c[2] == Q) return true;

@@ -78,6 +78,16 @@ int dgop_system_create(const dgop_space* space, int q, const dgop_coef* sigma, c
 int dgop_operator_destroy(dgop_operator* op);
 int64_t dgop_operator_num_dofs(const dgop_operator* op);
 
+/* Kernel family used by an operator (no reference counterpart; diagnostics and testing):
+ * DGOP_KERNEL_GENERIC is the sum-factorized kernel that follows the reference's element
+ * algorithm for every shape; DGOP_KERNEL_KRON is the register-resident Kronecker-form kernel
+ * (3D, GLL, orders 0..3, separable coefficients), chosen automatically when eligible.
+ * dgop_operator_kernel_note() says why the Kronecker form was not chosen. */
+enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1 };
+int dgop_operator_kernel(const dgop_operator* op);
+const char* dgop_operator_kernel_note(const dgop_operator* op);
+int dgop_operator_select_kernel(dgop_operator* op, int kernel);
+
 /* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers.
  * (MassFiniteElementOperator::operator() massoperator.hpp:209, AdvectionOperator::operator()
  * advectionoperator.hpp:1070: both overwrite y.) */

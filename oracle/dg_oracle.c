@@ -340,6 +340,7 @@ static void apply_test_add(const space_t *s, int fa, int fend, const double *in,
 static double sigma_eval(int D, int kind, double c, const double *X)
 {
    if (kind == DGO_SIGMA_CONST) return c;
+   if (kind == DGO_SIGMA_SEP) return (1.0 + 0.5 * X[0]) * (1.0 + X[1 % D] * X[1 % D]) * (2.0 - X[2 % D]);
    return 1.0 + X[0] * X[1 % D] + X[D - 1] * X[D - 1];
 }
 

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-enum { DGO_SIGMA_CONST = 0, DGO_SIGMA_POLY = 1 };
+enum { DGO_SIGMA_CONST = 0, DGO_SIGMA_POLY = 1, DGO_SIGMA_SEP = 2 };
 enum { DGO_BETA_CONST = 0, DGO_BETA_BUBBLE = 1, DGO_BETA_SINCOS = 2, DGO_BETA_PHASE = 3 };
 enum { DGO_ADV_NO_BC = 0, DGO_ADV_INFLOW = 1, DGO_MASS_ADV = 2 };
 

@@ -28,7 +28,7 @@ enum { GREF_UNSUPPORTED = -1 };
 
 // Coefficient presets.  The same formulas are tabulated for the B200 library by the tests, so
 // the reference evaluates them pointwise exactly as a GenDiL user lambda would.
-enum SigmaKind { SIGMA_CONST = 0, SIGMA_POLY = 1 };
+enum SigmaKind { SIGMA_CONST = 0, SIGMA_POLY = 1, SIGMA_SEP = 2 };
 enum BetaKind { BETA_CONST = 0, BETA_BUBBLE = 1, BETA_SINCOS = 2, BETA_PHASE = 3 };
 
 template < int D >
@@ -39,6 +39,7 @@ struct SigmaFn
    GENDIL_HOST_DEVICE Real operator()( const std::array< Real, D > & X ) const
    {
       if ( kind == SIGMA_CONST ) return c;
+      if ( kind == SIGMA_SEP ) return ( 1.0 + 0.5 * X[ 0 ] ) * ( 1.0 + X[ 1 % D ] * X[ 1 % D ] ) * ( 2.0 - X[ 2 % D ] );
       // test-mass-3d-generic.cpp:114-120 uses 1 + x*y + z*z in 3D.
       return 1.0 + X[ 0 ] * X[ 1 % D ] + X[ D - 1 ] * X[ D - 1 ];
    }

@@ -6,7 +6,7 @@
 #define GREF_MASS_LIST_A(X) \
    X(1,0,1,0) X(1,3,5,0) X(1,7,8,0) X(2,0,1,0) X(2,2,4,0) X(2,4,3,0) X(2,2,3,1)
 #define GREF_MASS_LIST_B(X) \
-   X(3,1,4,0) X(3,3,4,0) X(3,3,6,0) X(3,2,2,1) X(3,7,8,0)
+   X(3,1,4,0) X(3,3,4,0) X(3,3,6,0) X(3,2,2,1) X(3,7,8,0) X(3,1,2,0) X(3,4,5,0)
 #define GREF_MASS_LIST_C(X) \
    X(4,2,3,0) X(5,1,2,0) X(6,1,2,0) X(6,2,3,0)
 
@@ -15,7 +15,7 @@
 #define GREF_ADV_LIST_B(X) \
    X(3,0,2,0) X(3,1,3,0) X(3,3,4,0) X(3,2,2,1)
 #define GREF_ADV_LIST_C(X) \
-   X(3,5,6,0) X(3,7,8,0)
+   X(3,5,6,0) X(3,7,8,0) X(3,2,3,0) X(3,4,5,0) X(3,3,3,0)
 #define GREF_ADV_LIST_D(X) \
    X(4,1,2,0) X(5,1,2,0)
 #define GREF_ADV_LIST_E(X) \

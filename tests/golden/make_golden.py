@@ -51,6 +51,12 @@ def mass_cases():
     c.append(("m14", dict(cube(5, 2, 1, 2), sigma_kind=1)))
     c.append(("m15", dict(cube(6, 2, 1, 2), sigma_kind=1)))
     c.append(("m16", dict(cube(6, 0, 2, 3, sizes=[2, 1, 2, 1, 2, 1]), sigma_kind=1)))
+    # single separable products: these also run on the Kronecker-form kernel
+    c.append(("m17", dict(cube(3, 0, 3, 4, sizes=[4, 3, 5], h=[0.25, 0.5, 0.2], origin=[-0.5, 0.0, 0.25]),
+                          sigma_kind=2)))
+    c.append(("m18", dict(cube(3, 0, 1, 2, sizes=[9, 2, 3]), sigma_kind=2)))
+    c.append(("m19", dict(cube(3, 0, 4, 5, sizes=[3, 2, 2]), sigma_kind=2)))
+    c.append(("m20", dict(cube(3, 0, 3, 4, sizes=[7, 3, 2]), sigma_kind=0, sigma_c=3.5)))
     return c
 
 
@@ -86,6 +92,17 @@ def adv_cases():
     c.append(("a14", dict(cube(6, 0, 2, 3, sizes=[2, 2, 1, 2, 1, 2], h=[0.5, 0.5, 1.0, 1.0, 2.0, 1.0],
                           origin=[0, 0, 0, -1, -1, -1]),
                           beta_kind=3, g=0.0, sigma_kind=0, sigma_c=200.0)))
+    # 3D shapes that also run on the Kronecker-form kernel (separable velocity and density)
+    c.append(("a15", dict(cube(3, 0, 2, 3, sizes=[5, 3, 4], h=[0.2, 1 / 3, 0.25], origin=[0.1, -0.2, 0.0]),
+                          beta_kind=2, g=0.2, sigma_kind=2)))
+    c.append(("a16", dict(cube(3, 0, 3, 4, sizes=[3, 4, 2]), beta_kind=1, g=0.0, sigma_kind=0, sigma_c=50.0)))
+    c.append(("a17", dict(cube(3, 0, 4, 5, sizes=[3, 2, 3]), beta_kind=2, g=0.4, sigma_kind=0, sigma_c=2.0)))
+    c.append(("a18", dict(cube(3, 0, 3, 4, sizes=[6, 5, 3]), beta_kind=0, beta_c=[-0.7, 0.3, -0.4], g=0.3,
+                          sigma_kind=2)))
+    c.append(("a19", dict(cube(3, 0, 3, 3, sizes=[4, 4, 4], periodic=[0, 1, 0]), beta_kind=2, g=0.0, sigma_kind=0,
+                          sigma_c=1.0)))
+    c.append(("a20", dict(cube(3, 0, 3, 4, sizes=[10, 3, 3]), beta_kind=0, beta_c=[0.0, 0.5, -0.25], g=0.1,
+                          sigma_kind=0, sigma_c=1.0)))
     return c
 
 

@@ -1,6 +1,7 @@
 """GPU: the sm_100a operators against the reference's golden outputs and the oracle.
 
-FP64 applies must match to APPLY_TOL = 1e-13 relative in max norm per apply."""
+FP64 applies must match to APPLY_TOL = 1e-13 relative in max norm per apply.  Every case runs on
+the generic sum-factorized kernel and, where eligible, on the Kronecker-form kernel."""
 import numpy as np
 import pytest
 
@@ -8,35 +9,66 @@ from helpers import APPLY_TOL, cuda_apply, golden, inputs, make_operator, oracle
 
 pytestmark = pytest.mark.gpu
 CASES, ARR = golden()
+KERNELS = ["generic", "kron"]
 
 
+def _select(op, kernel):
+    if kernel == "kron" and op.kernel != "kron":
+        pytest.skip(f"not eligible for the Kronecker kernel: {op.kernel_note}")
+    if kernel == "generic" and op.kernel != "generic":
+        import gendil_b200 as g
+        try:
+            op.select_kernel("generic")
+        except g.DGOPError as exc:
+            pytest.skip(f"generic kernel not built for this shape: {exc}")
+    return op
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("case", CASES["mass"], ids=lambda c: c["id"])
-def test_mass_vs_reference_golden(case):
-    op = make_operator(case, "mass")
+def test_mass_vs_reference_golden(case, kernel):
+    op = _select(make_operator(case, "mass"), kernel)
     y = cuda_apply(op, inputs(case))
     assert rel_max(y, ARR[f"{case['id']}_y"]) <= APPLY_TOL
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("case", CASES["advection"], ids=lambda c: c["id"])
-def test_advection_vs_reference_golden(case, mode):
-    op = make_operator(case, "adv", mode)
+def test_advection_vs_reference_golden(case, mode, kernel):
+    op = _select(make_operator(case, "adv", mode), kernel)
     y = cuda_apply(op, inputs(case))
     assert rel_max(y, ARR[f"{case['id']}_mode{mode}_y"]) <= APPLY_TOL
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("case", CASES["advection"], ids=lambda c: c["id"])
-def test_transpose_adjoint_identity(case, mode):
+def test_transpose_adjoint_identity(case, mode, kernel):
     """<A x, z> = <x, A^T z> for the linear part (inflow value 0)."""
     case = dict(case, g=0.0)
-    op = make_operator(case, "adv", mode)
+    op = _select(make_operator(case, "adv", mode), kernel)
     x = inputs(case, seed=5)
     z = inputs(case, seed=6)
     ax = cuda_apply(op, x)
     atz = cuda_apply(op, z, transpose=True)
     lhs, rhs = float(ax @ z), float(x @ atz)
     assert abs(lhs - rhs) <= 1e-12 * (np.abs(ax).sum() * np.abs(z).max() + 1e-300)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("case", [c for c in CASES["advection"] if c["D"] == 3], ids=lambda c: c["id"])
+def test_transpose_kernels_agree(case, mode):
+    """Both kernel families give the same A^T x."""
+    case = dict(case, g=0.0)
+    op = make_operator(case, "adv", mode)
+    if op.kernel != "kron":
+        pytest.skip("not eligible for the Kronecker kernel")
+    x = inputs(case, seed=7)
+    yk = cuda_apply(op, x, transpose=True)
+    _select(op, "generic")
+    yg = cuda_apply(op, x, transpose=True)
+    assert rel_max(yk, yg) <= APPLY_TOL
 
 
 def _c1():
@@ -49,24 +81,49 @@ def _c2(n=64):
             "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "seed": 1}
 
 
-def test_config1_mass_full_size_vs_oracle():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_config1_mass_full_size_vs_oracle(kernel):
     case = _c1()
     x = inputs(case)
-    y = cuda_apply(make_operator(case, "mass"), x)
+    op = _select(make_operator(case, "mass"), kernel)
+    y = cuda_apply(op, x)
     assert rel_max(y, oracle().mass_apply(case, x)) <= APPLY_TOL
 
 
-def test_config2_advection_full_size_vs_oracle():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_config2_advection_full_size_vs_oracle(kernel):
     case = _c2(64)
     x = inputs(case)
-    y = cuda_apply(make_operator(case, "adv", 1), x)
+    op = _select(make_operator(case, "adv", 1), kernel)
+    y = cuda_apply(op, x)
     assert rel_max(y, oracle().advection_apply(case, x, 1)) <= APPLY_TOL
 
 
-def test_fp32_apply_error_bound():
+def test_config2_uses_kronecker_kernel():
+    op = make_operator(_c2(8), "adv", 1)
+    assert op.kernel == "kron", op.kernel_note
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fp32_apply_error_bound(kernel):
     case = _c2(16)
-    op = make_operator(case, "adv", 1)
+    op = _select(make_operator(case, "adv", 1), kernel)
     x = inputs(case)
     y64 = cuda_apply(op, x)
     y32 = cuda_apply(op, x, f32=True)
     assert rel_max(y32, y64) < 1e-5
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_apply_ex_alpha_beta(kernel):
+    import torch
+    case = _c2(8)
+    op = _select(make_operator(case, "adv", 1), kernel)
+    x = torch.from_numpy(inputs(case)).cuda()
+    y0 = torch.from_numpy(inputs(case, seed=9)).cuda()
+    ax = torch.empty_like(x)
+    op(x, ax)
+    y = y0.clone()
+    op.apply(x, y, alpha=2.5, beta=-0.5)
+    ref = 2.5 * ax - 0.5 * y0
+    assert float((y - ref).abs().max() / ref.abs().max()) < 1e-14
