@@ -25,7 +25,8 @@ import numpy as np
 from .coefficients import Coefficient, as_coefficient
 
 __all__ = ["Space", "MassOperator", "AdvectionOperator", "MassAdvectionOperator", "SystemOperator",
-           "Coefficient", "DGOPError", "lib", "GLL", "GL", "BC_NONE", "BC_INFLOW"]
+           "CGSolver", "GMRESSolver", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL", "BC_NONE",
+           "BC_INFLOW"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libdgop.so")
@@ -44,6 +45,10 @@ class DGOPError(RuntimeError):
 class _Coef(ctypes.Structure):
     _fields_ = [("constant", ctypes.c_double), ("nterms", ctypes.c_int),
                 ("tables", (ctypes.c_void_p * MAX_DIM) * MAX_TERMS), ("element_factor", ctypes.c_void_p)]
+
+
+class _SolveResult(ctypes.Structure):
+    _fields_ = [("success", ctypes.c_int), ("iterations", ctypes.c_int), ("relative_error", ctypes.c_double)]
 
 
 _lib = None
@@ -80,6 +85,10 @@ def lib():
         L.dgop_operator_kernel_note.argtypes = [vp]
         L.dgop_operator_kernel_note.restype = ctypes.c_char_p
         L.dgop_operator_select_kernel.argtypes = [vp, i]
+        L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
+        L.dgop_solver_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -282,6 +291,53 @@ class SystemOperator(_Operator):
         coefs = [self._coef(c) for c in _components(beta, space.dim)]
         check(lib().dgop_system_create(space.handle, q, ctypes.byref(self._coef(sigma)), self._vec(coefs), bc,
                                        float(g), ctypes.byref(h)))
+        self.handle = h
+
+
+class _Solver:
+    def __init__(self, op):
+        self.op = op
+        self.handle = None
+
+    def solve(self, b, x, max_iters, tol, stream=None):
+        """Solve A x = b on the device; x holds the initial guess and receives the solution.
+
+        Returns {"success", "iterations", "relative_error"} with the reference's conventions
+        (IterativeSolverResult, Solvers/iterativesolverresult.hpp:41)."""
+        res = _SolveResult()
+        check(lib().dgop_solver_solve(self.handle, _ptr(b), _ptr(x), int(max_iters), float(tol), ctypes.byref(res),
+                                      _stream(stream)))
+        return {"success": bool(res.success), "iterations": res.iterations, "relative_error": res.relative_error}
+
+    def close(self):
+        if self.handle:
+            lib().dgop_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CGSolver(_Solver):
+    """ConjugateGradient (Solvers/conjugategradient.hpp:125), device resident."""
+
+    def __init__(self, op):
+        super().__init__(op)
+        h = ctypes.c_void_p()
+        check(lib().dgop_cg_create(op.handle, ctypes.byref(h)))
+        self.handle = h
+
+
+class GMRESSolver(_Solver):
+    """GMRES_no_alloc(restart) (Solvers/gmres.hpp:74), device resident."""
+
+    def __init__(self, op, restart=30):
+        super().__init__(op)
+        h = ctypes.c_void_p()
+        check(lib().dgop_gmres_create(op.handle, int(restart), ctypes.byref(h)))
         self.handle = h
 
 

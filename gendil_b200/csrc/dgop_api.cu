@@ -512,7 +512,7 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 
 template <typename Real>
 static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, Real alpha, const Real* x, Real beta_y,
-                       Real* y, int extra_flags, cudaStream_t s) {
+                       Real* y, int extra_flags, cudaStream_t s, const int* skip) {
   if (!x || !y) {
     set_error("null vector");
     return DGOP_ERR_ARG;
@@ -528,6 +528,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.alpha = alpha;
     p.beta_y = beta_y;
     p.flags = op->flags | extra_flags;
+    p.skip = skip;
     K.entry->launch(p, K.grid, K.block, K.smem, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
@@ -543,6 +544,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   p.alpha = alpha;
   p.beta_y = beta_y;
   p.flags = op->flags | extra_flags;
+  p.skip = skip;
   L.entry->launch(p, L.grid, L.block, L.smem, s);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
@@ -550,13 +552,13 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
 }
 
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
-               cudaStream_t s) {
-  return launch_impl<double>(op, op->f64, op->k64, alpha, x, beta_y, y, extra_flags, s);
+               cudaStream_t s, const int* skip) {
+  return launch_impl<double>(op, op->f64, op->k64, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
-               cudaStream_t s) {
-  return launch_impl<float>(op, op->f32, op->k32, alpha, x, beta_y, y, extra_flags, s);
+               cudaStream_t s, const int* skip) {
+  return launch_impl<float>(op, op->f32, op->k32, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 }  // namespace dgop

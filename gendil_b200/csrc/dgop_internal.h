@@ -70,8 +70,9 @@ struct dgop_operator {
 
 namespace dgop {
 // Launch the operator kernel: y = alpha * Op(x) + beta_y * y, with `extra_flags` or-ed in.
+// When `skip` (a device word) is non-zero at run time the launch does nothing.
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
-               cudaStream_t s);
+               cudaStream_t s, const int* skip = nullptr);
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
-               cudaStream_t s);
+               cudaStream_t s, const int* skip = nullptr);
 }  // namespace dgop

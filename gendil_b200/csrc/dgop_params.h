@@ -58,6 +58,7 @@ struct OpParams {
   int eb;                   // elements per CTA
   Real* scratch;            // global workspace when the element does not fit in shared memory
   int64_t scratch_per_cta;  // in Real elements
+  const int* skip;          // device word; the launch does nothing when it is non-zero (solvers)
 };
 
 }  // namespace dgop

@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(256) generic_kernel(const __grid_constant__ Op
   using S = GenericShape<D, N, Q>;
   constexpr int ND = S::ND, QD = S::QD, MD = S::MD, NF = S::NF, QF = S::QF, MF = S::MF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (P.skip && *P.skip) return;  // a finished solve: nothing to do
   const int EB = P.eb;
   Real* sB = reinterpret_cast<Real*>(smem_raw);
   Real* sDq = sB + Q * N;

@@ -75,6 +75,7 @@ struct KronParams {
   const signed char* sgn[3][3];  // sgn[a][k][e_k] in {-1, 0, 1} (k != a)
   const Real* elem[3];           // per-element beta_a factor or nullptr
   const Real* elem_mass;         // per-element sigma factor or nullptr
+  const int* skip;               // device word; the launch does nothing when it is non-zero
 };
 
 struct KronPlanHost {

@@ -402,6 +402,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const bool adv = P.has_adv != 0;
   const bool slot = le < EPW;
+  if (P.skip && *P.skip) return;  // a finished solve: nothing to do
 
   int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if (g < ngroups) stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), wbase, lane, le, t, adv);

@@ -1,0 +1,607 @@
+// Device-resident Krylov solvers: unpreconditioned CG and restarted GMRES(m) with modified
+// Gram-Schmidt, following the reference's algorithms step by step
+// (Solvers/conjugategradient.hpp:125-209, Solvers/gmres.hpp:74-289).
+//
+// Every step is a kernel whose work is predicated on device-side state words (done / inactive),
+// so the host enqueues iterations without waiting and reads the state only occasionally (CG:
+// every kCheckEvery iterations; GMRES: once per restart cycle).  Iterations enqueued after
+// convergence do nothing; the operator kernels take the same word through their `skip` pointer.
+// Scalars (alpha, beta, the Hessenberg column, Givens rotations, stopping tests) never leave the
+// device.  Inner products are deterministic: a fixed grid writes per-block partial sums with a
+// fixed reduction tree, and every consumer sums the partials in the same fixed order.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "dgop_internal.h"
+
+namespace dgop {
+
+namespace {
+
+constexpr int kRB = 592;  // reduction blocks (4 per SM on 148 SMs)
+constexpr int kRT = 256;  // threads per reduction block
+constexpr int kCheckEvery = 8;
+
+// Sum over the block in a fixed order; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[kRT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < kRT / 32 ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  __syncthreads();
+  return s;
+}
+
+// Sum of the kRB partials in a fixed order, broadcast to every thread of the block.
+__device__ __forceinline__ double reduce_partials(const double* __restrict__ partials) {
+  __shared__ double res;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < kRB; i += kRT) v += partials[i];
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) res = s;
+  __syncthreads();
+  return res;
+}
+
+__device__ __forceinline__ void write_partial(double* partials, double v) {
+  const double s = block_sum(v);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+#define DGOP_GRID_LOOP(i, n) for (int64_t i = blockIdx.x * (int64_t)kRT + threadIdx.x; i < (n); i += (int64_t)kRB * kRT)
+
+// partials <- sum a .* b
+__global__ void __launch_bounds__(kRT) k_dot(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                                             double* partials, const int* skip) {
+  if (skip && *skip) return;
+  double v = 0.0;
+  DGOP_GRID_LOOP(i, n) v += a[i] * b[i];
+  write_partial(partials, v);
+}
+
+// out <- b - w ; partials <- |out|^2   (V[0] = rhs; V[0] -= w, residual = rhs; residual -= tmp)
+__global__ void __launch_bounds__(kRT) k_sub_norm(const double* __restrict__ b, const double* __restrict__ w,
+                                                  double* __restrict__ out, int64_t n, double* partials,
+                                                  const int* skip) {
+  if (skip && *skip) return;
+  double v = 0.0;
+  DGOP_GRID_LOOP(i, n) {
+    const double r = b[i] - w[i];
+    out[i] = r;
+    v += r * r;
+  }
+  write_partial(partials, v);
+}
+
+// ------------------------------------------------------------------------------- CG
+
+struct CGState {
+  int done, success, iters, zero_x;
+  double rhs_n, r_n, rel;
+  double abs_[2];  // (r, r) by iteration parity
+};
+
+// conjugategradient.hpp:143-165: norms of the initial residual, early exits.
+__global__ void __launch_bounds__(kRT) k_cg_init(CGState* st, const double* partials, double tol) {
+  const double R = reduce_partials(partials);
+  if (threadIdx.x != 0) return;
+  st->done = 0;
+  st->success = 0;
+  st->iters = 0;
+  st->zero_x = 0;
+  const double rhs_n = sqrt(R);  // the "rhs norm" is the norm of the initial residual
+  st->rhs_n = rhs_n;
+  if (rhs_n == 0.0 || rhs_n < 1e-30) {
+    st->zero_x = 1;
+    st->done = 1;
+    st->success = 1;
+    st->rel = 0.0;
+    return;
+  }
+  const double r_n = sqrt(R);
+  st->r_n = r_n;
+  if (r_n < tol * rhs_n) {
+    st->done = 1;
+    st->success = 1;
+    st->rel = sqrt(r_n / rhs_n);
+    return;
+  }
+  st->abs_[0] = R;  // dot(residual, p) with p = residual
+}
+
+// p <- r ; x <- 0 for a zero right-hand side
+__global__ void __launch_bounds__(kRT) k_cg_init_p(const CGState* st, const double* __restrict__ r,
+                                                   double* __restrict__ p, double* __restrict__ x, int64_t n) {
+  const int zero_x = st->zero_x;
+  DGOP_GRID_LOOP(i, n) {
+    p[i] = r[i];
+    if (zero_x) x[i] = 0.0;
+  }
+}
+
+// alpha = (r, r) / (p, A p); x += alpha p; r -= alpha A p; partials2 <- |r|^2   (:176-181)
+__global__ void __launch_bounds__(kRT) k_cg_update(int k, const CGState* st, double* __restrict__ x,
+                                                   double* __restrict__ r, const double* __restrict__ p,
+                                                   const double* __restrict__ ap, int64_t n, const double* partials1,
+                                                   double* partials2) {
+  if (st->done) return;
+  const double alpha = st->abs_[k & 1] / reduce_partials(partials1);
+  double v = 0.0;
+  DGOP_GRID_LOOP(i, n) {
+    x[i] = x[i] + alpha * p[i];
+    const double ri = r[i] + (-alpha) * ap[i];
+    r[i] = ri;
+    v += ri * ri;
+  }
+  write_partial(partials2, v);
+}
+
+// stopping test, beta = (r_new, r_new) / (r_old, r_old), p = beta p + r   (:183-205)
+__global__ void __launch_bounds__(kRT) k_cg_finish(int k, CGState* st, const double* __restrict__ r,
+                                                   double* __restrict__ p, int64_t n, const double* partials2,
+                                                   double tol, int max_iters) {
+  if (st->done) return;
+  const double R = reduce_partials(partials2);
+  const double r_n = sqrt(R);
+  const double rhs_n = st->rhs_n;
+  if (r_n < tol * rhs_n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->r_n = r_n;
+      st->iters = k + 1;
+      st->rel = sqrt(r_n / rhs_n);
+      st->success = 1;
+      st->done = 1;
+    }
+    return;
+  }
+  const double beta = R / st->abs_[k & 1];
+  DGOP_GRID_LOOP(i, n) p[i] = p[i] * beta + r[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->abs_[(k + 1) & 1] = R;
+    st->r_n = r_n;
+    if (k + 1 >= max_iters) {
+      st->iters = max_iters;
+      st->rel = sqrt(r_n / rhs_n);
+      st->success = 0;
+      st->done = 1;
+    }
+  }
+}
+
+// max_iters == 0 without early exit: the loop does not run (:207-208)
+__global__ void k_cg_no_iters(CGState* st) {
+  if (st->done) return;
+  st->iters = 0;
+  st->rel = sqrt(st->r_n / st->rhs_n);
+  st->success = 0;
+  st->done = 1;
+}
+
+// ------------------------------------------------------------------------------- GMRES
+
+struct GMState {
+  int done, success, iters, total, k, brk, inactive, pad;
+  double denom, beta, rel, inv_h;
+};
+
+__global__ void __launch_bounds__(kRT) k_gm_denom(GMState* st, const double* partials) {
+  const double R = reduce_partials(partials);
+  if (threadIdx.x != 0) return;
+  const double norm_rhs = sqrt(R);
+  st->denom = norm_rhs > 0.0 ? norm_rhs : 1.0;  // gmres.hpp:113-115
+  st->done = 0;
+  st->success = 0;
+  st->iters = 0;
+  st->total = 0;
+  st->k = 0;
+  st->brk = 0;
+  st->inactive = 0;
+}
+
+// true residual |b - A x| / denom and the decisions taken after it (gmres.hpp:117-123, 230-236, 269-280)
+// phase 0: initial; 1: end of a cycle; 2: residual-only solve (no iterations allowed)
+__global__ void __launch_bounds__(kRT) k_gm_resid(GMState* st, const double* partials, double tol, int max_iters,
+                                                  int phase) {
+  if (st->done) return;
+  const double R = reduce_partials(partials);
+  if (threadIdx.x != 0) return;
+  const double beta = sqrt(R);
+  const double rel = beta / st->denom;
+  st->beta = beta;
+  st->rel = rel;
+  if (phase == 2 || (phase == 1 && st->k == 0)) {
+    st->success = rel <= tol;
+    st->iters = st->total;
+    st->done = 1;
+    return;
+  }
+  if (rel <= tol) {
+    st->success = 1;
+    st->iters = st->total;
+    st->done = 1;
+    return;
+  }
+  if (phase == 1 && st->total >= max_iters) {
+    st->success = 0;
+    st->iters = st->total;
+    st->done = 1;
+  }
+}
+
+// start of a cycle: reset the rotations and the reduced right-hand side (gmres.hpp:132-146)
+__global__ void k_gm_cycle_start(GMState* st, double* cs, double* sn, double* e1, double* y, int m, int max_iters) {
+  if (st->done) {
+    st->inactive = 1;
+    return;
+  }
+  for (int i = 0; i < m; ++i) {
+    cs[i] = 1.0;
+    sn[i] = 0.0;
+    y[i] = 0.0;
+  }
+  for (int i = 0; i <= m; ++i) e1[i] = 0.0;
+  e1[0] = st->beta;
+  st->k = 0;
+  st->brk = 0;
+  st->inactive = st->total >= max_iters;
+  st->inv_h = 1.0 / st->beta;
+}
+
+// v <- v * s (s = st->inv_h): V[0] *= 1/beta at a cycle start (j < 0) and V[j+1] = w * (1/h_next)
+// after iteration j, when that iteration ran and did not end the cycle
+__global__ void __launch_bounds__(kRT) k_gm_scale(const GMState* st, const double* __restrict__ src,
+                                                  double* __restrict__ dst, int64_t n, int j) {
+  if (st->done || (j >= 0 && (st->brk || st->k != j + 1))) return;
+  const double s = st->inv_h;
+  DGOP_GRID_LOOP(i, n) dst[i] = src[i] * s;
+}
+
+// one modified Gram-Schmidt step (gmres.hpp:160-165), fused with the next inner product:
+// h = (V_i, w) from partials_in; H(i, j) = h; w -= h V_i; partials_out <- (next, w)
+__global__ void __launch_bounds__(kRT) k_gm_mgs(const GMState* st, int i, int j, int m, const double* __restrict__ vi,
+                                                const double* __restrict__ next, double* __restrict__ w, int64_t n,
+                                                double* H, const double* partials_in, double* partials_out) {
+  if (st->inactive) return;
+  const double h = reduce_partials(partials_in);
+  if (blockIdx.x == 0 && threadIdx.x == 0) H[j * (m + 1) + i] = h;
+  double v = 0.0;
+  const bool self = next == w;
+  DGOP_GRID_LOOP(l, n) {
+    const double wl = w[l] + (-h) * vi[l];
+    w[l] = wl;
+    v += (self ? wl : next[l]) * wl;
+  }
+  write_partial(partials_out, v);
+}
+
+// Hessenberg column j: norm, previous rotations, new rotation, stopping tests (gmres.hpp:167-222)
+__global__ void __launch_bounds__(kRT) k_gm_column(GMState* st, int j, int m, double* H, double* cs, double* sn,
+                                                   double* e1, const double* partials, double tol, int max_iters) {
+  if (st->inactive) return;
+  const double R = reduce_partials(partials);
+  if (threadIdx.x != 0) return;
+  const double eps = DBL_EPSILON;
+  const double beta = st->beta;
+  st->total += 1;
+#define HH(a, b) H[(b) * (m + 1) + (a)]
+  const double h_next = sqrt(R);
+  HH(j + 1, j) = h_next;
+  for (int i = 0; i < j; ++i) {
+    const double h_im = HH(i, j), h_ip = HH(i + 1, j);
+    HH(i, j) = cs[i] * h_im + sn[i] * h_ip;
+    HH(i + 1, j) = -sn[i] * h_im + cs[i] * h_ip;
+  }
+  const double h_mm = HH(j, j), h_m1m = HH(j + 1, j);
+  const double rho = sqrt(h_mm * h_mm + h_m1m * h_m1m);
+  if (rho <= eps * beta) {
+    HH(j, j) = 0.0;
+    HH(j + 1, j) = 0.0;
+    st->k = j;
+    st->brk = 1;
+    st->inactive = 1;
+    return;
+  }
+  cs[j] = h_mm / rho;
+  sn[j] = h_m1m / rho;
+  HH(j, j) = rho;
+  HH(j + 1, j) = 0.0;
+  const double g_m = e1[j], g_m1 = e1[j + 1];
+  e1[j] = cs[j] * g_m + sn[j] * g_m1;
+  e1[j + 1] = -sn[j] * g_m + cs[j] * g_m1;
+  st->k = j + 1;
+  const double rel_est = fabs(e1[j + 1]) / st->denom;
+  const bool happy = h_next <= eps * beta;
+  if (happy || rel_est <= tol) {
+    st->brk = 1;
+    st->inactive = 1;
+    return;
+  }
+  st->inv_h = 1.0 / h_next;
+  if (st->total >= max_iters || j + 1 >= m) st->inactive = 1;
+#undef HH
+}
+
+// back-substitution in the k x k triangle (gmres.hpp:238-261)
+__global__ void k_gm_backsub(const GMState* st, const double* H, const double* e1, double* y, int m) {
+  if (st->done || st->k == 0) return;
+  const double eps = DBL_EPSILON, beta = st->beta;
+  const int k = st->k;
+  for (int i = k; i-- > 0;) {
+    double sum = e1[i];
+    for (int j = i + 1; j < k; ++j) sum -= H[j * (m + 1) + i] * y[j];
+    const double diag = H[i * (m + 1) + i];
+    y[i] = fabs(diag) <= eps * beta ? 0.0 : sum / diag;
+  }
+}
+
+// x += y_i V_i for i < k, in order (the reference's sequence of Axpy calls, gmres.hpp:263-267)
+__global__ void __launch_bounds__(kRT) k_gm_update(const GMState* st, double* __restrict__ x,
+                                                   const double* __restrict__ V, int64_t ld, const double* y,
+                                                   int64_t n) {
+  if (st->done || st->k == 0) return;
+  const int k = st->k;
+  DGOP_GRID_LOOP(l, n) {
+    double xl = x[l];
+    for (int i = 0; i < k; ++i) xl = xl + y[i] * V[(int64_t)i * ld + l];
+    x[l] = xl;
+  }
+}
+
+// GMRES with the whole state resident: the residual of x into V0 and its norm
+}  // namespace
+
+struct SolverImpl {
+  int kind = 0;  // 0: CG, 1: GMRES
+  int restart = 0;
+  dgop_operator* op = nullptr;
+  int64_t n = 0;
+  double* work = nullptr;      // vectors
+  double* partials = nullptr;  // 2 x kRB
+  void* state = nullptr;       // CGState / GMState (device)
+  double* small = nullptr;     // GMRES: H, cs, sn, e1, y
+  int* h_flag = nullptr;       // pinned host copy of `done`
+};
+
+}  // namespace dgop
+
+struct dgop_solver {
+  dgop::SolverImpl s;
+};
+
+using namespace dgop;
+
+namespace {
+
+#define DGOP_CUDA_S(call)                               \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+int solver_alloc(dgop_solver* sv, int nvec, size_t state_bytes, size_t small_count) {
+  SolverImpl& s = sv->s;
+  DGOP_CUDA_S(cudaMalloc(&s.work, sizeof(double) * (size_t)s.n * nvec));
+  DGOP_CUDA_S(cudaMalloc(&s.partials, sizeof(double) * 2 * kRB));
+  DGOP_CUDA_S(cudaMalloc(&s.state, state_bytes));
+  DGOP_CUDA_S(cudaMemset(s.state, 0, state_bytes));
+  if (small_count) DGOP_CUDA_S(cudaMalloc(&s.small, sizeof(double) * small_count));
+  DGOP_CUDA_S(cudaMallocHost(&s.h_flag, sizeof(int)));
+  return DGOP_OK;
+}
+
+void solver_free(dgop_solver* sv) {
+  SolverImpl& s = sv->s;
+  if (s.work) cudaFree(s.work);
+  if (s.partials) cudaFree(s.partials);
+  if (s.state) cudaFree(s.state);
+  if (s.small) cudaFree(s.small);
+  if (s.h_flag) cudaFreeHost(s.h_flag);
+  s = SolverImpl{};
+}
+
+int read_done(SolverImpl& s, cudaStream_t st, int* done) {
+  DGOP_CUDA_S(cudaMemcpyAsync(s.h_flag, s.state, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DGOP_CUDA_S(cudaStreamSynchronize(st));
+  *done = *s.h_flag;
+  return DGOP_OK;
+}
+
+#define DGOP_TRY(call)             \
+  do {                             \
+    const int _rc = (call);        \
+    if (_rc != DGOP_OK) return _rc; \
+  } while (0)
+
+int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
+             cudaStream_t st) {
+  const int64_t n = s.n;
+  double* tmp = s.work;
+  double* r = s.work + n;
+  double* p = s.work + 2 * n;
+  double* pa = s.partials;
+  double* pb = s.partials + kRB;
+  CGState* cs = static_cast<CGState*>(s.state);
+  // 1) r = rhs - A x
+  DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, tmp, 0, st));
+  k_sub_norm<<<kRB, kRT, 0, st>>>(b, tmp, r, n, pa, nullptr);
+  k_cg_init<<<1, kRT, 0, st>>>(cs, pa, tol);
+  k_cg_init_p<<<kRB, kRT, 0, st>>>(cs, r, p, x, n);
+  if (max_iters <= 0) k_cg_no_iters<<<1, 1, 0, st>>>(cs);
+  DGOP_CUDA_S(cudaGetLastError());
+  const int* done = &cs->done;
+  for (int k = 0; k < max_iters; ++k) {
+    DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, 0, st, done));
+    k_dot<<<kRB, kRT, 0, st>>>(p, tmp, n, pa, done);
+    k_cg_update<<<kRB, kRT, 0, st>>>(k, cs, x, r, p, tmp, n, pa, pb);
+    k_cg_finish<<<kRB, kRT, 0, st>>>(k, cs, r, p, n, pb, tol, max_iters);
+    DGOP_CUDA_S(cudaGetLastError());
+    if ((k + 1) % kCheckEvery == 0) {
+      int d = 0;
+      DGOP_TRY(read_done(s, st, &d));
+      if (d) break;
+    }
+  }
+  CGState h;
+  DGOP_CUDA_S(cudaMemcpyAsync(&h, cs, sizeof(h), cudaMemcpyDeviceToHost, st));
+  DGOP_CUDA_S(cudaStreamSynchronize(st));
+  res->success = h.success;
+  res->iterations = h.iters;
+  res->relative_error = h.rel;
+  return DGOP_OK;
+}
+
+int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
+                cudaStream_t st) {
+  const int64_t n = s.n;
+  const int m = s.restart;
+  double* w = s.work;
+  double* V = s.work + n;  // m + 1 basis vectors
+  double* pa = s.partials;
+  double* pb = s.partials + kRB;
+  double* H = s.small;
+  double* csv = H + (m + 1) * m;
+  double* snv = csv + m;
+  double* e1 = snv + m;
+  double* y = e1 + m + 1;
+  GMState* gs = static_cast<GMState*>(s.state);
+  const int* done = &gs->done;
+  const int* inactive = &gs->inactive;
+  auto residual = [&](int phase) -> int {
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, 0, st, done));
+    k_sub_norm<<<kRB, kRT, 0, st>>>(b, w, V, n, pa, done);
+    k_gm_resid<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters, phase);
+    DGOP_CUDA_S(cudaGetLastError());
+    return DGOP_OK;
+  };
+  k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
+  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
+  DGOP_CUDA_S(cudaGetLastError());
+  if (max_iters <= 0 || m <= 0) {
+    DGOP_TRY(residual(2));
+  } else {
+    DGOP_TRY(residual(0));
+    // every cycle performs at least one iteration or finishes the solve
+    for (int cycle = 0; cycle <= max_iters; ++cycle) {
+      int d = 0;
+      DGOP_TRY(read_done(s, st, &d));
+      if (d) break;
+      k_gm_cycle_start<<<1, 1, 0, st>>>(gs, csv, snv, e1, y, m, max_iters);
+      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, V, V, n, -1);
+      for (int j = 0; j < m; ++j) {
+        double* vj = V + (int64_t)j * n;
+        DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, 0, st, inactive));
+        k_dot<<<kRB, kRT, 0, st>>>(V, w, n, pa, inactive);
+        double* pin = pa;
+        double* pout = pb;
+        for (int i = 0; i <= j; ++i) {
+          const double* next = (i < j) ? V + (int64_t)(i + 1) * n : w;
+          k_gm_mgs<<<kRB, kRT, 0, st>>>(gs, i, j, m, V + (int64_t)i * n, next, w, n, H, pin, pout);
+          std::swap(pin, pout);
+        }
+        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
+        k_gm_scale<<<kRB, kRT, 0, st>>>(gs, w, V + (int64_t)(j + 1) * n, n, j);
+        DGOP_CUDA_S(cudaGetLastError());
+      }
+      k_gm_backsub<<<1, 1, 0, st>>>(gs, H, e1, y, m);
+      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, V, n, y, n);
+      DGOP_TRY(residual(1));
+    }
+  }
+  GMState h;
+  DGOP_CUDA_S(cudaMemcpyAsync(&h, gs, sizeof(h), cudaMemcpyDeviceToHost, st));
+  DGOP_CUDA_S(cudaStreamSynchronize(st));
+  res->success = h.success;
+  res->iterations = h.iters;
+  res->relative_error = h.rel;
+  return DGOP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgop_cg_create(dgop_operator* op, dgop_solver** out) {
+  if (!op || !out) {
+    set_error("dgop_cg_create: null argument");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  auto* sv = new (std::nothrow) dgop_solver();
+  if (!sv) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  sv->s.kind = 0;
+  sv->s.op = op;
+  sv->s.n = op->sp.ndofs;
+  const int rc = solver_alloc(sv, 3, sizeof(CGState), 0);
+  if (rc != DGOP_OK) {
+    solver_free(sv);
+    delete sv;
+    return rc;
+  }
+  *out = sv;
+  return DGOP_OK;
+}
+
+int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out) {
+  if (!op || !out || restart < 1 || restart > 1000) {
+    set_error("dgop_gmres_create: null argument or restart outside [1, 1000]");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  auto* sv = new (std::nothrow) dgop_solver();
+  if (!sv) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  sv->s.kind = 1;
+  sv->s.op = op;
+  sv->s.n = op->sp.ndofs;
+  sv->s.restart = restart;
+  const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
+  const int rc = solver_alloc(sv, restart + 2, sizeof(GMState), small);
+  if (rc != DGOP_OK) {
+    solver_free(sv);
+    delete sv;
+    return rc;
+  }
+  *out = sv;
+  return DGOP_OK;
+}
+
+int dgop_solver_solve(dgop_solver* sv, const double* b, double* x, int max_iters, double tol,
+                      dgop_solve_result* result, void* stream) {
+  if (!sv || !b || !x || !result) {
+    set_error("dgop_solver_solve: null argument");
+    return DGOP_ERR_ARG;
+  }
+  if (!(tol >= 0.0)) {
+    set_error("dgop_solver_solve: tol must be >= 0");
+    return DGOP_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  return sv->s.kind == 0 ? cg_solve(sv->s, b, x, max_iters, tol, result, st)
+                         : gmres_solve(sv->s, b, x, max_iters, tol, result, st);
+}
+
+int dgop_solver_destroy(dgop_solver* sv) {
+  if (!sv) return DGOP_OK;
+  solver_free(sv);
+  delete sv;
+  return DGOP_OK;
+}
+
+}  // extern "C"

@@ -98,6 +98,28 @@ int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* st
 /* FP32 apply of the same operator (tables rounded to FP32); no reference counterpart. */
 int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
 
+/* ---- Krylov solvers, device resident (workspaces allocated at create time).
+ * CG: the reference's ConjugateGradient scratch overload (Solvers/conjugategradient.hpp:125-209),
+ *   including its conventions: the tolerance is relative to the norm of the INITIAL residual
+ *   b - A x0, `iterations` counts the iteration that converged, and `relative_error` is
+ *   sqrt(|r| / |r0|).
+ * GMRES(restart): GMRES_no_alloc (Solvers/gmres.hpp:74-289): modified Gram-Schmidt Arnoldi,
+ *   Givens rotations, breakdown test rho <= eps * beta, the true residual recomputed after every
+ *   cycle; `relative_error` = |b - A x| / |b|.
+ * x holds the initial guess on entry and the solution on return.  dgop_solver_solve enqueues on
+ * `stream` and synchronizes it before returning the result. */
+typedef struct {
+  int success;
+  int iterations;
+  double relative_error;
+} dgop_solve_result;
+typedef struct dgop_solver dgop_solver;
+int dgop_cg_create(dgop_operator* op, dgop_solver** out);
+int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out);
+int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_iters, double tol,
+                      dgop_solve_result* result, void* stream);
+int dgop_solver_destroy(dgop_solver* solver);
+
 /* FillRandom (Algebra/vector.hpp:632): out[i] = std::uniform_real_distribution<double>(lo, hi)
  * draws from std::mt19937(seed), in order, into a HOST buffer of n values. */
 int dgop_fill_random(double* out, int64_t n, unsigned seed, double lo, double hi);
