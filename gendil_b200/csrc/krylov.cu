@@ -15,6 +15,7 @@
 #include <cmath>
 #include <new>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "dgop_internal.h"
@@ -605,3 +606,79 @@ int dgop_solver_destroy(dgop_solver* sv) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// CG with a workspace that is never allocated at run time.
+//
+// Some callers cannot let a library call cudaMalloc: programs whose host framework owns every
+// byte of device memory through its own pool (a caching allocator with a fixed budget), and
+// latency-critical loops where cudaMalloc/cudaFree would add a device-wide synchronization.
+// For them dgop_cg_solve_static runs the same CG kernels as dgop_cg_create/dgop_solver_solve
+// with its three work vectors, partial sums and solver state in one file-scope device array of
+// fixed size (every GPU that loads this library holds it, about 6.3 MB, until the process exits).
+// ------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kStaticCgWords = 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS + 2 * kRB + (sizeof(CGState) + 7) / 8;
+static __device__ __align__(256) double g_static_cg_scratch[kStaticCgWords];
+
+std::mutex g_static_cg_mutex;
+double* g_static_cg_addr[64] = {};  // device address of the array, per device
+thread_local int g_static_cg_flag;  // host copy of the `done` word (pageable; no allocation)
+
+// Device address of the array on the current device, looked up once per device.  In host code
+// the array's name is only a stand-in; the kernels must be given this address.
+int static_cg_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) {
+    set_error("dgop_cg_solve_static: device index out of range");
+    return DGOP_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_static_cg_mutex);
+  if (!g_static_cg_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_cg_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static CG workspace)");
+    g_static_cg_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_static_cg_addr[dev];
+  return DGOP_OK;
+}
+
+}  // namespace
+
+extern "C" int dgop_cg_solve_static(dgop_operator* op, const double* b, double* x, int max_iters, double tol,
+                                    dgop_solve_result* result, void* stream) {
+  if (!op || !b || !x || !result) {
+    set_error("dgop_cg_solve_static: null argument");
+    return DGOP_ERR_ARG;
+  }
+  if (!(tol >= 0.0)) {
+    set_error("dgop_cg_solve_static: tol must be >= 0");
+    return DGOP_ERR_ARG;
+  }
+  const int64_t n = op->sp.ndofs;
+  if (n > DGOP_STATIC_CG_MAX_DOFS) {
+    set_error("dgop_cg_solve_static: " + std::to_string(n) + " DoFs exceed the static workspace limit of " +
+              std::to_string((long long)DGOP_STATIC_CG_MAX_DOFS) + " DoFs; use dgop_cg_create instead");
+    return DGOP_ERR_ARG;
+  }
+  double* base = nullptr;
+  const int rc = static_cg_scratch(&base);
+  if (rc != DGOP_OK) return rc;
+  SolverImpl s;
+  s.kind = 0;
+  s.op = op;
+  s.n = n;
+  s.work = base;
+  s.partials = base + 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS;
+  s.state = base + 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS + 2 * kRB;
+  s.h_flag = &g_static_cg_flag;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the array keeps the previous call's contents: start from a cleared solver state
+  const cudaError_t e = cudaMemsetAsync(s.state, 0, sizeof(CGState), st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(static CG state)");
+  return cg_solve(s, b, x, max_iters, tol, result, st);
+}

@@ -120,6 +120,22 @@ int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_i
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);
 
+/* CG without any allocation at call time (no counterpart in the reference).  For callers that
+ * must not let a library allocate device memory: a host framework that owns all device memory
+ * through its own pool, or a latency-critical loop where cudaMalloc/cudaFree would synchronize the
+ * device.  Same algorithm, kernels and results as dgop_cg_create + dgop_solver_solve, but the work
+ * vectors, partial sums and solver state live in one fixed device array inside the library
+ * (about 6.3 MB, held on every GPU that loads the library until the process exits).
+ *  - Operators with more than DGOP_STATIC_CG_MAX_DOFS DoFs are rejected with DGOP_ERR_ARG.
+ *  - The first call on a device looks the array's device address up once (cudaGetSymbolAddress);
+ *    make that first call before any stream capture on that device.
+ *  - Every call shares the one array: calls whose GPU work overlaps (other streams, other host
+ *    threads on the same device) race and corrupt each other's results; serialize them.
+ *  - Synchronizes `stream` before returning, like dgop_solver_solve. */
+#define DGOP_STATIC_CG_MAX_DOFS 262144
+int dgop_cg_solve_static(dgop_operator* op, const double* b, double* x, int max_iters, double tol,
+                         dgop_solve_result* result, void* stream);
+
 /* FillRandom (Algebra/vector.hpp:632): out[i] = std::uniform_real_distribution<double>(lo, hi)
  * draws from std::mt19937(seed), in order, into a HOST buffer of n values. */
 int dgop_fill_random(double* out, int64_t n, unsigned seed, double lo, double hi);
