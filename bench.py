@@ -34,6 +34,8 @@ N_AXIS, ORDER, NQ = 64, 3, 4
 METRIC = "GDoF/s per operator apply vs HBM roofline; mixed vs FP64 solve time @1e-10"
 WORKLOAD = "fp64 upwind DG advection apply, 3D 64^3 hex, p=3 GLL, q=4 GL, sin/cos velocity, inflow 0"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) of one launch measured by ncu on the 64^3 workload, by kernel family
+TRAFFIC_BYTES = {("kron", 64): 221.3e6}
 
 
 def case_dict(n=N_AXIS):
@@ -155,6 +157,44 @@ def run_reference(args):
     return 0
 
 
+def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10):
+    """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed 2), GMRES(restart) to tol
+    relative FP64 residual from x0 = 0, timed on the device (CUDA events around the whole solve):
+    once all-FP64, once with FP32 restart cycles and FP64 refinement.  Each leg reports the
+    residual it reached, recomputed here with the FP64 operator, and the mixed leg its max-norm
+    distance to the FP64 solution."""
+    import torch
+    A = g.SystemOperator(space, NQ, C.velocity_sincos(3), sigma=1.0 / dt, bc=g.BC_INFLOW, g=0.0)
+    b = torch.from_numpy(g.fill_random(space.num_dofs, 2)).to(dev)
+    bnorm = torch.linalg.vector_norm(b).item()
+    out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, x0 = 0, b = FillRandom(seed 2)"}
+    sols = {}
+    for name, cls in (("fp64_gmres", g.GMRESSolver), ("mixed_gmres_ir", g.GMRESIRSolver)):
+        solver = cls(A, restart)
+        x = torch.zeros_like(b)
+        solver.solve(b, x, 2, tol)  # warm-up (kernels, caches)
+        x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        info = solver.solve(b, x, 20000, tol)
+        e1.record()
+        torch.cuda.synchronize()
+        ax = torch.empty_like(x)
+        A(x, ax)
+        true_rel = torch.linalg.vector_norm(b - ax).item() / bnorm
+        out[name] = {"seconds": e0.elapsed_time(e1) * 1e-3, "iterations": info["iterations"],
+                     "relative_residual": info["relative_error"], "true_relative_residual": true_rel,
+                     "converged": info["success"]}
+        sols[name] = x
+        solver.close()
+    d = (sols["mixed_gmres_ir"] - sols["fp64_gmres"]).abs().max() / sols["fp64_gmres"].abs().max()
+    out["mixed_gmres_ir"]["rel_max_diff_vs_fp64"] = d.item()
+    out["fp64_over_mixed_time"] = out["fp64_gmres"]["seconds"] / out["mixed_gmres_ir"]["seconds"]
+    A.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -229,13 +269,8 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     alg_bytes = 16.0 * nd
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("advection_fp64_64cubed_p3")
-        except (OSError, ValueError):
-            traffic = None
+    # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu, summarized under profiles/)
+    traffic = TRAFFIC_BYTES.get((op.kernel, args.size))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -254,6 +289,8 @@ def run_ours(args):
         line["config"]["kernel"] = op.kernel
         if args.size != N_AXIS:
             line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
+        if world == 1 and not args.no_solve:
+            line["solve"] = solve_leg(g, C, space, dev)
         if world == 1 and not args.no_cpu_baseline and args.size == N_AXIS:
             try:
                 line["cpu_baseline"] = cpu_baseline(x_np)
@@ -268,7 +305,8 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--no-solve", action="store_true", help="skip the GMRES solve leg")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -521,7 +521,21 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     set_error("in-place apply is not supported (x and y alias)");
     return DGOP_ERR_ARG;
   }
-  if (op->kernel == DGOP_KERNEL_KRON && K.ready) {
+  const uintptr_t ax = reinterpret_cast<uintptr_t>(x), ay = reinterpret_cast<uintptr_t>(y);
+  if (ax % sizeof(Real) || ay % sizeof(Real)) {
+    set_error("vectors must be aligned to their element size");
+    return DGOP_ERR_ARG;
+  }
+  // the Kronecker kernel stages element blocks with 16-byte copies; other pointers take the
+  // generic kernel, or are rejected when the operator has none
+  const bool aligned16 = (ax % 16 == 0) && (ay % 16 == 0);
+  if (op->kernel == DGOP_KERNEL_KRON && K.ready && !aligned16 && !L.ready) {
+    set_error("the Kronecker kernel needs 16-byte aligned vectors and the operator has no generic kernel");
+    return DGOP_ERR_ARG;
+  }
+  const bool linear = (extra_flags & kLinear) != 0;
+  extra_flags &= ~kLinear;
+  if (op->kernel == DGOP_KERNEL_KRON && K.ready && aligned16) {
     KronParams<Real> p = (extra_flags & kTranspose) ? K.params_t : K.params;
     p.x = x;
     p.y = y;
@@ -529,6 +543,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.beta_y = beta_y;
     p.flags = op->flags | extra_flags;
     p.skip = skip;
+    if (linear) p.g = Real(0);
     K.entry->launch(p, K.grid, K.block, K.smem, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
@@ -545,6 +560,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   p.beta_y = beta_y;
   p.flags = op->flags | extra_flags;
   p.skip = skip;
+  if (linear) p.g = Real(0);
   L.entry->launch(p, L.grid, L.block, L.smem, s);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");

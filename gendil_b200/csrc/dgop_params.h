@@ -17,6 +17,7 @@ enum OpFlags : int {
   kFaceInt = 1 << 2,    // upwind flux on interior faces         (advectionoperator.hpp:339-389)
   kFaceBnd = 1 << 3,    // upwind flux on boundary faces, inflow value g (advectionoperator.hpp:391-438)
   kTranspose = 1 << 4,  // apply the transposed (adjoint) operator
+  kLinear = 1 << 5,     // host-side launch option: inflow value taken as 0 (the linear part)
 };
 
 // A scalar coefficient c(X) = constant + sum_t prod_k T_{t,k}(X_k), optionally multiplied by a

@@ -64,11 +64,13 @@ __device__ __forceinline__ void write_partial(double* partials, double v) {
 #define DGOP_GRID_LOOP(i, n) for (int64_t i = blockIdx.x * (int64_t)kRT + threadIdx.x; i < (n); i += (int64_t)kRB * kRT)
 
 // partials <- sum a .* b
-__global__ void __launch_bounds__(kRT) k_dot(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+// (vectors of any precision; products and sums in FP64)
+template <typename T>
+__global__ void __launch_bounds__(kRT) k_dot(const T* __restrict__ a, const T* __restrict__ b, int64_t n,
                                              double* partials, const int* skip) {
   if (skip && *skip) return;
   double v = 0.0;
-  DGOP_GRID_LOOP(i, n) v += a[i] * b[i];
+  DGOP_GRID_LOOP(i, n) v += (double)a[i] * (double)b[i];
   write_partial(partials, v);
 }
 
@@ -262,17 +264,20 @@ __global__ void k_gm_cycle_start(GMState* st, double* cs, double* sn, double* e1
 
 // v <- v * s (s = st->inv_h): V[0] *= 1/beta at a cycle start (j < 0) and V[j+1] = w * (1/h_next)
 // after iteration j, when that iteration ran and did not end the cycle
-__global__ void __launch_bounds__(kRT) k_gm_scale(const GMState* st, const double* __restrict__ src,
-                                                  double* __restrict__ dst, int64_t n, int j) {
+template <typename TS, typename TD>
+__global__ void __launch_bounds__(kRT) k_gm_scale(const GMState* st, const TS* __restrict__ src,
+                                                  TD* __restrict__ dst, int64_t n, int j) {
   if (st->done || (j >= 0 && (st->brk || st->k != j + 1))) return;
   const double s = st->inv_h;
-  DGOP_GRID_LOOP(i, n) dst[i] = src[i] * s;
+  DGOP_GRID_LOOP(i, n) dst[i] = (TD)((double)src[i] * s);
 }
 
 // one modified Gram-Schmidt step (gmres.hpp:160-165), fused with the next inner product:
 // h = (V_i, w) from partials_in; H(i, j) = h; w -= h V_i; partials_out <- (next, w)
-__global__ void __launch_bounds__(kRT) k_gm_mgs(const GMState* st, int i, int j, int m, const double* __restrict__ vi,
-                                                const double* __restrict__ next, double* __restrict__ w, int64_t n,
+// (basis vectors of any precision; the update and the product are formed in FP64)
+template <typename T>
+__global__ void __launch_bounds__(kRT) k_gm_mgs(const GMState* st, int i, int j, int m, const T* __restrict__ vi,
+                                                const T* __restrict__ next, T* __restrict__ w, int64_t n,
                                                 double* H, const double* partials_in, double* partials_out) {
   if (st->inactive) return;
   const double h = reduce_partials(partials_in);
@@ -280,9 +285,9 @@ __global__ void __launch_bounds__(kRT) k_gm_mgs(const GMState* st, int i, int j,
   double v = 0.0;
   const bool self = next == w;
   DGOP_GRID_LOOP(l, n) {
-    const double wl = w[l] + (-h) * vi[l];
+    const T wl = (T)((double)w[l] + (-h) * (double)vi[l]);
     w[l] = wl;
-    v += (self ? wl : next[l]) * wl;
+    v += (self ? (double)wl : (double)next[l]) * (double)wl;
   }
   write_partial(partials_out, v);
 }
@@ -348,23 +353,22 @@ __global__ void k_gm_backsub(const GMState* st, const double* H, const double* e
 }
 
 // x += y_i V_i for i < k, in order (the reference's sequence of Axpy calls, gmres.hpp:263-267)
+template <typename T>
 __global__ void __launch_bounds__(kRT) k_gm_update(const GMState* st, double* __restrict__ x,
-                                                   const double* __restrict__ V, int64_t ld, const double* y,
-                                                   int64_t n) {
+                                                   const T* __restrict__ V, int64_t ld, const double* y, int64_t n) {
   if (st->done || st->k == 0) return;
   const int k = st->k;
   DGOP_GRID_LOOP(l, n) {
     double xl = x[l];
-    for (int i = 0; i < k; ++i) xl = xl + y[i] * V[(int64_t)i * ld + l];
+    for (int i = 0; i < k; ++i) xl = xl + y[i] * (double)V[(int64_t)i * ld + l];
     x[l] = xl;
   }
 }
 
-// GMRES with the whole state resident: the residual of x into V0 and its norm
 }  // namespace
 
 struct SolverImpl {
-  int kind = 0;  // 0: CG, 1: GMRES
+  int kind = 0;  // 0: CG, 1: GMRES, 2: GMRES with FP32 inner cycles and FP64 refinement
   int restart = 0;
   dgop_operator* op = nullptr;
   int64_t n = 0;
@@ -391,9 +395,10 @@ namespace {
     if (_e != cudaSuccess) return cuda_fail(_e, #call); \
   } while (0)
 
-int solver_alloc(dgop_solver* sv, int nvec, size_t state_bytes, size_t small_count) {
+// `words`: FP64 words of vector workspace
+int solver_alloc(dgop_solver* sv, size_t words, size_t state_bytes, size_t small_count) {
   SolverImpl& s = sv->s;
-  DGOP_CUDA_S(cudaMalloc(&s.work, sizeof(double) * (size_t)s.n * nvec));
+  DGOP_CUDA_S(cudaMalloc(&s.work, sizeof(double) * words));
   DGOP_CUDA_S(cudaMalloc(&s.partials, sizeof(double) * 2 * kRB));
   DGOP_CUDA_S(cudaMalloc(&s.state, state_bytes));
   DGOP_CUDA_S(cudaMemset(s.state, 0, state_bytes));
@@ -529,9 +534,117 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   return DGOP_OK;
 }
 
+// FP32 vector stride of the mixed-precision workspace: n rounded up to 64 floats (256 bytes)
+int64_t ir_stride(int64_t n) { return (n + 63) / 64 * 64; }
+
+// GMRES with iterative refinement: every restart cycle solves for the correction of the FP64
+// residual with FP32 operator applies and an FP32 Krylov basis (FP64 inner products, Hessenberg
+// and rotations), then updates x and recomputes the true residual in FP64.  Stopping rules and
+// reported quantities are those of gmres_solve.
+int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
+                   cudaStream_t st) {
+  const int64_t n = s.n;
+  const int m = s.restart;
+  double* w64 = s.work;
+  double* r64 = s.work + n;
+  const int64_t ld = ir_stride(n);
+  float* w32 = reinterpret_cast<float*>(s.work + 2 * n);
+  float* V = w32 + ld;  // m + 1 FP32 basis vectors, stride ld
+  double* pa = s.partials;
+  double* pb = s.partials + kRB;
+  double* H = s.small;
+  double* csv = H + (m + 1) * m;
+  double* snv = csv + m;
+  double* e1 = snv + m;
+  double* y = e1 + m + 1;
+  GMState* gs = static_cast<GMState*>(s.state);
+  const int* done = &gs->done;
+  const int* inactive = &gs->inactive;
+  auto residual = [&](int phase) -> int {
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, 0, st, done));
+    k_sub_norm<<<kRB, kRT, 0, st>>>(b, w64, r64, n, pa, done);
+    k_gm_resid<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters, phase);
+    DGOP_CUDA_S(cudaGetLastError());
+    return DGOP_OK;
+  };
+  k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
+  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
+  DGOP_CUDA_S(cudaGetLastError());
+  if (max_iters <= 0 || m <= 0) {
+    DGOP_TRY(residual(2));
+  } else {
+    DGOP_TRY(residual(0));
+    for (int cycle = 0; cycle <= max_iters; ++cycle) {
+      int d = 0;
+      DGOP_TRY(read_done(s, st, &d));
+      if (d) break;
+      k_gm_cycle_start<<<1, 1, 0, st>>>(gs, csv, snv, e1, y, m, max_iters);
+      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, r64, V, n, -1);  // V0 = r / |r| in FP32
+      for (int j = 0; j < m; ++j) {
+        float* vj = V + (int64_t)j * ld;
+        DGOP_TRY(launch_f32(s.op, 1.0f, vj, 0.0f, w32, kLinear, st, inactive));
+        k_dot<<<kRB, kRT, 0, st>>>(static_cast<const float*>(V), static_cast<const float*>(w32), n, pa, inactive);
+        double* pin = pa;
+        double* pout = pb;
+        for (int i = 0; i <= j; ++i) {
+          const float* next = (i < j) ? V + (int64_t)(i + 1) * ld : w32;
+          k_gm_mgs<<<kRB, kRT, 0, st>>>(gs, i, j, m, static_cast<const float*>(V + (int64_t)i * ld), next, w32, n, H,
+                                       pin, pout);
+          std::swap(pin, pout);
+        }
+        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
+        k_gm_scale<<<kRB, kRT, 0, st>>>(gs, static_cast<const float*>(w32), V + (int64_t)(j + 1) * ld, n, j);
+        DGOP_CUDA_S(cudaGetLastError());
+      }
+      k_gm_backsub<<<1, 1, 0, st>>>(gs, H, e1, y, m);
+      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, static_cast<const float*>(V), ld, y, n);
+      DGOP_TRY(residual(1));
+    }
+  }
+  GMState h;
+  DGOP_CUDA_S(cudaMemcpyAsync(&h, gs, sizeof(h), cudaMemcpyDeviceToHost, st));
+  DGOP_CUDA_S(cudaStreamSynchronize(st));
+  res->success = h.success;
+  res->iterations = h.iters;
+  res->relative_error = h.rel;
+  return DGOP_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int dgop_gmres_ir_create(dgop_operator* op, int restart, dgop_solver** out) {
+  if (!op || !out || restart < 1 || restart > 1000) {
+    set_error("dgop_gmres_ir_create: null argument or restart outside [1, 1000]");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  if (!op->f32.ready && !op->k32.ready) {
+    set_error("dgop_gmres_ir_create: the operator has no FP32 kernel");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  auto* sv = new (std::nothrow) dgop_solver();
+  if (!sv) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  sv->s.kind = 2;
+  sv->s.op = op;
+  sv->s.n = op->sp.ndofs;
+  sv->s.restart = restart;
+  const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
+  // two FP64 vectors, then m + 2 FP32 vectors (w and the basis) with a 256-byte aligned stride
+  const size_t words = 2 * (size_t)sv->s.n + (size_t)(restart + 2) * (size_t)(ir_stride(sv->s.n) / 2);
+  const int rc = solver_alloc(sv, words, sizeof(GMState), small);
+  if (rc != DGOP_OK) {
+    solver_free(sv);
+    delete sv;
+    return rc;
+  }
+  *out = sv;
+  return DGOP_OK;
+}
 
 int dgop_cg_create(dgop_operator* op, dgop_solver** out) {
   if (!op || !out) {
@@ -547,7 +660,7 @@ int dgop_cg_create(dgop_operator* op, dgop_solver** out) {
   sv->s.kind = 0;
   sv->s.op = op;
   sv->s.n = op->sp.ndofs;
-  const int rc = solver_alloc(sv, 3, sizeof(CGState), 0);
+  const int rc = solver_alloc(sv, 3 * (size_t)sv->s.n, sizeof(CGState), 0);
   if (rc != DGOP_OK) {
     solver_free(sv);
     delete sv;
@@ -573,7 +686,7 @@ int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out) {
   sv->s.n = op->sp.ndofs;
   sv->s.restart = restart;
   const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
-  const int rc = solver_alloc(sv, restart + 2, sizeof(GMState), small);
+  const int rc = solver_alloc(sv, (size_t)(restart + 2) * sv->s.n, sizeof(GMState), small);
   if (rc != DGOP_OK) {
     solver_free(sv);
     delete sv;
@@ -594,8 +707,9 @@ int dgop_solver_solve(dgop_solver* sv, const double* b, double* x, int max_iters
     return DGOP_ERR_ARG;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  return sv->s.kind == 0 ? cg_solve(sv->s, b, x, max_iters, tol, result, st)
-                         : gmres_solve(sv->s, b, x, max_iters, tol, result, st);
+  if (sv->s.kind == 0) return cg_solve(sv->s, b, x, max_iters, tol, result, st);
+  if (sv->s.kind == 2) return gmres_ir_solve(sv->s, b, x, max_iters, tol, result, st);
+  return gmres_solve(sv->s, b, x, max_iters, tol, result, st);
 }
 
 int dgop_solver_destroy(dgop_solver* sv) {

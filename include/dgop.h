@@ -116,6 +116,14 @@ typedef struct {
 typedef struct dgop_solver dgop_solver;
 int dgop_cg_create(dgop_operator* op, dgop_solver** out);
 int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out);
+/* GMRES(restart) with mixed-precision inner cycles (no reference counterpart; it replaces
+ * GMRES_no_alloc, Solvers/gmres.hpp:74, where FP32 operator throughput is wanted): each restart
+ * cycle runs the Arnoldi process on the correction equation A d = r with FP32 operator applies
+ * and an FP32 basis (inner products, Hessenberg matrix and rotations in FP64), then x += d and
+ * the residual r = b - A x is recomputed with the FP64 operator.  The stopping test, iteration
+ * count and `relative_error` are those of dgop_gmres_create's solver; the attainable accuracy is
+ * the FP64 one because refinement uses the FP64 residual.  Needs an FP32 kernel for `op`. */
+int dgop_gmres_ir_create(dgop_operator* op, int restart, dgop_solver** out);
 int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_iters, double tol,
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);

@@ -111,3 +111,55 @@ def test_cg_zero_rhs_returns_zero():
     info = g.CGSolver(op).solve(b, torch.zeros_like(b), 10, 1e-10)
     assert info == {"success": True, "iterations": 0, "relative_error": 0.0}
     del x
+
+
+def _true_rel_residual(op, b, x):
+    ax = torch.empty_like(x)
+    op(x, ax)
+    return (torch.linalg.vector_norm(b - ax) / torch.linalg.vector_norm(b)).item()
+
+
+IR_CASES = [
+    # (id, case, restart): the bench system at 8^3, an inflow value g != 0 (the inner FP32 cycles
+    # must use the linear part), and an odd-sized generic-kernel mesh (FP32 vector stride padding)
+    ("sincos_8cubed", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [8] * 3, "h": [1 / 8] * 3, "origin": [0.0] * 3,
+                       "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "sigma_c": 1e3}, 30),
+    ("inflow_g", {"D": 3, "P": 2, "Q": 3, "basis": 0, "sizes": [6, 5, 4], "h": [1 / 6, 1 / 5, 1 / 4],
+                  "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 1, "g": 0.75, "sigma_c": 50.0}, 20),
+    ("odd_2d_p4", {"D": 2, "P": 4, "Q": 5, "basis": 0, "sizes": [7, 9], "h": [1 / 7, 1 / 9], "origin": [0.0] * 2,
+                   "periodic": [0] * 2, "beta_kind": 0, "beta_c": [0.7, -0.4], "g": 0.0, "sigma_c": 20.0}, 15),
+]
+
+
+@pytest.mark.parametrize("kernel", ["generic", "kron"])
+@pytest.mark.parametrize("cid,case,restart", IR_CASES, ids=[c[0] for c in IR_CASES])
+def test_gmres_ir_reaches_fp64_accuracy(cid, case, restart, kernel):
+    sp = make_space(case)
+    op = _system(case, sp)
+    if kernel == "kron" and op.kernel != "kron":
+        pytest.skip(op.kernel_note)
+    if kernel == "generic" and op.kernel != "generic":
+        op.select_kernel("generic")
+    b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 5)).cuda()
+    x64 = torch.zeros_like(b)
+    ref = g.GMRESSolver(op, restart).solve(b, x64, 5000, 1e-11)
+    x = torch.zeros_like(b)
+    info = g.GMRESIRSolver(op, restart).solve(b, x, 5000, 1e-11)
+    assert ref["success"] and info["success"], (ref, info)
+    # refinement recomputes the residual in FP64: the reported and the true residual meet the tolerance
+    assert info["relative_error"] <= 1e-11
+    assert _true_rel_residual(op, b, x) <= 1.01e-11
+    assert rel_max(x.cpu().numpy(), x64.cpu().numpy()) < 1e-8
+    # FP32 cycles lose at most a few cycles against the FP64 solver
+    assert info["iterations"] <= 2 * ref["iterations"] + 2 * restart, (info, ref)
+
+
+def test_gmres_ir_max_iters_reported_as_failure():
+    case = IR_CASES[0][1]
+    sp = make_space(case)
+    op = _system(case, sp)
+    b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 2)).cuda()
+    x = torch.zeros_like(b)
+    info = g.GMRESIRSolver(op, 5).solve(b, x, 7, 1e-14)
+    assert not info["success"] and info["iterations"] == 7
+    assert abs(info["relative_error"] - _true_rel_residual(op, b, x)) <= 1e-9
