@@ -87,7 +87,7 @@ def lib():
         L.dgop_operator_select_kernel.argtypes = [vp, i]
         L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
-        L.dgop_gmres_ir_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
         L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
         L.dgop_solver_destroy.argtypes = [vp]
         _lib = L
@@ -343,14 +343,16 @@ class GMRESSolver(_Solver):
 
 
 class GMRESIRSolver(_Solver):
-    """GMRES(restart) whose restart cycles run in FP32 (operator and basis) on the correction
-    equation, with the residual and the solution updated in FP64 (iterative refinement).  Same
-    solve() contract and stopping test as GMRESSolver; no reference counterpart."""
+    """GMRES(restart) with iterative refinement: restart cycles solve the correction equation
+    with operator applies and a Krylov basis in `inner` precision ("fp32" or "fp64"), the residual
+    and the solution are updated in FP64.  Same solve() contract and stopping test as
+    GMRESSolver; no reference counterpart."""
 
-    def __init__(self, op, restart=30):
+    def __init__(self, op, restart=30, inner="fp32"):
         super().__init__(op)
+        prec = {"fp32": 1, "fp64": 0}[inner]
         h = ctypes.c_void_p()
-        check(lib().dgop_gmres_ir_create(op.handle, int(restart), ctypes.byref(h)))
+        check(lib().dgop_gmres_ir_create(op.handle, int(restart), prec, ctypes.byref(h)))
         self.handle = h
 
 

@@ -5,6 +5,10 @@
 Objects go to ``gendil_b200/_build/<variant>/``; each object is rebuilt only when its source,
 the package headers or the flags change.  ``--fast`` (or DGOP_FAST_BUILD=1) compiles only the
 (dimension, order, quadrature) shapes the tests and benchmark workloads use.
+
+Every unit is compiled for sm_100a.  The hot-path units (Kronecker kernel, Krylov kernels, C ABI)
+and the fast build carry -lineinfo; the full build's generic instantiation units (several hundred
+kernels) do not, which keeps the library about three times smaller.
 """
 from __future__ import annotations
 
@@ -23,7 +27,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libdgop.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-BASE_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+BASE_FLAGS = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 # Non-instantiation sources; gen_generic.cu is compiled once per (dimension, N).
@@ -76,6 +80,8 @@ def build(fast=None, jobs=None, clean=False, verbose=False):
 
     def compile_one(job):
         name, src, extra = job
+        if fast or not name.startswith("gen_generic"):
+            extra = ["-lineinfo"] + extra
         obj = os.path.join(out_dir, name.rsplit(".", 1)[0] + ".o")
         stamp = obj + ".sha"
         h = hashlib.sha256()

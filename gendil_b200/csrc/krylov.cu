@@ -365,6 +365,125 @@ __global__ void __launch_bounds__(kRT) k_gm_update(const GMState* st, double* __
   }
 }
 
+// ---------------------------------------------- GMRES with iterative refinement (inner basis)
+
+constexpr int kGsChunk = 8;     // basis vectors per block row of the projection pass
+constexpr int kGsMaxRestart = 1000;
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int L = 4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int L = 2;
+};
+
+// wide[i * kRB + block] <- partial (V_i, w) for i <= j (blockIdx.y selects kGsChunk vectors);
+// 128-bit accesses over the padded stride, products and sums in FP64
+template <typename T>
+__global__ void __launch_bounds__(kRT) k_gs_dots(const GMState* st, const T* __restrict__ V, int64_t ld, int j,
+                                                 const T* __restrict__ w, double* wide) {
+  if (st->inactive) return;
+  using V16 = typename Vec16<T>::type;
+  constexpr int L = Vec16<T>::L;
+  const int i0 = blockIdx.y * kGsChunk;
+  const int cnt = min(kGsChunk, j + 1 - i0);
+  double acc[kGsChunk];
+#pragma unroll
+  for (int c = 0; c < kGsChunk; ++c) acc[c] = 0.0;
+  const int64_t nv = ld / L;
+  const V16* w16 = reinterpret_cast<const V16*>(w);
+  const V16* v16 = reinterpret_cast<const V16*>(V + (int64_t)i0 * ld);
+  const int64_t ldv = ld / L;
+  DGOP_GRID_LOOP(u, nv) {
+    T wv[L];
+    *reinterpret_cast<V16*>(wv) = w16[u];
+#pragma unroll
+    for (int c = 0; c < kGsChunk; ++c) {
+      if (c < cnt) {
+        T vv[L];
+        *reinterpret_cast<V16*>(vv) = v16[c * ldv + u];
+#pragma unroll
+        for (int k = 0; k < L; ++k) acc[c] += (double)vv[k] * (double)wv[k];
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kGsChunk; ++c)
+    if (c < cnt) write_partial(wide + (int64_t)(i0 + c) * kRB, acc[c]);
+}
+
+// H(i, j) <- (V_i, w), one block per i, partials summed in the fixed order
+__global__ void __launch_bounds__(kRT) k_gs_h(const GMState* st, int j, int m, double* H, const double* wide) {
+  if (st->inactive) return;
+  const int i = blockIdx.x;
+  const double h = reduce_partials(wide + (int64_t)i * kRB);
+  if (threadIdx.x == 0) H[j * (m + 1) + i] = h;
+}
+
+// out <- w - sum_{i <= j} H(i, j) V_i (formed in FP64, stored as T); partials <- |out|^2
+template <typename T>
+__global__ void __launch_bounds__(kRT) k_gs_update(const GMState* st, const T* __restrict__ V, int64_t ld, int j,
+                                                   int m, const double* H, const T* __restrict__ w,
+                                                   T* __restrict__ out, double* partials) {
+  if (st->inactive) return;
+  using V16 = typename Vec16<T>::type;
+  constexpr int L = Vec16<T>::L;
+  __shared__ double hs[kGsMaxRestart];
+  for (int i = threadIdx.x; i <= j; i += kRT) hs[i] = H[j * (m + 1) + i];
+  __syncthreads();
+  const int64_t nv = ld / L, ldv = ld / L;
+  const V16* w16 = reinterpret_cast<const V16*>(w);
+  const V16* v16 = reinterpret_cast<const V16*>(V);
+  V16* o16 = reinterpret_cast<V16*>(out);
+  double sq = 0.0;
+  DGOP_GRID_LOOP(u, nv) {
+    T wv[L];
+    *reinterpret_cast<V16*>(wv) = w16[u];
+    double a[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) a[k] = (double)wv[k];
+#pragma unroll 4
+    for (int i = 0; i <= j; ++i) {
+      T vv[L];
+      *reinterpret_cast<V16*>(vv) = v16[(int64_t)i * ldv + u];
+      const double h = hs[i];
+#pragma unroll
+      for (int k = 0; k < L; ++k) a[k] -= h * (double)vv[k];
+    }
+    T ov[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+      ov[k] = (T)a[k];
+      sq += (double)ov[k] * (double)ov[k];
+    }
+    o16[u] = *reinterpret_cast<V16*>(ov);
+  }
+  write_partial(partials, sq);
+}
+
+// v <- v * (1 / H(j + 1, j)) in place, when iteration j ran and did not end the cycle
+template <typename T>
+__global__ void __launch_bounds__(kRT) k_gs_rescale(const GMState* st, T* v, int64_t ld, int j) {
+  if (st->done || st->brk || st->k != j + 1) return;
+  using V16 = typename Vec16<T>::type;
+  constexpr int L = Vec16<T>::L;
+  const double sc = st->inv_h;
+  V16* v16 = reinterpret_cast<V16*>(v);
+  DGOP_GRID_LOOP(u, ld / L) {
+    T a[L];
+    *reinterpret_cast<V16*>(a) = v16[u];
+#pragma unroll
+    for (int k = 0; k < L; ++k) a[k] = (T)((double)a[k] * sc);
+    v16[u] = *reinterpret_cast<V16*>(a);
+  }
+}
+
 }  // namespace
 
 struct SolverImpl {
@@ -377,6 +496,8 @@ struct SolverImpl {
   void* state = nullptr;       // CGState / GMState (device)
   double* small = nullptr;     // GMRES: H, cs, sn, e1, y
   int* h_flag = nullptr;       // pinned host copy of `done`
+  int inner = 0;               // refinement solver: DGOP_FP32 or DGOP_FP64 inner cycles
+  double* wide = nullptr;      // refinement solver: (restart + 1) x kRB projection partials
 };
 
 }  // namespace dgop
@@ -414,6 +535,7 @@ void solver_free(dgop_solver* sv) {
   if (s.state) cudaFree(s.state);
   if (s.small) cudaFree(s.small);
   if (s.h_flag) cudaFreeHost(s.h_flag);
+  if (s.wide) cudaFree(s.wide);
   s = SolverImpl{};
 }
 
@@ -534,24 +656,37 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   return DGOP_OK;
 }
 
-// FP32 vector stride of the mixed-precision workspace: n rounded up to 64 floats (256 bytes)
+// Vector stride of the refinement solver's inner workspace: n rounded up to 64 entries
+// (256 bytes for FP32), so every inner vector starts 16-byte aligned for 128-bit accesses.
+// The padding entries are zero from creation on and stay zero.
 int64_t ir_stride(int64_t n) { return (n + 63) / 64 * 64; }
 
-// GMRES with iterative refinement: every restart cycle solves for the correction of the FP64
-// residual with FP32 operator applies and an FP32 Krylov basis (FP64 inner products, Hessenberg
-// and rotations), then updates x and recomputes the true residual in FP64.  Stopping rules and
-// reported quantities are those of gmres_solve.
+int apply_inner(dgop_operator* op, const float* x, float* y, cudaStream_t st, const int* skip) {
+  return launch_f32(op, 1.0f, x, 0.0f, y, kLinear, st, skip);
+}
+int apply_inner(dgop_operator* op, const double* x, double* y, cudaStream_t st, const int* skip) {
+  return launch_f64(op, 1.0, x, 0.0, y, kLinear, st, skip);
+}
+
+// GMRES with iterative refinement: every restart cycle solves the correction equation A d = r
+// for the FP64 residual r with inner operator applies and an inner Krylov basis of type T
+// (inner products, Hessenberg matrix and rotations in FP64), then x += d in FP64 and the true
+// residual is recomputed with the FP64 operator.  The Arnoldi step is classical Gram-Schmidt
+// fused into two passes (all projections of w in one pass, the update of w and its norm in the
+// next) instead of the reference's j + 1 modified Gram-Schmidt sweeps; the FP64 residual of the
+// refinement loop bounds the effect of the weaker orthogonality.  Stopping rules and reported
+// quantities are those of gmres_solve.
+template <typename T>
 int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
                    cudaStream_t st) {
   const int64_t n = s.n;
   const int m = s.restart;
+  const int64_t ld = ir_stride(n);
   double* w64 = s.work;
   double* r64 = s.work + n;
-  const int64_t ld = ir_stride(n);
-  float* w32 = reinterpret_cast<float*>(s.work + 2 * n);
-  float* V = w32 + ld;  // m + 1 FP32 basis vectors, stride ld
+  T* w = reinterpret_cast<T*>(s.work + 2 * n);
+  T* V = w + ld;  // m + 1 inner basis vectors, stride ld
   double* pa = s.partials;
-  double* pb = s.partials + kRB;
   double* H = s.small;
   double* csv = H + (m + 1) * m;
   double* snv = csv + m;
@@ -579,25 +714,21 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
       DGOP_TRY(read_done(s, st, &d));
       if (d) break;
       k_gm_cycle_start<<<1, 1, 0, st>>>(gs, csv, snv, e1, y, m, max_iters);
-      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, r64, V, n, -1);  // V0 = r / |r| in FP32
+      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, static_cast<const double*>(r64), V, n, -1);  // V0 = r / |r|
       for (int j = 0; j < m; ++j) {
-        float* vj = V + (int64_t)j * ld;
-        DGOP_TRY(launch_f32(s.op, 1.0f, vj, 0.0f, w32, kLinear, st, inactive));
-        k_dot<<<kRB, kRT, 0, st>>>(static_cast<const float*>(V), static_cast<const float*>(w32), n, pa, inactive);
-        double* pin = pa;
-        double* pout = pb;
-        for (int i = 0; i <= j; ++i) {
-          const float* next = (i < j) ? V + (int64_t)(i + 1) * ld : w32;
-          k_gm_mgs<<<kRB, kRT, 0, st>>>(gs, i, j, m, static_cast<const float*>(V + (int64_t)i * ld), next, w32, n, H,
-                                       pin, pout);
-          std::swap(pin, pout);
-        }
-        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
-        k_gm_scale<<<kRB, kRT, 0, st>>>(gs, static_cast<const float*>(w32), V + (int64_t)(j + 1) * ld, n, j);
+        T* vj = V + (int64_t)j * ld;
+        T* vn = vj + ld;
+        DGOP_TRY(apply_inner(s.op, vj, w, st, inactive));
+        const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
+        k_gs_dots<T><<<dgrid, kRT, 0, st>>>(gs, V, ld, j, w, s.wide);
+        k_gs_h<<<j + 1, kRT, 0, st>>>(gs, j, m, H, s.wide);
+        k_gs_update<T><<<kRB, kRT, 0, st>>>(gs, V, ld, j, m, H, w, vn, pa);
+        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pa, tol, max_iters);
+        k_gs_rescale<T><<<kRB, kRT, 0, st>>>(gs, vn, ld, j);
         DGOP_CUDA_S(cudaGetLastError());
       }
       k_gm_backsub<<<1, 1, 0, st>>>(gs, H, e1, y, m);
-      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, static_cast<const float*>(V), ld, y, n);
+      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, static_cast<const T*>(V), ld, y, n);
       DGOP_TRY(residual(1));
     }
   }
@@ -614,13 +745,17 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
 
 extern "C" {
 
-int dgop_gmres_ir_create(dgop_operator* op, int restart, dgop_solver** out) {
-  if (!op || !out || restart < 1 || restart > 1000) {
+int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dgop_solver** out) {
+  if (!op || !out || restart < 1 || restart > kGsMaxRestart) {
     set_error("dgop_gmres_ir_create: null argument or restart outside [1, 1000]");
     return DGOP_ERR_ARG;
   }
   *out = nullptr;
-  if (!op->f32.ready && !op->k32.ready) {
+  if (inner_precision != DGOP_FP32 && inner_precision != DGOP_FP64) {
+    set_error("dgop_gmres_ir_create: inner_precision must be DGOP_FP32 or DGOP_FP64");
+    return DGOP_ERR_ARG;
+  }
+  if (inner_precision == DGOP_FP32 && !op->f32.ready && !op->k32.ready) {
     set_error("dgop_gmres_ir_create: the operator has no FP32 kernel");
     return DGOP_ERR_UNSUPPORTED;
   }
@@ -629,14 +764,23 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, dgop_solver** out) {
     set_error("host allocation failed");
     return DGOP_ERR_ALLOC;
   }
-  sv->s.kind = 2;
-  sv->s.op = op;
-  sv->s.n = op->sp.ndofs;
-  sv->s.restart = restart;
+  SolverImpl& s = sv->s;
+  s.kind = 2;
+  s.inner = inner_precision;
+  s.op = op;
+  s.n = op->sp.ndofs;
+  s.restart = restart;
   const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
-  // two FP64 vectors, then m + 2 FP32 vectors (w and the basis) with a 256-byte aligned stride
-  const size_t words = 2 * (size_t)sv->s.n + (size_t)(restart + 2) * (size_t)(ir_stride(sv->s.n) / 2);
-  const int rc = solver_alloc(sv, words, sizeof(GMState), small);
+  // two FP64 vectors (A x, residual), then restart + 2 inner vectors (w and the basis) at stride
+  // ir_stride(n); the padding entries must read as zero, so the workspace starts zeroed
+  const size_t inner_words = (size_t)ir_stride(s.n) * (inner_precision == DGOP_FP32 ? 4 : 8) / 8;
+  const size_t words = 2 * (size_t)s.n + (size_t)(restart + 2) * inner_words;
+  int rc = solver_alloc(sv, words, sizeof(GMState), small);
+  if (rc == DGOP_OK) {
+    cudaError_t e = cudaMemset(s.work, 0, sizeof(double) * words);
+    if (e == cudaSuccess) e = cudaMalloc(&s.wide, sizeof(double) * (size_t)(restart + 1) * kRB);
+    if (e != cudaSuccess) rc = cuda_fail(e, "dgop_gmres_ir_create workspace");
+  }
   if (rc != DGOP_OK) {
     solver_free(sv);
     delete sv;
@@ -708,7 +852,9 @@ int dgop_solver_solve(dgop_solver* sv, const double* b, double* x, int max_iters
   }
   cudaStream_t st = (cudaStream_t)stream;
   if (sv->s.kind == 0) return cg_solve(sv->s, b, x, max_iters, tol, result, st);
-  if (sv->s.kind == 2) return gmres_ir_solve(sv->s, b, x, max_iters, tol, result, st);
+  if (sv->s.kind == 2)
+    return sv->s.inner == DGOP_FP32 ? gmres_ir_solve<float>(sv->s, b, x, max_iters, tol, result, st)
+                                    : gmres_ir_solve<double>(sv->s, b, x, max_iters, tol, result, st);
   return gmres_solve(sv->s, b, x, max_iters, tol, result, st);
 }
 

@@ -88,7 +88,9 @@ int dgop_operator_kernel(const dgop_operator* op);
 const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);
 
-/* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers.
+/* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers, aligned to their
+ * element size; the Kronecker-form kernel runs on 16-byte aligned vectors (any cudaMalloc'd or
+ * torch-allocated tensor), other alignments take the generic kernel.
  * (MassFiniteElementOperator::operator() massoperator.hpp:209, AdvectionOperator::operator()
  * advectionoperator.hpp:1070: both overwrite y.) */
 int dgop_apply(dgop_operator* op, const double* x, double* y, void* stream);
@@ -116,14 +118,16 @@ typedef struct {
 typedef struct dgop_solver dgop_solver;
 int dgop_cg_create(dgop_operator* op, dgop_solver** out);
 int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out);
-/* GMRES(restart) with mixed-precision inner cycles (no reference counterpart; it replaces
- * GMRES_no_alloc, Solvers/gmres.hpp:74, where FP32 operator throughput is wanted): each restart
- * cycle runs the Arnoldi process on the correction equation A d = r with FP32 operator applies
- * and an FP32 basis (inner products, Hessenberg matrix and rotations in FP64), then x += d and
- * the residual r = b - A x is recomputed with the FP64 operator.  The stopping test, iteration
- * count and `relative_error` are those of dgop_gmres_create's solver; the attainable accuracy is
- * the FP64 one because refinement uses the FP64 residual.  Needs an FP32 kernel for `op`. */
-int dgop_gmres_ir_create(dgop_operator* op, int restart, dgop_solver** out);
+/* GMRES(restart) with iterative refinement (no reference counterpart; it replaces
+ * GMRES_no_alloc, Solvers/gmres.hpp:74, where inner-precision throughput is wanted): each restart
+ * cycle runs the Arnoldi process on the correction equation A d = r with operator applies and a
+ * Krylov basis in `inner_precision` (DGOP_FP32 or DGOP_FP64; inner products, Hessenberg matrix and
+ * rotations always FP64, Gram-Schmidt in classical form fused into two vector passes), then
+ * x += d and the residual r = b - A x are formed with the FP64 operator.  The stopping test,
+ * iteration count and `relative_error` are those of dgop_gmres_create's solver, and the attainable
+ * accuracy is the FP64 one because the refinement uses the FP64 residual.  The inner applies use
+ * the linear part of the operator (inflow value 0).  DGOP_FP32 needs an FP32 kernel for `op`. */
+int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dgop_solver** out);
 int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_iters, double tol,
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);
