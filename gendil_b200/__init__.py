@@ -88,6 +88,7 @@ def lib():
         L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
+        L.dgop_solver_set_graphs.argtypes = [vp, i]
         L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
         L.dgop_solver_destroy.argtypes = [vp]
         _lib = L
@@ -309,6 +310,11 @@ class _Solver:
         check(lib().dgop_solver_solve(self.handle, _ptr(b), _ptr(x), int(max_iters), float(tol), ctypes.byref(res),
                                       _stream(stream)))
         return {"success": bool(res.success), "iterations": res.iterations, "relative_error": res.relative_error}
+
+    def use_graphs(self, enable=True):
+        """Replay solver segments from CUDA graphs (default) or launch every kernel directly."""
+        check(lib().dgop_solver_set_graphs(self.handle, 1 if enable else 0))
+        return self
 
     def close(self):
         if self.handle:

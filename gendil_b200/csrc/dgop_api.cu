@@ -732,6 +732,7 @@ int dgop_operator_select_kernel(dgop_operator* op, int kernel) {
     return DGOP_ERR_UNSUPPORTED;
   }
   op->kernel = kernel;
+  ++op->version;
   return DGOP_OK;
 }
 

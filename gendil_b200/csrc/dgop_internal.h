@@ -62,6 +62,7 @@ struct dgop_operator {
   int device = 0;
   int kernel = 0;             // DGOP_KERNEL_GENERIC or DGOP_KERNEL_KRON
   const char* kron_why = "";  // why the Kronecker form is unavailable
+  int version = 0;            // bumped whenever the launch configuration changes
   dgop::LaunchCfg<double> f64;
   dgop::LaunchCfg<float> f32;
   dgop::KronCfg<double> k64;

@@ -26,7 +26,7 @@ namespace {
 
 constexpr int kRB = 592;  // reduction blocks (4 per SM on 148 SMs)
 constexpr int kRT = 256;  // threads per reduction block
-constexpr int kCheckEvery = 8;
+constexpr int kCheckEvery = 8;  // CG iterations per chunk (even)
 
 // Sum over the block in a fixed order; the result is valid in thread 0.
 __device__ __forceinline__ double block_sum(double v) {
@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kRT) k_sub_norm(const double* __restrict__ b, 
 
 struct CGState {
   int done, success, iters, zero_x;
+  int base, pad_[3];  // iteration index of the current chunk's first iteration
   double rhs_n, r_n, rel;
   double abs_[2];  // (r, r) by iteration parity
 };
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(kRT) k_cg_init(CGState* st, const double* part
   st->success = 0;
   st->iters = 0;
   st->zero_x = 0;
+  st->base = 0;
   const double rhs_n = sqrt(R);  // the "rhs norm" is the norm of the initial residual
   st->rhs_n = rhs_n;
   if (rhs_n == 0.0 || rhs_n < 1e-30) {
@@ -134,12 +136,16 @@ __global__ void __launch_bounds__(kRT) k_cg_init_p(const CGState* st, const doub
   }
 }
 
+// Iterations run in chunks of kCheckEvery; iteration kk of a chunk is iteration st->base + kk
+// of the solve (kCheckEvery is even, so the parity of the two agrees).
+
 // alpha = (r, r) / (p, A p); x += alpha p; r -= alpha A p; partials2 <- |r|^2   (:176-181)
-__global__ void __launch_bounds__(kRT) k_cg_update(int k, const CGState* st, double* __restrict__ x,
+__global__ void __launch_bounds__(kRT) k_cg_update(int kk, const CGState* st, double* __restrict__ x,
                                                    double* __restrict__ r, const double* __restrict__ p,
                                                    const double* __restrict__ ap, int64_t n, const double* partials1,
                                                    double* partials2) {
   if (st->done) return;
+  const int k = st->base + kk;
   const double alpha = st->abs_[k & 1] / reduce_partials(partials1);
   double v = 0.0;
   DGOP_GRID_LOOP(i, n) {
@@ -152,10 +158,11 @@ __global__ void __launch_bounds__(kRT) k_cg_update(int k, const CGState* st, dou
 }
 
 // stopping test, beta = (r_new, r_new) / (r_old, r_old), p = beta p + r   (:183-205)
-__global__ void __launch_bounds__(kRT) k_cg_finish(int k, CGState* st, const double* __restrict__ r,
+__global__ void __launch_bounds__(kRT) k_cg_finish(int kk, CGState* st, const double* __restrict__ r,
                                                    double* __restrict__ p, int64_t n, const double* partials2,
                                                    double tol, int max_iters) {
   if (st->done) return;
+  const int k = st->base + kk;
   const double R = reduce_partials(partials2);
   const double r_n = sqrt(R);
   const double rhs_n = st->rhs_n;
@@ -181,6 +188,11 @@ __global__ void __launch_bounds__(kRT) k_cg_finish(int k, CGState* st, const dou
       st->done = 1;
     }
   }
+}
+
+// end of a chunk: the next chunk starts kCheckEvery iterations later
+__global__ void k_cg_next_chunk(CGState* st) {
+  if (!st->done) st->base += kCheckEvery;
 }
 
 // max_iters == 0 without early exit: the loop does not run (:207-208)
@@ -495,9 +507,20 @@ struct SolverImpl {
   double* partials = nullptr;  // 2 x kRB
   void* state = nullptr;       // CGState / GMState (device)
   double* small = nullptr;     // GMRES: H, cs, sn, e1, y
-  int* h_flag = nullptr;       // pinned host copy of `done`
+  int* h_flag = nullptr;       // host copies of `done`, one per segment parity (pinned)
   int inner = 0;               // refinement solver: DGOP_FP32 or DGOP_FP64 inner cycles
   double* wide = nullptr;      // refinement solver: (restart + 1) x kRB projection partials
+  // Segments (a CG chunk, a GMRES cycle) are replayed from one CUDA graph, captured for the
+  // current (b, x, tol, max_iters, operator version) and re-captured when any of them changes.
+  bool use_graphs = true;
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void* key_b = nullptr;
+  const void* key_x = nullptr;
+  double key_tol = 0.0;
+  int key_iters = -1, key_version = -1;
+  // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
+  cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
 }  // namespace dgop
@@ -516,6 +539,12 @@ namespace {
     if (_e != cudaSuccess) return cuda_fail(_e, #call); \
   } while (0)
 
+#define DGOP_TRY(call)             \
+  do {                             \
+    const int _rc = (call);        \
+    if (_rc != DGOP_OK) return _rc; \
+  } while (0)
+
 // `words`: FP64 words of vector workspace
 int solver_alloc(dgop_solver* sv, size_t words, size_t state_bytes, size_t small_count) {
   SolverImpl& s = sv->s;
@@ -524,7 +553,8 @@ int solver_alloc(dgop_solver* sv, size_t words, size_t state_bytes, size_t small
   DGOP_CUDA_S(cudaMalloc(&s.state, state_bytes));
   DGOP_CUDA_S(cudaMemset(s.state, 0, state_bytes));
   if (small_count) DGOP_CUDA_S(cudaMalloc(&s.small, sizeof(double) * small_count));
-  DGOP_CUDA_S(cudaMallocHost(&s.h_flag, sizeof(int)));
+  DGOP_CUDA_S(cudaMallocHost(&s.h_flag, 2 * sizeof(int)));
+  for (auto& e : s.ev) DGOP_CUDA_S(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return DGOP_OK;
 }
 
@@ -536,21 +566,80 @@ void solver_free(dgop_solver* sv) {
   if (s.small) cudaFree(s.small);
   if (s.h_flag) cudaFreeHost(s.h_flag);
   if (s.wide) cudaFree(s.wide);
+  if (s.exec) cudaGraphExecDestroy(s.exec);
+  if (s.cap) cudaStreamDestroy(s.cap);
+  for (auto e : s.ev)
+    if (e) cudaEventDestroy(e);
   s = SolverImpl{};
 }
 
-int read_done(SolverImpl& s, cudaStream_t st, int* done) {
-  DGOP_CUDA_S(cudaMemcpyAsync(s.h_flag, s.state, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DGOP_CUDA_S(cudaStreamSynchronize(st));
-  *done = *s.h_flag;
+// Enqueues one segment on `st`: replays the cached graph, capturing it first when the key
+// changed, or launches directly when graphs are off.
+template <typename F>
+int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, double tol, int max_iters,
+                F&& enqueue) {
+  if (!s.use_graphs) return enqueue(st);
+  const bool same = s.exec && s.key_b == b && s.key_x == x && s.key_tol == tol && s.key_iters == max_iters &&
+                    s.key_version == s.op->version;
+  if (!same) {
+    if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
+    DGOP_CUDA_S(cudaStreamBeginCapture(s.cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue(s.cap);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s.cap, &graph);
+    if (rc != DGOP_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc != DGOP_OK ? rc : cuda_fail(e, "solver graph capture");
+    }
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+    s.exec = nullptr;
+    s.key_iters = -1;
+    const cudaError_t e2 = cudaGraphInstantiateWithFlags(&s.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+      s.exec = nullptr;
+      return cuda_fail(e2, "solver graph instantiation");
+    }
+    s.key_b = b;
+    s.key_x = x;
+    s.key_tol = tol;
+    s.key_iters = max_iters;
+    s.key_version = s.op->version;
+  }
+  DGOP_CUDA_S(cudaGraphLaunch(s.exec, st));
   return DGOP_OK;
 }
 
-#define DGOP_TRY(call)             \
-  do {                             \
-    const int _rc = (call);        \
-    if (_rc != DGOP_OK) return _rc; \
-  } while (0)
+// After segment `seg` was enqueued: starts the read of its `done` word and reports whether the
+// solve had finished by the end of segment seg - 1 (one segment of look-ahead, whose kernels are
+// no-ops once `done` is set).  Without events the read is synchronous and reports segment seg.
+int segment_done(SolverImpl& s, cudaStream_t st, int seg, bool* stop) {
+  int* flag = s.h_flag + (seg & 1);
+  DGOP_CUDA_S(cudaMemcpyAsync(flag, s.state, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!s.ev[0]) {
+    DGOP_CUDA_S(cudaStreamSynchronize(st));
+    *stop = *flag != 0;
+    return DGOP_OK;
+  }
+  DGOP_CUDA_S(cudaEventRecord(s.ev[seg & 1], st));
+  *stop = false;
+  if (seg > 0) {
+    DGOP_CUDA_S(cudaEventSynchronize(s.ev[(seg - 1) & 1]));
+    *stop = s.h_flag[(seg - 1) & 1] != 0;
+  }
+  return DGOP_OK;
+}
+
+template <typename State>
+int finish(SolverImpl& s, cudaStream_t st, dgop_solve_result* res) {
+  State h;
+  DGOP_CUDA_S(cudaMemcpyAsync(&h, s.state, sizeof(h), cudaMemcpyDeviceToHost, st));
+  DGOP_CUDA_S(cudaStreamSynchronize(st));
+  res->success = h.success;
+  res->iterations = h.iters;
+  res->relative_error = h.rel;
+  return DGOP_OK;
+}
 
 int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
              cudaStream_t st) {
@@ -569,25 +658,24 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
   if (max_iters <= 0) k_cg_no_iters<<<1, 1, 0, st>>>(cs);
   DGOP_CUDA_S(cudaGetLastError());
   const int* done = &cs->done;
-  for (int k = 0; k < max_iters; ++k) {
-    DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, 0, st, done));
-    k_dot<<<kRB, kRT, 0, st>>>(p, tmp, n, pa, done);
-    k_cg_update<<<kRB, kRT, 0, st>>>(k, cs, x, r, p, tmp, n, pa, pb);
-    k_cg_finish<<<kRB, kRT, 0, st>>>(k, cs, r, p, n, pb, tol, max_iters);
-    DGOP_CUDA_S(cudaGetLastError());
-    if ((k + 1) % kCheckEvery == 0) {
-      int d = 0;
-      DGOP_TRY(read_done(s, st, &d));
-      if (d) break;
+  auto chunk = [&](cudaStream_t q) -> int {
+    for (int kk = 0; kk < kCheckEvery; ++kk) {
+      DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, 0, q, done));
+      k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(p), static_cast<const double*>(tmp), n, pa, done);
+      k_cg_update<<<kRB, kRT, 0, q>>>(kk, cs, x, r, p, tmp, n, pa, pb);
+      k_cg_finish<<<kRB, kRT, 0, q>>>(kk, cs, r, p, n, pb, tol, max_iters);
     }
+    k_cg_next_chunk<<<1, 1, 0, q>>>(cs);
+    DGOP_CUDA_S(cudaGetLastError());
+    return DGOP_OK;
+  };
+  for (int c = 0; (int64_t)c * kCheckEvery < max_iters; ++c) {
+    DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, chunk));
+    bool stop = false;
+    DGOP_TRY(segment_done(s, st, c, &stop));
+    if (stop) break;
   }
-  CGState h;
-  DGOP_CUDA_S(cudaMemcpyAsync(&h, cs, sizeof(h), cudaMemcpyDeviceToHost, st));
-  DGOP_CUDA_S(cudaStreamSynchronize(st));
-  res->success = h.success;
-  res->iterations = h.iters;
-  res->relative_error = h.rel;
-  return DGOP_OK;
+  return finish<CGState>(s, st, res);
 }
 
 int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double tol, dgop_solve_result* res,
@@ -606,54 +694,52 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   GMState* gs = static_cast<GMState*>(s.state);
   const int* done = &gs->done;
   const int* inactive = &gs->inactive;
-  auto residual = [&](int phase) -> int {
-    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, 0, st, done));
-    k_sub_norm<<<kRB, kRT, 0, st>>>(b, w, V, n, pa, done);
-    k_gm_resid<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters, phase);
+  auto residual = [&](int phase, cudaStream_t q) -> int {
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, 0, q, done));
+    k_sub_norm<<<kRB, kRT, 0, q>>>(b, w, V, n, pa, done);
+    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, tol, max_iters, phase);
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
+  };
+  auto cycle = [&](cudaStream_t q) -> int {
+    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m, max_iters);
+    k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
+    for (int j = 0; j < m; ++j) {
+      double* vj = V + (int64_t)j * n;
+      DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, 0, q, inactive));
+      k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(V), static_cast<const double*>(w), n, pa, inactive);
+      double* pin = pa;
+      double* pout = pb;
+      for (int i = 0; i <= j; ++i) {
+        const double* next = (i < j) ? V + (int64_t)(i + 1) * n : w;
+        k_gm_mgs<<<kRB, kRT, 0, q>>>(gs, i, j, m, static_cast<const double*>(V + (int64_t)i * n), next, w, n, H,
+                                     pin, pout);
+        std::swap(pin, pout);
+      }
+      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
+      k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(w), V + (int64_t)(j + 1) * n, n, j);
+      DGOP_CUDA_S(cudaGetLastError());
+    }
+    k_gm_backsub<<<1, 1, 0, q>>>(gs, H, e1, y, m);
+    k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const double*>(V), n, y, n);
+    return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
   k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
   DGOP_CUDA_S(cudaGetLastError());
   if (max_iters <= 0 || m <= 0) {
-    DGOP_TRY(residual(2));
+    DGOP_TRY(residual(2, st));
   } else {
-    DGOP_TRY(residual(0));
+    DGOP_TRY(residual(0, st));
     // every cycle performs at least one iteration or finishes the solve
-    for (int cycle = 0; cycle <= max_iters; ++cycle) {
-      int d = 0;
-      DGOP_TRY(read_done(s, st, &d));
-      if (d) break;
-      k_gm_cycle_start<<<1, 1, 0, st>>>(gs, csv, snv, e1, y, m, max_iters);
-      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, V, V, n, -1);
-      for (int j = 0; j < m; ++j) {
-        double* vj = V + (int64_t)j * n;
-        DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, 0, st, inactive));
-        k_dot<<<kRB, kRT, 0, st>>>(V, w, n, pa, inactive);
-        double* pin = pa;
-        double* pout = pb;
-        for (int i = 0; i <= j; ++i) {
-          const double* next = (i < j) ? V + (int64_t)(i + 1) * n : w;
-          k_gm_mgs<<<kRB, kRT, 0, st>>>(gs, i, j, m, V + (int64_t)i * n, next, w, n, H, pin, pout);
-          std::swap(pin, pout);
-        }
-        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
-        k_gm_scale<<<kRB, kRT, 0, st>>>(gs, w, V + (int64_t)(j + 1) * n, n, j);
-        DGOP_CUDA_S(cudaGetLastError());
-      }
-      k_gm_backsub<<<1, 1, 0, st>>>(gs, H, e1, y, m);
-      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, V, n, y, n);
-      DGOP_TRY(residual(1));
+    for (int c = 0; c <= max_iters; ++c) {
+      DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, cycle));
+      bool stop = false;
+      DGOP_TRY(segment_done(s, st, c, &stop));
+      if (stop) break;
     }
   }
-  GMState h;
-  DGOP_CUDA_S(cudaMemcpyAsync(&h, gs, sizeof(h), cudaMemcpyDeviceToHost, st));
-  DGOP_CUDA_S(cudaStreamSynchronize(st));
-  res->success = h.success;
-  res->iterations = h.iters;
-  res->relative_error = h.rel;
-  return DGOP_OK;
+  return finish<GMState>(s, st, res);
 }
 
 // Vector stride of the refinement solver's inner workspace: n rounded up to 64 entries
@@ -695,50 +781,47 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
   GMState* gs = static_cast<GMState*>(s.state);
   const int* done = &gs->done;
   const int* inactive = &gs->inactive;
-  auto residual = [&](int phase) -> int {
-    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, 0, st, done));
-    k_sub_norm<<<kRB, kRT, 0, st>>>(b, w64, r64, n, pa, done);
-    k_gm_resid<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters, phase);
+  auto residual = [&](int phase, cudaStream_t q) -> int {
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, 0, q, done));
+    k_sub_norm<<<kRB, kRT, 0, q>>>(b, w64, r64, n, pa, done);
+    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, tol, max_iters, phase);
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
+  };
+  auto cycle = [&](cudaStream_t q) -> int {
+    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m, max_iters);
+    k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(r64), V, n, -1);  // V0 = r / |r|
+    for (int j = 0; j < m; ++j) {
+      T* vj = V + (int64_t)j * ld;
+      T* vn = vj + ld;
+      DGOP_TRY(apply_inner(s.op, vj, w, q, inactive));
+      const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
+      k_gs_dots<T><<<dgrid, kRT, 0, q>>>(gs, V, ld, j, w, s.wide);
+      k_gs_h<<<j + 1, kRT, 0, q>>>(gs, j, m, H, s.wide);
+      k_gs_update<T><<<kRB, kRT, 0, q>>>(gs, V, ld, j, m, H, w, vn, pa);
+      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pa, tol, max_iters);
+      k_gs_rescale<T><<<kRB, kRT, 0, q>>>(gs, vn, ld, j);
+      DGOP_CUDA_S(cudaGetLastError());
+    }
+    k_gm_backsub<<<1, 1, 0, q>>>(gs, H, e1, y, m);
+    k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const T*>(V), ld, y, n);
+    return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
   k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
   DGOP_CUDA_S(cudaGetLastError());
   if (max_iters <= 0 || m <= 0) {
-    DGOP_TRY(residual(2));
+    DGOP_TRY(residual(2, st));
   } else {
-    DGOP_TRY(residual(0));
-    for (int cycle = 0; cycle <= max_iters; ++cycle) {
-      int d = 0;
-      DGOP_TRY(read_done(s, st, &d));
-      if (d) break;
-      k_gm_cycle_start<<<1, 1, 0, st>>>(gs, csv, snv, e1, y, m, max_iters);
-      k_gm_scale<<<kRB, kRT, 0, st>>>(gs, static_cast<const double*>(r64), V, n, -1);  // V0 = r / |r|
-      for (int j = 0; j < m; ++j) {
-        T* vj = V + (int64_t)j * ld;
-        T* vn = vj + ld;
-        DGOP_TRY(apply_inner(s.op, vj, w, st, inactive));
-        const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
-        k_gs_dots<T><<<dgrid, kRT, 0, st>>>(gs, V, ld, j, w, s.wide);
-        k_gs_h<<<j + 1, kRT, 0, st>>>(gs, j, m, H, s.wide);
-        k_gs_update<T><<<kRB, kRT, 0, st>>>(gs, V, ld, j, m, H, w, vn, pa);
-        k_gm_column<<<1, kRT, 0, st>>>(gs, j, m, H, csv, snv, e1, pa, tol, max_iters);
-        k_gs_rescale<T><<<kRB, kRT, 0, st>>>(gs, vn, ld, j);
-        DGOP_CUDA_S(cudaGetLastError());
-      }
-      k_gm_backsub<<<1, 1, 0, st>>>(gs, H, e1, y, m);
-      k_gm_update<<<kRB, kRT, 0, st>>>(gs, x, static_cast<const T*>(V), ld, y, n);
-      DGOP_TRY(residual(1));
+    DGOP_TRY(residual(0, st));
+    for (int c = 0; c <= max_iters; ++c) {
+      DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, cycle));
+      bool stop = false;
+      DGOP_TRY(segment_done(s, st, c, &stop));
+      if (stop) break;
     }
   }
-  GMState h;
-  DGOP_CUDA_S(cudaMemcpyAsync(&h, gs, sizeof(h), cudaMemcpyDeviceToHost, st));
-  DGOP_CUDA_S(cudaStreamSynchronize(st));
-  res->success = h.success;
-  res->iterations = h.iters;
-  res->relative_error = h.rel;
-  return DGOP_OK;
+  return finish<GMState>(s, st, res);
 }
 
 }  // namespace
@@ -858,6 +941,15 @@ int dgop_solver_solve(dgop_solver* sv, const double* b, double* x, int max_iters
   return gmres_solve(sv->s, b, x, max_iters, tol, result, st);
 }
 
+int dgop_solver_set_graphs(dgop_solver* sv, int enable) {
+  if (!sv) {
+    set_error("dgop_solver_set_graphs: null solver");
+    return DGOP_ERR_ARG;
+  }
+  sv->s.use_graphs = enable != 0;
+  return DGOP_OK;
+}
+
 int dgop_solver_destroy(dgop_solver* sv) {
   if (!sv) return DGOP_OK;
   solver_free(sv);
@@ -884,7 +976,7 @@ static __device__ __align__(256) double g_static_cg_scratch[kStaticCgWords];
 
 std::mutex g_static_cg_mutex;
 double* g_static_cg_addr[64] = {};  // device address of the array, per device
-thread_local int g_static_cg_flag;  // host copy of the `done` word (pageable; no allocation)
+thread_local int g_static_cg_flag[2];  // host copies of the `done` word (pageable; no allocation)
 
 // Device address of the array on the current device, looked up once per device.  In host code
 // the array's name is only a stand-in; the kernels must be given this address.
@@ -935,7 +1027,8 @@ extern "C" int dgop_cg_solve_static(dgop_operator* op, const double* b, double* 
   s.work = base;
   s.partials = base + 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS;
   s.state = base + 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS + 2 * kRB;
-  s.h_flag = &g_static_cg_flag;
+  s.h_flag = g_static_cg_flag;
+  s.use_graphs = false;  // direct launches and synchronous done reads: nothing is created
   cudaStream_t st = (cudaStream_t)stream;
   // the array keeps the previous call's contents: start from a cleared solver state
   const cudaError_t e = cudaMemsetAsync(s.state, 0, sizeof(CGState), st);

@@ -109,7 +109,8 @@ int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
  *   Givens rotations, breakdown test rho <= eps * beta, the true residual recomputed after every
  *   cycle; `relative_error` = |b - A x| / |b|.
  * x holds the initial guess on entry and the solution on return.  dgop_solver_solve enqueues on
- * `stream` and synchronizes it before returning the result. */
+ * `stream` and synchronizes it before returning the result; it reads the solver's done flag once
+ * per segment, one segment behind the work already enqueued. */
 typedef struct {
   int success;
   int iterations;
@@ -131,6 +132,11 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dg
 int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_iters, double tol,
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);
+/* Solver segments (a chunk of CG iterations, a GMRES restart cycle) are captured once as a CUDA
+ * graph and replayed; the graph is re-captured when b, x, tol, max_iters or the operator's kernel
+ * selection change.  enable = 0 launches every kernel directly instead (same results, bit for
+ * bit).  No reference counterpart. */
+int dgop_solver_set_graphs(dgop_solver* solver, int enable);
 
 /* CG without any allocation at call time (no counterpart in the reference).  For callers that
  * must not let a library allocate device memory: a host framework that owns all device memory

@@ -167,3 +167,34 @@ def test_gmres_ir_max_iters_reported_as_failure(inner):
     info = g.GMRESIRSolver(op, 5, inner=inner).solve(b, x, 7, 1e-14)
     assert not info["success"] and info["iterations"] == 7
     assert abs(info["relative_error"] - _true_rel_residual(op, b, x)) <= 1e-9
+
+
+def _solvers(op):
+    return {"cg": lambda: g.CGSolver(op), "gmres": lambda: g.GMRESSolver(op, 10),
+            "ir32": lambda: g.GMRESIRSolver(op, 10, inner="fp32"), "ir64": lambda: g.GMRESIRSolver(op, 10, inner="fp64")}
+
+
+@pytest.mark.parametrize("kind", ["cg", "gmres", "ir32", "ir64"])
+def test_graph_replay_equals_direct_launches(kind):
+    """Graph-replayed segments give the same iterates, bit for bit, as direct launches, also when
+    the graph has to be re-captured for new vectors, a new tolerance or a new kernel selection."""
+    case = {"D": 3, "P": 2, "Q": 3, "basis": 0, "sizes": [5, 4, 6], "h": [0.2, 0.25, 1 / 6], "origin": [0.0] * 3,
+            "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "sigma_c": 30.0}
+    sp = make_space(case)
+    op = g.MassOperator(sp, 3, C.sigma_preset(1, 3, 1.0)) if kind == "cg" else _system(case, sp)
+    direct = _solvers(op)[kind]().use_graphs(False)
+    graphed = _solvers(op)[kind]()
+    for seed, tol in ((2, 1e-10), (3, 1e-10), (3, 1e-6)):
+        b = torch.from_numpy(oracle().fill_random(sp.num_dofs, seed)).cuda()
+        x0 = torch.zeros_like(b)
+        x1 = torch.zeros_like(b)
+        r0 = direct.solve(b, x0, 300, tol)
+        r1 = graphed.solve(b, x1, 300, tol)
+        assert r0 == r1
+        assert torch.equal(x0, x1)
+    if op.kernel == "kron":
+        op.select_kernel("generic")
+        b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 4)).cuda()
+        x0, x1 = torch.zeros_like(b), torch.zeros_like(b)
+        assert direct.solve(b, x0, 300, 1e-10) == graphed.solve(b, x1, 300, 1e-10)
+        assert torch.equal(x0, x1)
