@@ -52,6 +52,23 @@ def _headers_digest():
     return h.hexdigest()
 
 
+def _deps_digest(cc, src, flags):
+    """Digest of the package headers a unit includes (from nvcc -M), so a header change rebuilds
+    only the units that use it."""
+    cmd = [cc] + flags + (["-x", "cu"] if src.endswith(".cpp") else []) + ["-M", src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        return _headers_digest()
+    deps = sorted({t for t in r.stdout.replace("\\\n", " ").split() if t.startswith(ROOT) and not t.endswith(":")})
+    h = hashlib.sha256()
+    for d in deps:
+        if os.path.isfile(d):
+            with open(d, "rb") as f:
+                h.update(d.encode())
+                h.update(f.read())
+    return h.hexdigest()
+
+
 def _jobs(fast):
     jobs = []
     for src in SOURCES:
@@ -74,7 +91,6 @@ def build(fast=None, jobs=None, clean=False, verbose=False):
         shutil.rmtree(out_dir)
     os.makedirs(out_dir, exist_ok=True)
     flags = BASE_FLAGS + (["-DDGOP_FAST_BUILD"] if fast else [])
-    hdr = _headers_digest()
     cc = nvcc()
     work = _jobs(fast)
 
@@ -87,7 +103,7 @@ def build(fast=None, jobs=None, clean=False, verbose=False):
         h = hashlib.sha256()
         with open(src, "rb") as f:
             h.update(f.read())
-        h.update(hdr.encode())
+        h.update(_deps_digest(cc, src, flags + extra).encode())
         h.update(" ".join(flags + extra).encode())
         digest = h.hexdigest()
         if os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == digest:

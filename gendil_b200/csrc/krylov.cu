@@ -92,15 +92,17 @@ __global__ void __launch_bounds__(kRT) k_sub_norm(const double* __restrict__ b, 
 
 struct CGState {
   int done, success, iters, zero_x;
-  int base, pad_[3];  // iteration index of the current chunk's first iteration
-  double rhs_n, r_n, rel;
+  int base, max_iters, pad_[2];  // base: iteration index of the current chunk's first iteration
+  double tol, rhs_n, r_n, rel;
   double abs_[2];  // (r, r) by iteration parity
 };
 
 // conjugategradient.hpp:143-165: norms of the initial residual, early exits.
-__global__ void __launch_bounds__(kRT) k_cg_init(CGState* st, const double* partials, double tol) {
+__global__ void __launch_bounds__(kRT) k_cg_init(CGState* st, const double* partials, double tol, int max_iters) {
   const double R = reduce_partials(partials);
   if (threadIdx.x != 0) return;
+  st->tol = tol;
+  st->max_iters = max_iters;
   st->done = 0;
   st->success = 0;
   st->iters = 0;
@@ -159,10 +161,11 @@ __global__ void __launch_bounds__(kRT) k_cg_update(int kk, const CGState* st, do
 
 // stopping test, beta = (r_new, r_new) / (r_old, r_old), p = beta p + r   (:183-205)
 __global__ void __launch_bounds__(kRT) k_cg_finish(int kk, CGState* st, const double* __restrict__ r,
-                                                   double* __restrict__ p, int64_t n, const double* partials2,
-                                                   double tol, int max_iters) {
+                                                   double* __restrict__ p, int64_t n, const double* partials2) {
   if (st->done) return;
   const int k = st->base + kk;
+  const double tol = st->tol;
+  const int max_iters = st->max_iters;
   const double R = reduce_partials(partials2);
   const double r_n = sqrt(R);
   const double rhs_n = st->rhs_n;
@@ -207,13 +210,15 @@ __global__ void k_cg_no_iters(CGState* st) {
 // ------------------------------------------------------------------------------- GMRES
 
 struct GMState {
-  int done, success, iters, total, k, brk, inactive, pad;
-  double denom, beta, rel, inv_h;
+  int done, success, iters, total, k, brk, inactive, max_iters;
+  double denom, beta, rel, inv_h, tol;
 };
 
-__global__ void __launch_bounds__(kRT) k_gm_denom(GMState* st, const double* partials) {
+__global__ void __launch_bounds__(kRT) k_gm_denom(GMState* st, const double* partials, double tol, int max_iters) {
   const double R = reduce_partials(partials);
   if (threadIdx.x != 0) return;
+  st->tol = tol;
+  st->max_iters = max_iters;
   const double norm_rhs = sqrt(R);
   st->denom = norm_rhs > 0.0 ? norm_rhs : 1.0;  // gmres.hpp:113-115
   st->done = 0;
@@ -227,11 +232,12 @@ __global__ void __launch_bounds__(kRT) k_gm_denom(GMState* st, const double* par
 
 // true residual |b - A x| / denom and the decisions taken after it (gmres.hpp:117-123, 230-236, 269-280)
 // phase 0: initial; 1: end of a cycle; 2: residual-only solve (no iterations allowed)
-__global__ void __launch_bounds__(kRT) k_gm_resid(GMState* st, const double* partials, double tol, int max_iters,
-                                                  int phase) {
+__global__ void __launch_bounds__(kRT) k_gm_resid(GMState* st, const double* partials, int phase) {
   if (st->done) return;
   const double R = reduce_partials(partials);
   if (threadIdx.x != 0) return;
+  const double tol = st->tol;
+  const int max_iters = st->max_iters;
   const double beta = sqrt(R);
   const double rel = beta / st->denom;
   st->beta = beta;
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(kRT) k_gm_resid(GMState* st, const double* par
 }
 
 // start of a cycle: reset the rotations and the reduced right-hand side (gmres.hpp:132-146)
-__global__ void k_gm_cycle_start(GMState* st, double* cs, double* sn, double* e1, double* y, int m, int max_iters) {
+__global__ void k_gm_cycle_start(GMState* st, double* cs, double* sn, double* e1, double* y, int m) {
   if (st->done) {
     st->inactive = 1;
     return;
@@ -270,7 +276,7 @@ __global__ void k_gm_cycle_start(GMState* st, double* cs, double* sn, double* e1
   e1[0] = st->beta;
   st->k = 0;
   st->brk = 0;
-  st->inactive = st->total >= max_iters;
+  st->inactive = st->total >= st->max_iters;
   st->inv_h = 1.0 / st->beta;
 }
 
@@ -306,10 +312,12 @@ __global__ void __launch_bounds__(kRT) k_gm_mgs(const GMState* st, int i, int j,
 
 // Hessenberg column j: norm, previous rotations, new rotation, stopping tests (gmres.hpp:167-222)
 __global__ void __launch_bounds__(kRT) k_gm_column(GMState* st, int j, int m, double* H, double* cs, double* sn,
-                                                   double* e1, const double* partials, double tol, int max_iters) {
+                                                   double* e1, const double* partials) {
   if (st->inactive) return;
   const double R = reduce_partials(partials);
   if (threadIdx.x != 0) return;
+  const double tol = st->tol;
+  const int max_iters = st->max_iters;
   const double eps = DBL_EPSILON;
   const double beta = st->beta;
   st->total += 1;
@@ -511,14 +519,14 @@ struct SolverImpl {
   int inner = 0;               // refinement solver: DGOP_FP32 or DGOP_FP64 inner cycles
   double* wide = nullptr;      // refinement solver: (restart + 1) x kRB projection partials
   // Segments (a CG chunk, a GMRES cycle) are replayed from one CUDA graph, captured for the
-  // current (b, x, tol, max_iters, operator version) and re-captured when any of them changes.
+  // current (b, x, operator version) and re-captured when any of them changes (tolerance and
+  // iteration limit are device state).
   bool use_graphs = true;
   cudaStream_t cap = nullptr;
   cudaGraphExec_t exec = nullptr;
   const void* key_b = nullptr;
   const void* key_x = nullptr;
-  double key_tol = 0.0;
-  int key_iters = -1, key_version = -1;
+  int key_version = -1;
   // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -576,11 +584,9 @@ void solver_free(dgop_solver* sv) {
 // Enqueues one segment on `st`: replays the cached graph, capturing it first when the key
 // changed, or launches directly when graphs are off.
 template <typename F>
-int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, double tol, int max_iters,
-                F&& enqueue) {
+int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&& enqueue) {
   if (!s.use_graphs) return enqueue(st);
-  const bool same = s.exec && s.key_b == b && s.key_x == x && s.key_tol == tol && s.key_iters == max_iters &&
-                    s.key_version == s.op->version;
+  const bool same = s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version;
   if (!same) {
     if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
     DGOP_CUDA_S(cudaStreamBeginCapture(s.cap, cudaStreamCaptureModeThreadLocal));
@@ -593,7 +599,7 @@ int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, do
     }
     if (s.exec) cudaGraphExecDestroy(s.exec);
     s.exec = nullptr;
-    s.key_iters = -1;
+    s.key_version = -1;
     const cudaError_t e2 = cudaGraphInstantiateWithFlags(&s.exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) {
@@ -602,8 +608,6 @@ int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, do
     }
     s.key_b = b;
     s.key_x = x;
-    s.key_tol = tol;
-    s.key_iters = max_iters;
     s.key_version = s.op->version;
   }
   DGOP_CUDA_S(cudaGraphLaunch(s.exec, st));
@@ -653,7 +657,7 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
   // 1) r = rhs - A x
   DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, tmp, 0, st));
   k_sub_norm<<<kRB, kRT, 0, st>>>(b, tmp, r, n, pa, nullptr);
-  k_cg_init<<<1, kRT, 0, st>>>(cs, pa, tol);
+  k_cg_init<<<1, kRT, 0, st>>>(cs, pa, tol, max_iters);
   k_cg_init_p<<<kRB, kRT, 0, st>>>(cs, r, p, x, n);
   if (max_iters <= 0) k_cg_no_iters<<<1, 1, 0, st>>>(cs);
   DGOP_CUDA_S(cudaGetLastError());
@@ -663,14 +667,14 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
       DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, 0, q, done));
       k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(p), static_cast<const double*>(tmp), n, pa, done);
       k_cg_update<<<kRB, kRT, 0, q>>>(kk, cs, x, r, p, tmp, n, pa, pb);
-      k_cg_finish<<<kRB, kRT, 0, q>>>(kk, cs, r, p, n, pb, tol, max_iters);
+      k_cg_finish<<<kRB, kRT, 0, q>>>(kk, cs, r, p, n, pb);
     }
     k_cg_next_chunk<<<1, 1, 0, q>>>(cs);
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
   };
   for (int c = 0; (int64_t)c * kCheckEvery < max_iters; ++c) {
-    DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, chunk));
+    DGOP_TRY(run_segment(s, st, b, x, chunk));
     bool stop = false;
     DGOP_TRY(segment_done(s, st, c, &stop));
     if (stop) break;
@@ -697,12 +701,12 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   auto residual = [&](int phase, cudaStream_t q) -> int {
     DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, 0, q, done));
     k_sub_norm<<<kRB, kRT, 0, q>>>(b, w, V, n, pa, done);
-    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, tol, max_iters, phase);
+    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, phase);
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
   };
   auto cycle = [&](cudaStream_t q) -> int {
-    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m, max_iters);
+    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m);
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
     for (int j = 0; j < m; ++j) {
       double* vj = V + (int64_t)j * n;
@@ -716,7 +720,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
                                      pin, pout);
         std::swap(pin, pout);
       }
-      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pin, tol, max_iters);
+      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pin);
       k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(w), V + (int64_t)(j + 1) * n, n, j);
       DGOP_CUDA_S(cudaGetLastError());
     }
@@ -725,7 +729,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
-  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
+  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters);
   DGOP_CUDA_S(cudaGetLastError());
   if (max_iters <= 0 || m <= 0) {
     DGOP_TRY(residual(2, st));
@@ -733,7 +737,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     DGOP_TRY(residual(0, st));
     // every cycle performs at least one iteration or finishes the solve
     for (int c = 0; c <= max_iters; ++c) {
-      DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, cycle));
+      DGOP_TRY(run_segment(s, st, b, x, cycle));
       bool stop = false;
       DGOP_TRY(segment_done(s, st, c, &stop));
       if (stop) break;
@@ -784,12 +788,12 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
   auto residual = [&](int phase, cudaStream_t q) -> int {
     DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, 0, q, done));
     k_sub_norm<<<kRB, kRT, 0, q>>>(b, w64, r64, n, pa, done);
-    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, tol, max_iters, phase);
+    k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, phase);
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
   };
   auto cycle = [&](cudaStream_t q) -> int {
-    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m, max_iters);
+    k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m);
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(r64), V, n, -1);  // V0 = r / |r|
     for (int j = 0; j < m; ++j) {
       T* vj = V + (int64_t)j * ld;
@@ -799,7 +803,7 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
       k_gs_dots<T><<<dgrid, kRT, 0, q>>>(gs, V, ld, j, w, s.wide);
       k_gs_h<<<j + 1, kRT, 0, q>>>(gs, j, m, H, s.wide);
       k_gs_update<T><<<kRB, kRT, 0, q>>>(gs, V, ld, j, m, H, w, vn, pa);
-      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pa, tol, max_iters);
+      k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pa);
       k_gs_rescale<T><<<kRB, kRT, 0, q>>>(gs, vn, ld, j);
       DGOP_CUDA_S(cudaGetLastError());
     }
@@ -808,14 +812,14 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
     return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
-  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa);
+  k_gm_denom<<<1, kRT, 0, st>>>(gs, pa, tol, max_iters);
   DGOP_CUDA_S(cudaGetLastError());
   if (max_iters <= 0 || m <= 0) {
     DGOP_TRY(residual(2, st));
   } else {
     DGOP_TRY(residual(0, st));
     for (int c = 0; c <= max_iters; ++c) {
-      DGOP_TRY(run_segment(s, st, b, x, tol, max_iters, cycle));
+      DGOP_TRY(run_segment(s, st, b, x, cycle));
       bool stop = false;
       DGOP_TRY(segment_done(s, st, c, &stop));
       if (stop) break;

@@ -133,8 +133,8 @@ int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_i
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);
 /* Solver segments (a chunk of CG iterations, a GMRES restart cycle) are captured once as a CUDA
- * graph and replayed; the graph is re-captured when b, x, tol, max_iters or the operator's kernel
- * selection change.  enable = 0 launches every kernel directly instead (same results, bit for
+ * graph and replayed; the graph is re-captured when b, x or the operator's kernel selection
+ * change (tolerance and iteration limit live in device memory).  enable = 0 launches every kernel directly instead (same results, bit for
  * bit).  No reference counterpart. */
 int dgop_solver_set_graphs(dgop_solver* solver, int enable);
 
