@@ -292,6 +292,9 @@ def run_ours(args):
                 "gpu_launches": args.steps,
                 "clocks": clocks.summary()}
         line["config"]["kernel"] = op.kernel
+        if op.variant:
+            line["config"]["kernel_variant"] = op.variant
+            line["config"]["autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in op.variant_times().items() if v}
         if args.size != N_AXIS:
             line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
         if world == 1 and not args.no_solve:

@@ -85,6 +85,11 @@ def lib():
         L.dgop_operator_kernel_note.argtypes = [vp]
         L.dgop_operator_kernel_note.restype = ctypes.c_char_p
         L.dgop_operator_select_kernel.argtypes = [vp, i]
+        L.dgop_operator_variant.argtypes = [vp]
+        L.dgop_operator_variant_name.argtypes = [vp]
+        L.dgop_operator_variant_name.restype = ctypes.c_char_p
+        L.dgop_operator_set_variant.argtypes = [vp, i]
+        L.dgop_operator_variant_time.argtypes = [vp, i, ctypes.POINTER(ctypes.c_float)]
         L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
@@ -234,6 +239,27 @@ class _Operator:
 
     def select_kernel(self, name):
         check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1}[name]))
+
+    VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl")
+
+    @property
+    def variant(self):
+        """Kronecker-kernel variant picked by the autotuner (None without a Kronecker kernel)."""
+        v = lib().dgop_operator_variant(self.handle)
+        return None if v < 0 else self.VARIANTS[v]
+
+    def set_variant(self, name):
+        """Force a Kronecker-kernel variant by name, or None to re-run the autotuner."""
+        check(lib().dgop_operator_set_variant(self.handle, -1 if name is None else self.VARIANTS.index(name)))
+
+    def variant_times(self):
+        """Autotuner time per launch (ms) of every variant (0.0: not available or not timed)."""
+        out = {}
+        for k, name in enumerate(self.VARIANTS):
+            ms = ctypes.c_float()
+            check(lib().dgop_operator_variant_time(self.handle, k, ctypes.byref(ms)))
+            out[name] = ms.value
+        return out
         return self
 
     def close(self):

@@ -259,7 +259,7 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
   KronEntry<Real>* entry = nullptr;
   if constexpr (sizeof(Real) == 8) entry = &kron3d_slot_f64(s.n);
   else entry = &kron3d_slot_f32(s.n);
-  if (!entry->launch) {
+  if (!entry->v[0].launch) {
     set_error("no Kronecker kernel for this order");
     return DGOP_ERR_UNSUPPORTED;
   }
@@ -355,27 +355,93 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
     put(K.params_t, kSlotDY, plan.Dt[1]);
     put(K.params_t, kSlotDZ, plan.Dt[2]);
   }
-  // persistent grid: every warp walks groups of entry->epw consecutive elements
+  // persistent grid: every warp walks groups of entry->epw consecutive elements; one launch
+  // shape per kernel variant (their shared memory per warp differs)
   const int threads = kKronThreads, warps = threads / 32;
-  K.block = dim3(threads);
-  K.smem = (size_t)warps * entry->warp_smem * sizeof(Real);
   int max_smem = 0;
   DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
-  if ((int)K.smem > max_smem) {
+  const bool sep = plan.has_adv && plan.has_mass && !plan.mass_merged;
+  const int64_t groups = (s.nelem + entry->epw - 1) / entry->epw;
+  int usable = 0;
+  for (int v = 0; v < kKronVariants; ++v) {
+    const KronVariant<Real>& kv = entry->v[v];
+    auto& L = K.launch[v];
+    L.ok = false;
+    if (!kv.launch) continue;
+    L.block = dim3(threads);
+    L.smem = (size_t)warps * kv.warp_smem * sizeof(Real);
+    if ((int)L.smem > max_smem) continue;
+    DGOP_CUDA(cudaFuncSetAttribute(kv.func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    DGOP_CUDA(cudaFuncSetAttribute(kv.func_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    int per_sm = 0;
+    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? kv.func_sep : kv.func, threads, L.smem));
+    if (per_sm < 1) continue;
+    const int64_t ctas = std::min<int64_t>((groups + warps - 1) / warps, (int64_t)device_sm_count(op->device) * per_sm);
+    L.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+    L.ok = true;
+    ++usable;
+  }
+  if (!usable) {
     set_error("Kronecker kernel shared memory exceeds the device limit");
     return DGOP_ERR_UNSUPPORTED;
   }
-  DGOP_CUDA(cudaFuncSetAttribute(entry->func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-  DGOP_CUDA(cudaFuncSetAttribute(entry->func_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-  const bool sep = plan.has_adv && plan.has_mass && !plan.mass_merged;
-  int per_sm = 0;
-  DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? entry->func_sep : entry->func, threads,
-                                                          K.smem));
-  if (per_sm < 1) per_sm = 1;
-  const int64_t groups = (s.nelem + entry->epw - 1) / entry->epw;
-  const int64_t ctas = std::min<int64_t>((groups + warps - 1) / warps, (int64_t)device_sm_count(op->device) * per_sm);
-  K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+  K.variant = 0;
+  while (!K.launch[K.variant].ok) ++K.variant;
   K.ready = true;
+  return DGOP_OK;
+}
+
+// Autotuner: times every usable kernel variant of the operator on scratch vectors (three
+// launches after one warm-up, CUDA events) and keeps the fastest.  Operators above
+// kTuneMaxDofs keep the default variant (the scratch vectors would cost more than they save).
+constexpr int64_t kTuneMaxDofs = int64_t(1) << 26;
+
+template <typename Real>
+int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
+  int usable = 0;
+  for (const auto& L : K.launch) usable += L.ok ? 1 : 0;
+  if (!K.ready || usable < 2 || op->sp.ndofs > kTuneMaxDofs) return DGOP_OK;
+  const int64_t n = op->sp.ndofs;
+  Real* x = nullptr;
+  Real* y = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int best = K.variant;
+  float best_ms = 0.0f;
+  bool ok = cudaMalloc(&x, sizeof(Real) * n) == cudaSuccess && cudaMalloc(&y, sizeof(Real) * n) == cudaSuccess &&
+            cudaMemset(x, 0, sizeof(Real) * n) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+            cudaEventCreate(&e1) == cudaSuccess;
+  for (int v = 0; ok && v < kKronVariants; ++v) {
+    auto& L = K.launch[v];
+    if (!L.ok) continue;
+    KronParams<Real> p = K.params;
+    p.x = x;
+    p.y = y;
+    p.alpha = Real(1);
+    p.beta_y = Real(0);
+    p.flags = op->flags;
+    p.skip = nullptr;
+    K.entry->v[v].launch(p, L.grid, L.block, L.smem, 0);
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < 3; ++r) K.entry->v[v].launch(p, L.grid, L.block, L.smem, 0);
+    cudaEventRecord(e1, 0);
+    ok = cudaEventSynchronize(e1) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    float ms = 0.0f;
+    if (ok) cudaEventElapsedTime(&ms, e0, e1);
+    L.ms = ms / 3.0f;
+    if (ok && (best_ms == 0.0f || L.ms < best_ms)) {
+      best_ms = L.ms;
+      best = v;
+    }
+  }
+  if (x) cudaFree(x);
+  if (y) cudaFree(y);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!ok) {
+    cudaGetLastError();
+    return DGOP_OK;  // keep the default variant
+  }
+  K.variant = best;
   return DGOP_OK;
 }
 
@@ -488,6 +554,8 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
       if (krc == DGOP_OK) {
         if (setup_kron<float>(op, op->k32, plan, es, elem_beta) != DGOP_OK) free_kron(op->k32);
         op->kernel = DGOP_KERNEL_KRON;
+        autotune_kron(op, op->k64);
+        autotune_kron(op, op->k32);
       } else {
         free_kron(op->k64);
         op->kron_why = "Kronecker setup failed";
@@ -544,7 +612,8 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.flags = op->flags | extra_flags;
     p.skip = skip;
     if (linear) p.g = Real(0);
-    K.entry->launch(p, K.grid, K.block, K.smem, s);
+    const auto& KL = K.launch[K.variant];
+    K.entry->v[K.variant].launch(p, KL.grid, KL.block, KL.smem, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
     return DGOP_OK;
@@ -733,6 +802,49 @@ int dgop_operator_select_kernel(dgop_operator* op, int kernel) {
   }
   op->kernel = kernel;
   ++op->version;
+  return DGOP_OK;
+}
+
+int dgop_operator_variant(const dgop_operator* op) {
+  if (!op || !op->k64.ready) return -1;
+  return op->k64.variant;
+}
+
+const char* dgop_operator_variant_name(const dgop_operator* op) {
+  const int v = dgop_operator_variant(op);
+  return v < 0 ? "" : kKronVariantNames[v];
+}
+
+int dgop_operator_set_variant(dgop_operator* op, int variant) {
+  if (!op || variant < -1 || variant >= kKronVariants) {
+    set_error("dgop_operator_set_variant: bad arguments");
+    return DGOP_ERR_ARG;
+  }
+  if (!op->k64.ready) {
+    set_error("dgop_operator_set_variant: the operator has no Kronecker kernel");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (variant == -1) {
+    autotune_kron(op, op->k64);
+    autotune_kron(op, op->k32);
+  } else {
+    if (!op->k64.launch[variant].ok) {
+      set_error(std::string("kernel variant ") + kKronVariantNames[variant] + " is not available for this operator");
+      return DGOP_ERR_UNSUPPORTED;
+    }
+    op->k64.variant = variant;
+    if (op->k32.ready && op->k32.launch[variant].ok) op->k32.variant = variant;
+  }
+  ++op->version;
+  return DGOP_OK;
+}
+
+int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms) {
+  if (!op || !ms || variant < 0 || variant >= kKronVariants || !op->k64.ready) {
+    set_error("dgop_operator_variant_time: bad arguments");
+    return DGOP_ERR_ARG;
+  }
+  *ms = op->k64.launch[variant].ms;
   return DGOP_OK;
 }
 

@@ -41,8 +41,13 @@ struct KronCfg {
   const KronEntry<Real>* entry = nullptr;
   KronParams<Real> params{};    // forward operator
   KronParams<Real> params_t{};  // transposed operator
-  dim3 grid, block;
-  size_t smem = 0;
+  struct Launch {
+    bool ok = false;
+    dim3 grid, block;
+    size_t smem = 0;
+    float ms = 0.0f;  // autotuner timing (0: not timed)
+  } launch[kKronVariants];
+  int variant = 0;  // the kernel variant in use
   Real* d_mats = nullptr;
   Real* d_phi = nullptr;
   signed char* d_sgn = nullptr;

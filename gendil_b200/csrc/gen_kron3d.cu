@@ -1,23 +1,32 @@
-// Instantiations of the 3D Kronecker-form kernel, N = 1..5, FP64 and FP32.
+// Instantiations of the 3D Kronecker-form kernel, N = 1..5, FP64 and FP32, every variant.
 #include "kron3d_kernel.cuh"
 #include "kron_registry.h"
 
 namespace dgop {
 
+const char* const kKronVariantNames[kKronVariants] = {"stage2-tile", "stage1-tile", "stage2-shfl"};
+
 namespace {
-template <int N, typename Real>
+template <int N, typename Real, int STAGES, bool SHFL>
 void launch_kron3d(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
-  if (p.has_adv && p.has_mass && !p.mass_merged) kron3d_kernel<N, Real, true><<<grid, block, smem, s>>>(p);
-  else kron3d_kernel<N, Real, false><<<grid, block, smem, s>>>(p);
+  if (p.has_adv && p.has_mass && !p.mass_merged) kron3d_kernel<N, Real, true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+  else kron3d_kernel<N, Real, false, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+}
+
+template <int N, typename Real, int STAGES, bool SHFL>
+void fill_variant(KronVariant<Real>& v) {
+  v.launch = &launch_kron3d<N, Real, STAGES, SHFL>;
+  v.func = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, STAGES, SHFL>);
+  v.func_sep = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, STAGES, SHFL>);
+  v.warp_smem = Kron3DShape<N, Real>::warp_smem(STAGES, SHFL);
 }
 
 template <int N, typename Real>
 void fill(KronEntry<Real>& d) {
-  d.launch = &launch_kron3d<N, Real>;
-  d.func = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false>);
-  d.func_sep = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true>);
   d.epw = Kron3DShape<N, Real>::EPW;
-  d.warp_smem = Kron3DShape<N, Real>::WARP_SMEM;
+  fill_variant<N, Real, 2, false>(d.v[0]);
+  fill_variant<N, Real, 1, false>(d.v[1]);
+  if constexpr (Kron3DShape<N, Real>::BUTTERFLY) fill_variant<N, Real, 2, true>(d.v[2]);
 }
 
 template <int N>

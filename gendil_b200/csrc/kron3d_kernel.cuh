@@ -51,13 +51,18 @@ struct Kron3DShape {
   // face record per element: 12 coefficients (axis, side, {corner, neighbour/inflow}) + flag word
   static constexpr int RE = 12 + (16 / (int)sizeof(Real));
   static constexpr int STAGE = EPW * (SE + TE + RE);  // one pipeline stage: DoFs, traces, records
-  static constexpr bool BUTTERFLY = (N == 2 || N == 4);
-  static constexpr int SI = N * (N + 1);      // exchange tile (odd N)
-  static constexpr int TSE = SI * N + 4;
+  static constexpr bool BUTTERFLY = (N == 2 || N == 4);  // shuffle exchanges possible
+  // shared exchange tile per element: value (x, y, z) at tix(x, y, z); for N a power of two the
+  // z index is XOR-swizzled by y and the element stride is N^3 + N, so both the layout-Z and the
+  // layout-Y side of an exchange hit distinct banks
+  static constexpr bool POW2 = (N & (N - 1)) == 0;
+  static constexpr int TSE = NNN + (POW2 ? N : 1);
+  __host__ __device__ static constexpr int tix(int x, int y, int z) { return x * NN + y * N + (POW2 ? (z ^ y) : z); }
   static constexpr int TILE = EPW * TSE;
-  __host__ __device__ static constexpr int tidx(int i, int j, int k) { return k + (N + 1) * j + SI * i; }
-  // shared memory per warp (Reals): 2 pipeline stages + 3 exchange tiles for odd N
-  static constexpr int WARP_SMEM = 2 * STAGE + (BUTTERFLY ? 0 : 3 * TILE);
+  // shared memory per warp (Reals): STAGES pipeline stages (+ the exchange tile unless shuffles)
+  static constexpr int warp_smem(int stages, bool shfl) {
+    return stages * STAGE + ((shfl && BUTTERFLY) ? 0 : ((TILE + 3) / 4) * 4);
+  }
 };
 
 // Y[i][j] = sum_r A(i, r) X[r][j]      (operator along the first plane index)
@@ -144,35 +149,26 @@ __device__ __forceinline__ void exchange_butterfly(int t, Real (&X)[N][N]) {
   }
 }
 
+// Layout exchange through the warp's shared tile.  z_to_y: lane t holds X[i][j] = (x=i, y=j, z=t)
+// and receives X[i][k] = (x=i, y=t, z=k); otherwise the reverse.
 template <int N, typename Real>
-__device__ __forceinline__ void tile_put(Real* tile, int le, int t, bool from_z, const Real (&X)[N][N]) {
+__device__ __forceinline__ void exchange_tile(Real* tile, int le, int t, bool slot, bool z_to_y, Real (&X)[N][N]) {
   using S = Kron3DShape<N, Real>;
   Real* b = tile + le * S::TSE;
+  if (slot) {
 #pragma unroll
-  for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i)
 #pragma unroll
-    for (int j = 0; j < N; ++j) b[from_z ? S::tidx(i, j, t) : S::tidx(i, t, j)] = X[i][j];
-}
-
-template <int N, typename Real>
-__device__ __forceinline__ void tile_get(const Real* tile, int le, int t, bool to_z, Real (&X)[N][N]) {
-  using S = Kron3DShape<N, Real>;
-  const Real* b = tile + le * S::TSE;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N; ++j) X[i][j] = b[to_z ? S::tidx(i, j, t) : S::tidx(i, t, j)];
-}
-
-template <int N, typename Real>
-__device__ __forceinline__ void exchange(int le, int t, bool slot, Real* tile, bool z_to_y, Real (&X)[N][N]) {
-  if constexpr (Kron3DShape<N, Real>::BUTTERFLY) {
-    exchange_butterfly<N>(t, X);
-  } else {
-    if (slot) tile_put<N>(tile, le, t, z_to_y, X);
-    __syncwarp();
-    if (slot) tile_get<N>(tile, le, t, !z_to_y, X);
+      for (int j = 0; j < N; ++j) b[z_to_y ? S::tix(i, j, t) : S::tix(i, t, j)] = X[i][j];
   }
+  __syncwarp();
+  if (slot) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) X[i][j] = b[z_to_y ? S::tix(i, t, j) : S::tix(i, j, t)];
+  }
+  __syncwarp();  // the tile is free again
 }
 
 // Element coordinates (x fastest).
@@ -389,15 +385,20 @@ __device__ __forceinline__ void stage_group(const KronParams<Real>& P, int64_t e
   if (t == 0) *reinterpret_cast<uint32_t*>(rb + 12) = flags;
 }
 
-template <int N, typename Real, bool SEP>
+// Kernel variants (chosen per operator by the autotuner):
+//   STAGES 2: the next group is staged while this one computes; 1: no overlap inside the warp,
+//   less shared memory per warp and so more warps per SM
+//   SHFL:    layout exchanges by shuffle butterflies (even N) instead of the shared tile
+template <int N, typename Real, bool SEP, int STAGES, bool SHFL>
 __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ KronParams<Real> P) {
   using S = Kron3DShape<N, Real>;
   constexpr int NN = S::NN, NNN = S::NNN, EPW = S::EPW;
+  constexpr bool BFLY = SHFL && S::BUTTERFLY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int le = lane / N, t = lane - le * N;
-  Real* wbase = reinterpret_cast<Real*>(smem_raw) + (size_t)warp * S::WARP_SMEM;
-  Real* tiles = wbase + 2 * S::STAGE;  // odd N only
+  Real* wbase = reinterpret_cast<Real*>(smem_raw) + (size_t)warp * S::warp_smem(STAGES, SHFL);
+  [[maybe_unused]] Real* tile = wbase + STAGES * S::STAGE;
   const int64_t ngroups = (P.nelem + EPW - 1) / EPW;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const bool adv = P.has_adv != 0;
@@ -405,19 +406,25 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
   if (P.skip && *P.skip) return;  // a finished solve: nothing to do
 
   int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (g < ngroups) stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), wbase, lane, le, t, adv);
-  cp_async_commit();
+  if constexpr (STAGES == 2) {
+    if (g < ngroups) stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), wbase, lane, le, t, adv);
+    cp_async_commit();
+  }
   for (int it = 0; g < ngroups; g += nwarps, ++it) {
-    Real* buf = wbase + (it & 1) * S::STAGE;
-    {
+    Real* buf = wbase + (STAGES == 2 ? (it & 1) * S::STAGE : 0);
+    if constexpr (STAGES == 2) {
       const int64_t gn = g + nwarps;
       if (gn < ngroups)
         stage_group<N>(P, gn * EPW, group_size(EPW, P.nelem - gn * EPW), wbase + ((it + 1) & 1) * S::STAGE, lane, le,
                        t, adv);
       cp_async_commit();
       cp_async_wait<1>();
-      __syncwarp();
+    } else {
+      stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), buf, lane, le, t, adv);
+      cp_async_commit();
+      cp_async_wait<0>();
     }
+    __syncwarp();
     const int64_t e0 = g * EPW;
     const int ne = group_size(EPW, P.nelem - e0);
     const int64_t e = e0 + le;
@@ -469,8 +476,13 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
           if (src == kTraceSlot) return tb[1 * S::TS + t * S::TR + r];
           return P.x[en * NNN + r + N * (s ? 0 : N - 1) + NN * t];
         });
-      exchange<N>(le, t, slot, tiles, true, qx);
-      exchange<N>(le, t, slot, tiles + S::TILE, true, py);
+      if constexpr (BFLY) {
+        exchange_butterfly<N>(t, qx);
+        exchange_butterfly<N>(t, py);
+      } else {
+        exchange_tile<N>(tile, le, t, slot, true, qx);
+        exchange_tile<N>(tile, le, t, slot, true, py);
+      }
     }
 
     // ------------------------------------------------------------ layout Y (plane y = t)
@@ -531,31 +543,43 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
         kron_apply<N, Real, kSlotMX, true>(P, c[0], pz, qm);
       }
     }
-    if constexpr (!S::BUTTERFLY) __syncwarp();  // the tiles are reused
-    exchange<N>(le, t, slot, tiles, false, qz);
-    exchange<N>(le, t, slot, tiles + S::TILE, false, out);
-    if constexpr (SEP) exchange<N>(le, t, slot, tiles + 2 * S::TILE, false, qm);
+    __syncwarp();  // every lane is done reading the staged input of this group
+    Real* ob = buf + le * S::SE;  // output staging: the group's DoF slots, staged layout
+    if constexpr (BFLY) {
+      exchange_butterfly<N>(t, qz);
+      exchange_butterfly<N>(t, out);
+      if constexpr (SEP) exchange_butterfly<N>(t, qm);
+    } else {
+      // x and y terms leave in layout Y straight to the output slots; the z term crosses to
+      // layout Z through the tile and is added there
+      if (slot) {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int k = 0; k < N; ++k) ob[k * S::SP + i + N * t] = out[i][k];
+      }
+      exchange_tile<N>(tile, le, t, slot, false, qz);
+      if constexpr (SEP) exchange_tile<N>(tile, le, t, slot, false, qm);
+    }
 
     // ------------------------------------------------------------ layout Z, output
     kron_apply<N, Real, kSlotTZY, false>(P, c[1], qz, py);
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-#pragma unroll
-      for (int j = 0; j < N; ++j) out[i][j] += py[i][j];
     if constexpr (SEP) {
-      kron_apply<N, Real, kSlotMY, false>(P, c[1], qm, py);
+      kron_apply<N, Real, kSlotMY, false>(P, c[1], qm, qx);
 #pragma unroll
       for (int i = 0; i < N; ++i)
 #pragma unroll
-        for (int j = 0; j < N; ++j) out[i][j] += py[i][j];
+        for (int j = 0; j < N; ++j) py[i][j] += qx[i][j];
     }
-    __syncwarp();  // every lane is done reading the staged input of this group
     if (slot) {
-      Real* ob = buf + le * S::SE + t * S::SP;
+      Real* op = ob + t * S::SP;
 #pragma unroll
       for (int i = 0; i < N; ++i)
 #pragma unroll
-        for (int j = 0; j < N; ++j) ob[i + N * j] = out[i][j];
+        for (int j = 0; j < N; ++j) {
+          if constexpr (BFLY) op[i + N * j] = out[i][j] + py[i][j];
+          else op[i + N * j] += py[i][j];
+        }
     }
     __syncwarp();
     {
@@ -575,7 +599,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
         }
       }
     }
-    __syncwarp();  // the buffer is refilled by the prefetch of the next-but-one group
+    __syncwarp();  // the buffer is refilled by a later prefetch
   }
   cp_async_wait<0>();
 }

@@ -9,13 +9,25 @@ namespace dgop {
 
 constexpr int kKronThreads = 128;
 
+// Kernel variants of one (N, precision); the autotuner picks one per operator.
+//   0: two staging stages, exchanges through the shared tile
+//   1: one staging stage (more warps per SM), exchanges through the shared tile
+//   2: two staging stages, exchanges by shuffle butterflies (even N only)
+constexpr int kKronVariants = 3;
+extern const char* const kKronVariantNames[kKronVariants];
+
 template <typename Real>
-struct KronEntry {
+struct KronVariant {
   void (*launch)(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func = nullptr;      // kernel symbol (mass merged or absent)
   const void* func_sep = nullptr;  // kernel symbol with a separate mass term
-  int epw = 0;        // elements per warp group
-  int warp_smem = 0;  // Real values of shared memory per warp
+  int warp_smem = 0;               // Real values of shared memory per warp
+};
+
+template <typename Real>
+struct KronEntry {
+  int epw = 0;  // elements per warp group
+  KronVariant<Real> v[kKronVariants];
 };
 
 KronEntry<double>& kron3d_slot_f64(int N);

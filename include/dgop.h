@@ -87,6 +87,18 @@ enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1 };
 int dgop_operator_kernel(const dgop_operator* op);
 const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);
+/* Kronecker-kernel variants (no reference counterpart): 0 "stage2-tile" (next element group staged
+ * while this one computes, layout exchanges through shared memory), 1 "stage1-tile" (one staging
+ * buffer, more warps per SM), 2 "stage2-shfl" (exchanges by warp shuffles; even orders).  At
+ * creation the autotuner times every variant on scratch vectors (operators of at most 2^26 DoFs)
+ * and keeps the fastest; all variants give bit-identical results.  dgop_operator_variant returns
+ * the FP64 variant in use (-1 without a Kronecker kernel); dgop_operator_set_variant forces one
+ * (-1 re-runs the autotuner); dgop_operator_variant_time gives the autotuner's time per launch in
+ * ms (0 when not timed). */
+int dgop_operator_variant(const dgop_operator* op);
+const char* dgop_operator_variant_name(const dgop_operator* op);
+int dgop_operator_set_variant(dgop_operator* op, int variant);
+int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers, aligned to their
  * element size; the Kronecker-form kernel runs on 16-byte aligned vectors (any cudaMalloc'd or

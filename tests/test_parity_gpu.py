@@ -127,3 +127,43 @@ def test_apply_ex_alpha_beta(kernel):
     op.apply(x, y, alpha=2.5, beta=-0.5)
     ref = 2.5 * ax - 0.5 * y0
     assert float((y - ref).abs().max() / ref.abs().max()) < 1e-14
+
+
+VARIANT_CASES = [
+    # (id, case, kind, mode): advection with inflow, mass + advection with a separate mass term,
+    # odd order, FP64 and FP32
+    ("adv_p3_sincos", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [9, 6, 5], "h": [1 / 9, 1 / 6, 0.2],
+                       "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 2, "g": 0.5}, "adv", 1),
+    ("sys_p2_bubble", {"D": 3, "P": 2, "Q": 3, "basis": 0, "sizes": [7, 5, 6], "h": [1 / 7, 0.2, 1 / 6],
+                       "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 1, "sigma_kind": 2, "g": 0.0}, "adv", 2),
+    ("mass_p1", {"D": 3, "P": 1, "Q": 2, "basis": 0, "sizes": [11, 3, 4], "h": [1 / 11, 1 / 3, 0.25],
+                 "origin": [0.0] * 3, "periodic": [0, 1, 0], "sigma_kind": 1}, "mass", 1),
+]
+
+
+@pytest.mark.parametrize("cid,case,kind,mode", VARIANT_CASES, ids=[c[0] for c in VARIANT_CASES])
+def test_kron_variants_are_bit_identical(cid, case, kind, mode):
+    """Every Kronecker-kernel variant the autotuner can pick computes the same bits (forward,
+    transposed and FP32 applies), and the forward apply meets the parity bar."""
+    op = make_operator(case, kind, mode)
+    if op.kernel != "kron":
+        pytest.skip(op.kernel_note)
+    assert op.variant in op.VARIANTS
+    x = inputs(dict(case, seed=1))
+    ref = None
+    for name in op.VARIANTS:
+        try:
+            op.set_variant(name)
+        except RuntimeError:
+            assert name == "stage2-shfl" and case["P"] % 2 == 0  # shuffles need an even N = P + 1
+            continue
+        got = (cuda_apply(op, x), cuda_apply(op, x, transpose=True), cuda_apply(op, x, f32=True))
+        if ref is None:
+            ref = got
+            want = oracle().mass_apply(case, x) if kind == "mass" else oracle().advection_apply(case, x, mode)
+            assert rel_max(got[0], want) <= APPLY_TOL
+        else:
+            for a, b in zip(got, ref):
+                assert np.array_equal(a, b), name
+    op.set_variant(None)  # the autotuner again
+    assert op.variant in op.VARIANTS
