@@ -218,6 +218,8 @@ def run_ours(args):
 
     space = g.Space(3, [args.size] * 3, order=ORDER)
     op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
+    if args.variant and op.kernel == "kron":
+        op.set_variant(args.variant)  # a fixed kernel for profiling; the autotuner's pick otherwise
     nd = space.num_dofs
     x_np = g.fill_random(nd, 1)
     x = torch.from_numpy(x_np).to(dev)
@@ -319,6 +321,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=N_AXIS, help="elements per axis (profiling runs only)")
+    ap.add_argument("--variant", default=None, help="force a Kronecker-kernel variant (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

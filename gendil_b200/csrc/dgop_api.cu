@@ -283,6 +283,9 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
   p.mats = K.d_mats;
   // slot -> matrix table; constant tables go to kernel-parameter space
   const int N = s.n;
+  // the kernel reads element-dependent matrices with 16-byte loads when N allows them
+  const int vec = (N % (16 / (int)sizeof(Real)) == 0) ? 16 / (int)sizeof(Real) : 1;
+  bool aligned = true;
   auto put = [&](KronParams<Real>& q, int slot, const KronMat& m) {
     q.vary[slot] = 0;
     q.vm[slot] = m;
@@ -291,6 +294,7 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
       for (int i = 0; i < N * N; ++i) q.cm[slot][i] = (Real)plan.mats[m.off + i];
     } else {
       q.vary[slot] = 1;
+      aligned = aligned && m.off % vec == 0 && m.stride % vec == 0;
     }
   };
   if (plan.has_adv) {
@@ -354,6 +358,10 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
     put(K.params_t, kSlotDX, plan.Dt[0]);
     put(K.params_t, kSlotDY, plan.Dt[1]);
     put(K.params_t, kSlotDZ, plan.Dt[2]);
+  }
+  if (!aligned) {
+    set_error("Kronecker matrix table misaligned for vector loads");
+    return DGOP_ERR_UNSUPPORTED;
   }
   // persistent grid: every warp walks groups of entry->epw consecutive elements; one launch
   // shape per kernel variant (their shared memory per warp differs)

@@ -52,18 +52,93 @@ struct Kron3DShape {
   static constexpr int RE = 12 + (16 / (int)sizeof(Real));
   static constexpr int STAGE = EPW * (SE + TE + RE);  // one pipeline stage: DoFs, traces, records
   static constexpr bool BUTTERFLY = (N == 2 || N == 4);  // shuffle exchanges possible
-  // shared exchange tile per element: value (x, y, z) at tix(x, y, z); for N a power of two the
-  // z index is XOR-swizzled by y and the element stride is N^3 + N, so both the layout-Z and the
-  // layout-Y side of an exchange hit distinct banks
-  static constexpr bool POW2 = (N & (N - 1)) == 0;
-  static constexpr int TSE = NNN + (POW2 ? N : 1);
-  __host__ __device__ static constexpr int tix(int x, int y, int z) { return x * NN + y * N + (POW2 ? (z ^ y) : z); }
+  // vector width (Reals) of shared-memory accesses along x: 16 bytes when N allows it
+  static constexpr int V = (N % (16 / (int)sizeof(Real)) == 0) ? 16 / (int)sizeof(Real) : 1;
+  // Exchange tile per element, layout [y][z][x]: value (x, y, z) at y * TA + z * N + x, element
+  // stride TSE.  Both sides of an exchange access V consecutive x values; TA and TSE are the
+  // smallest strides for which neither side has a shared-memory bank conflict (tile_geom).
+  struct Geom {
+    int A, TSE;
+  };
+  static constexpr Geom tile_geom() {
+    const int G = V * (int)sizeof(Real);  // bytes per access
+    const int L = G == 16 ? 8 : (G == 8 ? 16 : 32);  // lanes served together
+    const int CH = 128 / G;                          // access granules per 128 bytes
+    for (int tse = NNN; tse <= NNN + 96; ++tse) {
+      if (tse % V) continue;
+      for (int a = NN; N == 1 || (N - 1) * a + NN <= tse; ++a) {
+        if (a % V) continue;
+        bool ok = true;
+        for (int ph = 0; ph < 32 / L && ok; ++ph) {
+          unsigned put = 0, get = 0;
+          for (int l = ph * L; l < ph * L + L && ok; ++l) {
+            const int le = l / N, t = l - le * N;
+            if (le >= EPW) continue;
+            const int cp = ((le * tse + t * N) / V) % CH, cg = ((le * tse + t * a) / V) % CH;
+            if ((put >> cp) & 1u || (get >> cg) & 1u) ok = false;
+            put |= 1u << cp;
+            get |= 1u << cg;
+          }
+        }
+        if (ok) return {a, tse};
+        if (N == 1) break;
+      }
+    }
+    return {NN, NNN};  // dense (bank conflicts accepted)
+  }
+  static constexpr int TA = tile_geom().A;
+  static constexpr int TSE = tile_geom().TSE;
   static constexpr int TILE = EPW * TSE;
   // shared memory per warp (Reals): STAGES pipeline stages (+ the exchange tile unless shuffles)
   static constexpr int warp_smem(int stages, bool shfl) {
     return stages * STAGE + ((shfl && BUTTERFLY) ? 0 : ((TILE + 3) / 4) * 4);
   }
 };
+
+// V consecutive Reals as one shared or global access (V = 1, 2 or 4; 16-byte aligned addresses
+// when V > 1), moved component-wise into register arrays.
+template <typename Real, int V>
+__device__ __forceinline__ void vload(const Real* p, Real (&v)[V]) {
+  if constexpr (V == 1) {
+    v[0] = p[0];
+  } else if constexpr (V == 2) {
+    const double2 w = *reinterpret_cast<const double2*>(p);
+    v[0] = w.x;
+    v[1] = w.y;
+  } else {
+    const float4 w = *reinterpret_cast<const float4*>(p);
+    v[0] = w.x;
+    v[1] = w.y;
+    v[2] = w.z;
+    v[3] = w.w;
+  }
+}
+template <typename Real, int V>
+__device__ __forceinline__ void vstore(Real* p, const Real (&v)[V]) {
+  if constexpr (V == 1) {
+    p[0] = v[0];
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  } else {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+template <typename Real, int V>
+__device__ __forceinline__ void vldg(const Real* p, Real (&v)[V]) {
+  if constexpr (V == 1) {
+    v[0] = __ldg(p);
+  } else if constexpr (V == 2) {
+    const double2 w = __ldg(reinterpret_cast<const double2*>(p));
+    v[0] = w.x;
+    v[1] = w.y;
+  } else {
+    const float4 w = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = w.x;
+    v[1] = w.y;
+    v[2] = w.z;
+    v[3] = w.w;
+  }
+}
 
 // Y[i][j] = sum_r A(i, r) X[r][j]      (operator along the first plane index)
 template <int N, typename Real, typename Mat>
@@ -113,10 +188,17 @@ __device__ __forceinline__ void kron_apply(const KronParams<Real>& P, uint32_t c
   if (P.vary[SLOT]) {
     RegMat<N, Real> A;
     const Real* p = P.mats + P.vm[SLOT].off + (int64_t)coord * P.vm[SLOT].stride;
+    // N x N blocks at offsets that are multiples of the vector width (checked at setup)
+    constexpr int V = Kron3DShape<N, Real>::V;
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
-      for (int j = 0; j < N; ++j) A.a[i][j] = __ldg(p + i * N + j);
+      for (int j = 0; j < N; j += V) {
+        Real v[V];
+        vldg<Real, V>(p + i * N + j, v);
+#pragma unroll
+        for (int q = 0; q < V; ++q) A.a[i][j + q] = v[q];
+      }
     if (FIRST) apply_first<N>(A, X, Y);
     else apply_second<N>(A, X, Y);
   } else {
@@ -149,24 +231,72 @@ __device__ __forceinline__ void exchange_butterfly(int t, Real (&X)[N][N]) {
   }
 }
 
+// Plane of an element in layout Z (values [x][y] of plane z = t) from the staged layout, where
+// (x, y, z) sits at z * SP + y * N + x: V-wide loads along x.
+template <int N, typename Real>
+__device__ __forceinline__ void load_plane_z(const Real* ub, int t, bool active, Real (&u)[N][N]) {
+  using S = Kron3DShape<N, Real>;
+  constexpr int V = S::V;
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; i += V) {
+      Real v[V];
+      if (active) vload<Real, V>(ub + t * S::SP + N * j + i, v);
+#pragma unroll
+      for (int q = 0; q < V; ++q) u[i + q][j] = active ? v[q] : Real(0);
+    }
+}
+
+// Plane of an element in layout Y (values [x][z] of plane y = t) from the staged layout.
+template <int N, typename Real>
+__device__ __forceinline__ void load_plane_y(const Real* ub, int t, bool active, Real (&u)[N][N]) {
+  using S = Kron3DShape<N, Real>;
+  constexpr int V = S::V;
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int i = 0; i < N; i += V) {
+      Real v[V];
+      if (active) vload<Real, V>(ub + k * S::SP + N * t + i, v);
+#pragma unroll
+      for (int q = 0; q < V; ++q) u[i + q][k] = active ? v[q] : Real(0);
+    }
+}
+
 // Layout exchange through the warp's shared tile.  z_to_y: lane t holds X[i][j] = (x=i, y=j, z=t)
-// and receives X[i][k] = (x=i, y=t, z=k); otherwise the reverse.
+// and receives X[i][k] = (x=i, y=t, z=k); otherwise the reverse.  Tile layout [y][z][x].
 template <int N, typename Real>
 __device__ __forceinline__ void exchange_tile(Real* tile, int le, int t, bool slot, bool z_to_y, Real (&X)[N][N]) {
   using S = Kron3DShape<N, Real>;
+  constexpr int V = S::V;
   Real* b = tile + le * S::TSE;
+  // layout Z side: lane t = z owns (x, y = j) at j * TA + t * N + x;
+  // layout Y side: lane t = y owns (x, z = k) at t * TA + k * N + x
+  auto z_side = [&](int j, int i) { return b + j * S::TA + t * N + i; };
+  auto y_side = [&](int k, int i) { return b + t * S::TA + k * N + i; };
   if (slot) {
 #pragma unroll
-    for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
 #pragma unroll
-      for (int j = 0; j < N; ++j) b[z_to_y ? S::tix(i, j, t) : S::tix(i, t, j)] = X[i][j];
+      for (int i = 0; i < N; i += V) {
+        Real v[V];
+#pragma unroll
+        for (int q = 0; q < V; ++q) v[q] = X[i + q][j];
+        vstore<Real, V>(z_to_y ? z_side(j, i) : y_side(j, i), v);
+      }
   }
   __syncwarp();
   if (slot) {
 #pragma unroll
-    for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
 #pragma unroll
-      for (int j = 0; j < N; ++j) X[i][j] = b[z_to_y ? S::tix(i, t, j) : S::tix(i, j, t)];
+      for (int i = 0; i < N; i += V) {
+        Real v[V];
+        vload<Real, V>(z_to_y ? y_side(j, i) : z_side(j, i), v);
+#pragma unroll
+        for (int q = 0; q < V; ++q) X[i + q][j] = v[q];
+      }
   }
   __syncwarp();  // the tile is free again
 }
@@ -440,10 +570,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
     // ------------------------------------------------------------ layout Z (plane z = t)
     if (adv) {
       Real u[N][N];
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-#pragma unroll
-        for (int j = 0; j < N; ++j) u[i][j] = active ? ub[t * S::SP + i + N * j] : Real(0);
+      load_plane_z<N>(ub, t, active, u);
       {
         Real px[N][N];
         kron_apply<N, Real, kSlotDX, true>(P, c[0], u, px);
@@ -505,10 +632,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
           for (int k = 0; k < N; ++k) out[i][k] = Real(0);
       }
       Real u[N][N], pz[N][N];
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-#pragma unroll
-        for (int k = 0; k < N; ++k) u[i][k] = active ? ub[k * S::SP + i + N * t] : Real(0);
+      load_plane_y<N>(ub, t, active, u);
       kron_apply<N, Real, kSlotDZ, false>(P, c[2], u, pz);
       if (adv) {
         if (P.elem[2]) {
@@ -554,9 +678,14 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
       // layout Z through the tile and is added there
       if (slot) {
 #pragma unroll
-        for (int i = 0; i < N; ++i)
+        for (int k = 0; k < N; ++k)
 #pragma unroll
-          for (int k = 0; k < N; ++k) ob[k * S::SP + i + N * t] = out[i][k];
+          for (int i = 0; i < N; i += S::V) {
+            Real v[S::V];
+#pragma unroll
+            for (int q = 0; q < S::V; ++q) v[q] = out[i + q][k];
+            vstore<Real, S::V>(ob + k * S::SP + N * t + i, v);
+          }
       }
       exchange_tile<N>(tile, le, t, slot, false, qz);
       if constexpr (SEP) exchange_tile<N>(tile, le, t, slot, false, qm);
@@ -574,11 +703,19 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
     if (slot) {
       Real* op = ob + t * S::SP;
 #pragma unroll
-      for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-          if constexpr (BFLY) op[i + N * j] = out[i][j] + py[i][j];
-          else op[i + N * j] += py[i][j];
+        for (int i = 0; i < N; i += S::V) {
+          Real v[S::V];
+          if constexpr (BFLY) {
+#pragma unroll
+            for (int q = 0; q < S::V; ++q) v[q] = out[i + q][j] + py[i + q][j];
+          } else {
+            vload<Real, S::V>(op + N * j + i, v);
+#pragma unroll
+            for (int q = 0; q < S::V; ++q) v[q] += py[i + q][j];
+          }
+          vstore<Real, S::V>(op + N * j + i, v);
         }
     }
     __syncwarp();
