@@ -40,20 +40,69 @@ struct Kron3DShape {
   static constexpr int CB = (NN * (int)sizeof(Real)) % 16 == 0 ? 16 : ((NN * (int)sizeof(Real)) % 8 == 0 ? 8 : 4);
   static constexpr int CR = CB / (int)sizeof(Real);  // Reals per chunk
   static constexpr int pad_for(int p) { return ((NN + p) * (int)sizeof(Real)) % CB == 0 ? p : pad_for(p + 1); }
-  static constexpr int SP = NN + pad_for(1);  // staged plane stride (Reals)
-  static constexpr int SE = N * SP;           // staged element stride
+  // vector width (Reals) of shared-memory accesses along x: 16 bytes when N allows it
+  static constexpr int V = (N % (16 / (int)sizeof(Real)) == 0) ? 16 / (int)sizeof(Real) : 1;
+  // Shared-memory bank model: accesses of G bytes are served 128 bytes at a time (8, 16 or 32
+  // lanes together); two lanes of one such phase conflict when their G-byte granules fall in the
+  // same bank group.  `distinct` checks one access pattern: offset(le, t) in Reals.
+  template <typename F>
+  static constexpr bool distinct(int vreals, F offset) {
+    const int G = vreals * (int)sizeof(Real);
+    const int L = G >= 16 ? 8 : (G == 8 ? 16 : 32);
+    const int CH = 128 / (G >= 16 ? 16 : G);
+    for (int ph = 0; ph < 32 / L; ++ph) {
+      unsigned long long seen = 0;
+      for (int l = ph * L; l < ph * L + L; ++l) {
+        const int le = l / N, t = l - le * N;
+        if (le >= EPW) continue;
+        const int c = (offset(le, t) / vreals) % CH;
+        if ((seen >> c) & 1ull) return false;
+        seen |= 1ull << c;
+      }
+    }
+    return true;
+  }
+  // Staged element layout: (x, y, z) at z * SP + y * N + x, element stride SE.  The smallest
+  // strides (keeping the copy granule's alignment) for which the layout-Z and layout-Y plane
+  // accesses are conflict-free; fallback: the dense plane padded to the copy granule.
+  struct Staged {
+    int SP, SE;
+  };
+  static constexpr Staged staged_geom() {
+    // a conflict-free layout more than 25 % larger than the dense one costs more shared memory
+    // (warps per SM) than its conflicts cost
+    const int dense = N * (NN + pad_for(1));
+    for (int se = N * NN; se <= dense + dense / 4; ++se) {
+      if ((se * (int)sizeof(Real)) % CB || se % V) continue;
+      for (int sp = NN; N * sp <= se; ++sp) {
+        if ((sp * (int)sizeof(Real)) % CB || sp % V) continue;
+        if (distinct(V, [&](int le, int t) { return le * se + t * sp; }) &&
+            distinct(V, [&](int le, int t) { return le * se + t * N; }))
+          return {sp, se};
+      }
+    }
+    return {NN + pad_for(1), N * (NN + pad_for(1))};
+  }
+  static constexpr int SP = staged_geom().SP;  // staged plane stride (Reals)
+  static constexpr int SE = staged_geom().SE;  // staged element stride
   // neighbour traces: one slot per axis (N rows of N), used by the first face of that axis that
-  // needs a neighbour trace; a second one on the same axis (rare) is read from global memory
+  // needs a neighbour trace; a second one on the same axis (rare) is read from global memory.
+  // Rows are read V-wide; the element stride TE is the smallest conflict-free one.
   static constexpr int RB = (N * (int)sizeof(Real)) % 16 == 0 ? 16 : ((N * (int)sizeof(Real)) % 8 == 0 ? 8 : 4);
   static constexpr int TR = N;                // trace row stride
   static constexpr int TS = N * TR;           // trace slot stride
-  static constexpr int TE = 3 * TS;           // traces per element
+  static constexpr int trace_stride() {
+    for (int te = 3 * TS; te <= 3 * TS + 64; ++te) {
+      if ((te * (int)sizeof(Real)) % RB || te % V) continue;
+      if (distinct(V, [&](int le, int t) { return le * te + t * TR; })) return te;
+    }
+    return 3 * TS;
+  }
+  static constexpr int TE = trace_stride();   // traces per element
   // face record per element: 12 coefficients (axis, side, {corner, neighbour/inflow}) + flag word
   static constexpr int RE = 12 + (16 / (int)sizeof(Real));
   static constexpr int STAGE = EPW * (SE + TE + RE);  // one pipeline stage: DoFs, traces, records
   static constexpr bool BUTTERFLY = (N == 2 || N == 4);  // shuffle exchanges possible
-  // vector width (Reals) of shared-memory accesses along x: 16 bytes when N allows it
-  static constexpr int V = (N % (16 / (int)sizeof(Real)) == 0) ? 16 / (int)sizeof(Real) : 1;
   // Exchange tile per element, layout [y][z][x]: value (x, y, z) at y * TA + z * N + x, element
   // stride TSE.  Both sides of an exchange access V consecutive x values; TA and TSE are the
   // smallest strides for which neither side has a shared-memory bank conflict (tile_geom).
@@ -62,9 +111,10 @@ struct Kron3DShape {
   };
   static constexpr Geom tile_geom() {
     const int G = V * (int)sizeof(Real);  // bytes per access
+    const int limit = (NNN + 1) + (NNN + 1) / 4;  // at most 25 % above the dense tile
     const int L = G == 16 ? 8 : (G == 8 ? 16 : 32);  // lanes served together
     const int CH = 128 / G;                          // access granules per 128 bytes
-    for (int tse = NNN; tse <= NNN + 96; ++tse) {
+    for (int tse = NNN; tse <= limit; ++tse) {
       if (tse % V) continue;
       for (int a = NN; N == 1 || (N - 1) * a + NN <= tse; ++a) {
         if (a % V) continue;
@@ -98,14 +148,30 @@ struct Kron3DShape {
 // V consecutive Reals as one shared or global access (V = 1, 2 or 4; 16-byte aligned addresses
 // when V > 1), moved component-wise into register arrays.
 template <typename Real, int V>
+struct Vec16 {};
+template <>
+struct Vec16<double, 2> {
+  using T = double2;
+};
+template <>
+struct Vec16<float, 2> {
+  using T = float2;
+};
+template <>
+struct Vec16<float, 4> {
+  using T = float4;
+};
+
+template <typename Real, int V>
 __device__ __forceinline__ void vload(const Real* p, Real (&v)[V]) {
   if constexpr (V == 1) {
     v[0] = p[0];
   } else if constexpr (V == 2) {
-    const double2 w = *reinterpret_cast<const double2*>(p);
+    const auto w = *reinterpret_cast<const typename Vec16<Real, 2>::T*>(p);
     v[0] = w.x;
     v[1] = w.y;
   } else {
+    static_assert(V == 4 && sizeof(Real) == 4, "unsupported vector width");
     const float4 w = *reinterpret_cast<const float4*>(p);
     v[0] = w.x;
     v[1] = w.y;
@@ -118,8 +184,13 @@ __device__ __forceinline__ void vstore(Real* p, const Real (&v)[V]) {
   if constexpr (V == 1) {
     p[0] = v[0];
   } else if constexpr (V == 2) {
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    using T = typename Vec16<Real, 2>::T;
+    T w;
+    w.x = v[0];
+    w.y = v[1];
+    *reinterpret_cast<T*>(p) = w;
   } else {
+    static_assert(V == 4 && sizeof(Real) == 4, "unsupported vector width");
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
   }
 }
@@ -128,10 +199,11 @@ __device__ __forceinline__ void vldg(const Real* p, Real (&v)[V]) {
   if constexpr (V == 1) {
     v[0] = __ldg(p);
   } else if constexpr (V == 2) {
-    const double2 w = __ldg(reinterpret_cast<const double2*>(p));
+    const auto w = __ldg(reinterpret_cast<const typename Vec16<Real, 2>::T*>(p));
     v[0] = w.x;
     v[1] = w.y;
   } else {
+    static_assert(V == 4 && sizeof(Real) == 4, "unsupported vector width");
     const float4 w = __ldg(reinterpret_cast<const float4*>(p));
     v[0] = w.x;
     v[1] = w.y;
@@ -386,14 +458,27 @@ __device__ __forceinline__ int64_t neighbour_offset(const KronParams<Real>& P, i
   return (int64_t)ca + 1 < n ? st : -(n - 1) * st;
 }
 
+// One staged neighbour-trace row (N Reals), V-wide.
+template <int N, typename Real>
+__device__ __forceinline__ void trace_row(const Real* p, Real (&v)[N]) {
+  constexpr int V = Kron3DShape<N, Real>::V;
+#pragma unroll
+  for (int r = 0; r < N; r += V) {
+    Real w[V];
+    vload<Real, V>(p + r, w);
+#pragma unroll
+    for (int q = 0; q < V; ++q) v[r + q] = w[q];
+  }
+}
+
 // Face terms of axis a added to a D-pass output Pm (plane [first][second]; the face slice is along
-// the first index when FIRST), from the element's face record (see stage_group).  nbval(side, r,
-// src, e_nb) reads the neighbour trace of that side from the group's staged DoFs (x only), the
-// axis' staged trace slot, or global memory.
-template <int N, typename Real, bool FIRST, typename NbVal>
+// the first index when FIRST), from the element's face record (see stage_group).  nbrow(side, src,
+// e_nb, v) reads this lane's row of the neighbour trace of that side from the group's staged DoFs
+// (x only), the axis' staged trace slot (V-wide), or global memory.
+template <int N, typename Real, bool FIRST, typename NbRow>
 __device__ __forceinline__ void kron_faces(const KronParams<Real>& P, int a, const uint32_t (&c)[3], int64_t e,
                                            uint32_t flags, const Real* rec, const Real (&U)[N][N], Real (&Pm)[N][N],
-                                           NbVal nbval) {
+                                           NbRow nbrow) {
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
     const int sl = s ? N - 1 : 0;
@@ -411,11 +496,12 @@ __device__ __forceinline__ void kron_faces(const KronParams<Real>& P, int a, con
       if (f & kRecNb) {
         const int src = (int)(f >> 3);
         const int64_t en = src == kTraceGlobal ? e + neighbour_offset(P, a, s, c[a]) : e;
+        Real v[N];
+        nbrow(s, src, en, v);
 #pragma unroll
         for (int r = 0; r < N; ++r) {
-          const Real v = nbval(s, r, src, en);
-          if (FIRST) Pm[sl][r] += k * v;
-          else Pm[r][sl] += k * v;
+          if (FIRST) Pm[sl][r] += k * v[r];
+          else Pm[r][sl] += k * v[r];
         }
       } else {
 #pragma unroll
@@ -582,11 +668,16 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
             for (int j = 0; j < N; ++j) px[i][j] *= elx;
         }
         if (active)
-          kron_faces<N, Real, true>(P, 0, c, e, fflags, rec, u, px, [&](int s, int r, int src, int64_t en) {
+          kron_faces<N, Real, true>(P, 0, c, e, fflags, rec, u, px, [&](int s, int src, int64_t en, Real(&v)[N]) {
             const int sl = s ? 0 : N - 1;  // the neighbour's opposite slice
-            if (src == kTraceLocal) return ub[(s ? 1 : -1) * S::SE + t * S::SP + sl + N * r];
-            if (src == kTraceSlot) return tb[0 * S::TS + t * S::TR + r];
-            return P.x[en * NNN + sl + N * r + NN * t];
+            if (src == kTraceSlot) {
+              trace_row<N>(tb + 0 * S::TS + t * S::TR, v);
+            } else {
+#pragma unroll
+              for (int r = 0; r < N; ++r)
+                v[r] = src == kTraceLocal ? ub[(s ? 1 : -1) * S::SE + t * S::SP + sl + N * r]
+                                          : P.x[en * NNN + sl + N * r + NN * t];
+            }
           });
         kron_apply<N, Real, kSlotTXY, false>(P, c[1], px, qx);
       }
@@ -599,9 +690,13 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
           for (int j = 0; j < N; ++j) py[i][j] *= ely;
       }
       if (active)
-        kron_faces<N, Real, false>(P, 1, c, e, fflags, rec, u, py, [&](int s, int r, int src, int64_t en) {
-          if (src == kTraceSlot) return tb[1 * S::TS + t * S::TR + r];
-          return P.x[en * NNN + r + N * (s ? 0 : N - 1) + NN * t];
+        kron_faces<N, Real, false>(P, 1, c, e, fflags, rec, u, py, [&](int s, int src, int64_t en, Real(&v)[N]) {
+          if (src == kTraceSlot) {
+            trace_row<N>(tb + 1 * S::TS + t * S::TR, v);
+          } else {
+#pragma unroll
+            for (int r = 0; r < N; ++r) v[r] = P.x[en * NNN + r + N * (s ? 0 : N - 1) + NN * t];
+          }
         });
       if constexpr (BFLY) {
         exchange_butterfly<N>(t, qx);
@@ -643,9 +738,13 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
             for (int k = 0; k < N; ++k) pz[i][k] *= elz;
         }
         if (active)
-          kron_faces<N, Real, false>(P, 2, c, e, fflags, rec, u, pz, [&](int s, int r, int src, int64_t en) {
-            if (src == kTraceSlot) return tb[2 * S::TS + t * S::TR + r];
-            return P.x[en * NNN + r + N * t + NN * (s ? 0 : N - 1)];
+          kron_faces<N, Real, false>(P, 2, c, e, fflags, rec, u, pz, [&](int s, int src, int64_t en, Real(&v)[N]) {
+            if (src == kTraceSlot) {
+              trace_row<N>(tb + 2 * S::TS + t * S::TR, v);
+            } else {
+#pragma unroll
+              for (int r = 0; r < N; ++r) v[r] = P.x[en * NNN + r + N * t + NN * (s ? 0 : N - 1)];
+            }
           });
       } else if (P.elem_mass) {
         const Real em = active ? P.elem_mass[e] : Real(1);
@@ -728,12 +827,18 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
         const int d = ch * S::CR;
         const int r = d / NNN, o = d - r * NNN;
         const int z = o / NN, w = o - z * NN;
-        const Real* sp = buf + r * S::SE + z * S::SP + w;
+        Real v[S::CR];
+        vload<Real, S::CR>(buf + r * S::SE + z * S::SP + w, v);
+        if (by == Real(0)) {
 #pragma unroll
-        for (int q = 0; q < S::CR; ++q) {
-          const Real v = sp[q];
-          dst[d + q] = (by == Real(0)) ? alpha * v : alpha * v + by * dst[d + q];
+          for (int q = 0; q < S::CR; ++q) v[q] = alpha * v[q];
+        } else {
+          Real o[S::CR];
+          vload<Real, S::CR>(dst + d, o);
+#pragma unroll
+          for (int q = 0; q < S::CR; ++q) v[q] = alpha * v[q] + by * o[q];
         }
+        vstore<Real, S::CR>(dst + d, v);
       }
     }
     __syncwarp();  // the buffer is refilled by a later prefetch
