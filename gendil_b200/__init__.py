@@ -94,6 +94,9 @@ def lib():
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
         L.dgop_solver_set_graphs.argtypes = [vp, i]
+        L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.dgop_host_io_apply.argtypes = [vp, vp, vp, vp]
+        L.dgop_host_io_destroy.argtypes = [vp]
         L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
         L.dgop_solver_destroy.argtypes = [vp]
         _lib = L
@@ -386,6 +389,39 @@ class GMRESIRSolver(_Solver):
         h = ctypes.c_void_p()
         check(lib().dgop_gmres_ir_create(op.handle, int(restart), prec, ctypes.byref(h)))
         self.handle = h
+
+
+class HostIO:
+    """y = A x for vectors in host memory (numpy arrays or CPU tensors, float64, contiguous):
+    upload, apply and download pipelined over slabs of element planes (dgop_host_io_apply)."""
+
+    def __init__(self, op, slabs=8):
+        self.op = op
+        h = ctypes.c_void_p()
+        check(lib().dgop_host_io_create(op.handle, int(slabs), ctypes.byref(h)))
+        self.handle = h
+
+    @staticmethod
+    def _host_ptr(a):
+        if isinstance(a, np.ndarray):
+            assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+            return a.ctypes.data
+        assert a.device.type == "cpu" and a.is_contiguous() and str(a.dtype) == "torch.float64"
+        return a.data_ptr()
+
+    def apply(self, x, y, stream=None):
+        check(lib().dgop_host_io_apply(self.handle, self._host_ptr(x), self._host_ptr(y), _stream(stream)))
+
+    def close(self):
+        if self.handle:
+            lib().dgop_host_io_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fill_random(n, seed=12345, lo=-1.0, hi=1.0):

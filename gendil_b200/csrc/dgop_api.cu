@@ -588,7 +588,9 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 
 template <typename Real>
 static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, Real alpha, const Real* x, Real beta_y,
-                       Real* y, int extra_flags, cudaStream_t s, const int* skip) {
+                       Real* y, int extra_flags, cudaStream_t s, const int* skip, int64_t e_begin = 0,
+                       int64_t e_end = -1) {
+  if (e_end < 0) e_end = op->sp.nelem;
   if (!x || !y) {
     set_error("null vector");
     return DGOP_ERR_ARG;
@@ -619,6 +621,8 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.beta_y = beta_y;
     p.flags = op->flags | extra_flags;
     p.skip = skip;
+    p.e_begin = e_begin;
+    p.nelem = e_end;
     if (linear) p.g = Real(0);
     const auto& KL = K.launch[K.variant];
     K.entry->v[K.variant].launch(p, KL.grid, KL.block, KL.smem, s);
@@ -637,6 +641,8 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   p.beta_y = beta_y;
   p.flags = op->flags | extra_flags;
   p.skip = skip;
+  p.e_begin = e_begin;
+  p.nelem = e_end;
   if (linear) p.g = Real(0);
   L.entry->launch(p, L.grid, L.block, L.smem, s);
   const cudaError_t e = cudaGetLastError();
@@ -652,6 +658,10 @@ int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s, const int* skip) {
   return launch_impl<float>(op, op->f32, op->k32, alpha, x, beta_y, y, extra_flags, s, skip);
+}
+
+int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s) {
+  return launch_impl<double>(op, op->f64, op->k64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
 }
 
 }  // namespace dgop

@@ -81,4 +81,6 @@ int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, 
                cudaStream_t s, const int* skip = nullptr);
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s, const int* skip = nullptr);
+// y = Op(x) on the elements [e_begin, e_end) only (y elsewhere untouched; x read around them)
+int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s);
 }  // namespace dgop

@@ -35,7 +35,8 @@ struct CoefDev {
 
 template <typename Real>
 struct OpParams {
-  int64_t nelem;
+  int64_t nelem;    // the launch processes elements [e_begin, nelem)
+  int64_t e_begin;
   int64_t sizes[kMaxDim];
   int64_t estride[kMaxDim];  // element linear index = sum_k e_k * estride[k], x fastest
   int periodic[kMaxDim];

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256) generic_kernel(const __grid_constant__ Op
   const Real detJ = P.detJ;
   const bool GLL = P.gll != 0;
 
-  for (int64_t e0 = (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
+  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
     __syncthreads();
     // element coordinates and neighbours (cartesianndmesh.hpp:95-198)

@@ -55,7 +55,8 @@ enum KronSlot : int {
 
 template <typename Real>
 struct KronParams {
-  int64_t nelem;      // < 2^32 (checked by the planner)
+  int64_t nelem;      // < 2^32 (checked by the planner); the launch processes [e_begin, nelem)
+  int64_t e_begin;
   FastDiv fdx, fdy;   // element index -> (x, y, z) coordinates
   int64_t sizes[3];
   int periodic[3];

@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
   const int le = lane / N, t = lane - le * N;
   Real* wbase = reinterpret_cast<Real*>(smem_raw) + (size_t)warp * S::warp_smem(STAGES, SHFL);
   [[maybe_unused]] Real* tile = wbase + STAGES * S::STAGE;
-  const int64_t ngroups = (P.nelem + EPW - 1) / EPW;
+  const int64_t ngroups = (P.nelem - P.e_begin + EPW - 1) / EPW;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const bool adv = P.has_adv != 0;
   const bool slot = le < EPW;
@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
 
   int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if constexpr (STAGES == 2) {
-    if (g < ngroups) stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), wbase, lane, le, t, adv);
+    if (g < ngroups) stage_group<N>(P, P.e_begin + g * EPW, group_size(EPW, P.nelem - P.e_begin - g * EPW), wbase, lane, le, t, adv);
     cp_async_commit();
   }
   for (int it = 0; g < ngroups; g += nwarps, ++it) {
@@ -631,17 +631,17 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
     if constexpr (STAGES == 2) {
       const int64_t gn = g + nwarps;
       if (gn < ngroups)
-        stage_group<N>(P, gn * EPW, group_size(EPW, P.nelem - gn * EPW), wbase + ((it + 1) & 1) * S::STAGE, lane, le,
+        stage_group<N>(P, P.e_begin + gn * EPW, group_size(EPW, P.nelem - P.e_begin - gn * EPW), wbase + ((it + 1) & 1) * S::STAGE, lane, le,
                        t, adv);
       cp_async_commit();
       cp_async_wait<1>();
     } else {
-      stage_group<N>(P, g * EPW, group_size(EPW, P.nelem - g * EPW), buf, lane, le, t, adv);
+      stage_group<N>(P, P.e_begin + g * EPW, group_size(EPW, P.nelem - P.e_begin - g * EPW), buf, lane, le, t, adv);
       cp_async_commit();
       cp_async_wait<0>();
     }
     __syncwarp();
-    const int64_t e0 = g * EPW;
+    const int64_t e0 = P.e_begin + g * EPW;
     const int ne = group_size(EPW, P.nelem - e0);
     const int64_t e = e0 + le;
     const bool active = slot && le < ne;

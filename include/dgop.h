@@ -112,6 +112,19 @@ int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* st
 /* FP32 apply of the same operator (tables rounded to FP32); no reference counterpart. */
 int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
 
+/* Applies on HOST vectors (the reference's operator() on a host-resident Vector,
+ * massoperator.hpp:209, advectionoperator.hpp:1070, where the data lives in host memory):
+ * y_host = A x_host.  The host-to-device copy, the apply and the device-to-host copy are pipelined
+ * over `slabs` ranges of element planes of the last axis (slabs <= 0: 8), so upload and download
+ * overlap.  The handle owns two device vectors and three streams (allocated at creation).  The
+ * call starts after the work queued on `stream`, makes `stream` wait for its end and returns when
+ * y_host is written.  Pinned host memory (cudaMallocHost / cudaHostRegister) copies at full link
+ * speed; pageable memory works, more slowly. */
+typedef struct dgop_host_io dgop_host_io;
+int dgop_host_io_create(dgop_operator* op, int slabs, dgop_host_io** out);
+int dgop_host_io_apply(dgop_host_io* io, const double* x_host, double* y_host, void* stream);
+int dgop_host_io_destroy(dgop_host_io* io);
+
 /* ---- Krylov solvers, device resident (workspaces allocated at create time).
  * CG: the reference's ConjugateGradient scratch overload (Solvers/conjugategradient.hpp:125-209),
  *   including its conventions: the tolerance is relative to the norm of the INITIAL residual
