@@ -53,6 +53,33 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+# FP64 work of the Kronecker-form apply: 9 n x n passes, each n FMA per DoF (n = 4), 2 flop per FMA
+# (face terms, about 3 FMA per DoF more, not counted)
+KRON_FLOP_PER_DOF = 9 * (ORDER + 1) * 2
+
+
+def fp64_gemm_peak(torch, dev):
+    """Measured FP64 dense throughput of this GPU: cuBLAS DGEMM 8192^3 through torch, best of 3
+    (CUDA events).  The denominator of the FP64 roofline of the apply kernel."""
+    n = 8192
+    a = torch.rand(n, n, dtype=torch.float64, device=dev)
+    b = torch.rand(n, n, dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    torch.matmul(a, b, out=c)
+    best = None
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
@@ -294,6 +321,12 @@ def run_ours(args):
                         "path": f"dgop_host_io_apply (pinned host vectors, {HOST_SLABS} slabs)"},
                 "gpu_launches": args.steps,
                 "clocks": clocks.summary()}
+        if op.kernel == "kron":
+            peak64 = fp64_gemm_peak(torch, dev)
+            a64 = KRON_FLOP_PER_DOF * nd / (ms_step * 1e-3) / 1e12
+            line["roofline_fp64"] = {"bound": "fp64", "achieved": a64, "peak": peak64, "unit": "TFLOP/s",
+                                     "frac": a64 / peak64, "flop_per_dof": KRON_FLOP_PER_DOF,
+                                     "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch), best of 3"}
         line["config"]["kernel"] = op.kernel
         if op.variant:
             line["config"]["kernel_variant"] = op.variant
