@@ -94,6 +94,8 @@ def lib():
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
         L.dgop_solver_set_graphs.argtypes = [vp, i]
+        L.dgop_solver_set_transpose.argtypes = [vp, i]
+        L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_host_io_apply.argtypes = [vp, vp, vp, vp]
         L.dgop_host_io_destroy.argtypes = [vp]
@@ -340,6 +342,11 @@ class _Solver:
                                       _stream(stream)))
         return {"success": bool(res.success), "iterations": res.iterations, "relative_error": res.relative_error}
 
+    def transpose(self, enable=True):
+        """Solve with the transposed operator A^T (adjoint solves)."""
+        check(lib().dgop_solver_set_transpose(self.handle, 1 if enable else 0))
+        return self
+
     def use_graphs(self, enable=True):
         """Replay solver segments from CUDA graphs (default) or launch every kernel directly."""
         check(lib().dgop_solver_set_graphs(self.handle, 1 if enable else 0))
@@ -422,6 +429,16 @@ class HostIO:
             self.close()
         except Exception:
             pass
+
+
+def element_dot(op, a, b, scale=None, out=None, stream=None):
+    """out[e] = scale[e] * sum over the DoFs of element e of a * b (FP64 device tensors)."""
+    import torch
+    if out is None:
+        out = torch.empty(op.space.num_elements, dtype=torch.float64, device=a.device)
+    check(lib().dgop_element_dot(op.handle, _ptr(a), _ptr(b), None if scale is None else _ptr(scale), _ptr(out),
+                                 _stream(stream)))
+    return out
 
 
 def fill_random(n, seed=12345, lo=-1.0, hi=1.0):

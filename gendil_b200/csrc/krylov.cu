@@ -11,6 +11,7 @@
 // fixed reduction tree, and every consumer sums the partials in the same fixed order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <new>
@@ -504,6 +505,25 @@ __global__ void __launch_bounds__(kRT) k_gs_rescale(const GMState* st, T* v, int
   }
 }
 
+// ------------------------------------------------------------- per-element inner products
+
+// out[e] = scale[e] * sum_{i in element e} a_i b_i  (one warp per element, fixed summation order)
+__global__ void __launch_bounds__(kRT) k_element_dot(const double* __restrict__ a, const double* __restrict__ b,
+                                                     const double* __restrict__ scale, double* __restrict__ out,
+                                                     int64_t nelem, int64_t nd) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (kRT / 32);
+  for (int64_t e = (int64_t)blockIdx.x * (kRT / 32) + (threadIdx.x >> 5); e < nelem; e += warps) {
+    const double* pa = a + e * nd;
+    const double* pb = b + e * nd;
+    double v = 0.0;
+    for (int64_t i = lane; i < nd; i += 32) v += pa[i] * pb[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) out[e] = scale ? scale[e] * v : v;
+  }
+}
+
 }  // namespace
 
 struct SolverImpl {
@@ -526,7 +546,8 @@ struct SolverImpl {
   cudaGraphExec_t exec = nullptr;
   const void* key_b = nullptr;
   const void* key_x = nullptr;
-  int key_version = -1;
+  int key_version = -1, key_flags = -1;
+  int op_flags = 0;  // extra operator flags of every apply (kTranspose: solve with A^T)
   // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -586,7 +607,8 @@ void solver_free(dgop_solver* sv) {
 template <typename F>
 int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&& enqueue) {
   if (!s.use_graphs) return enqueue(st);
-  const bool same = s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version;
+  const bool same =
+      s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version && s.key_flags == s.op_flags;
   if (!same) {
     if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
     DGOP_CUDA_S(cudaStreamBeginCapture(s.cap, cudaStreamCaptureModeThreadLocal));
@@ -609,6 +631,7 @@ int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&
     s.key_b = b;
     s.key_x = x;
     s.key_version = s.op->version;
+    s.key_flags = s.op_flags;
   }
   DGOP_CUDA_S(cudaGraphLaunch(s.exec, st));
   return DGOP_OK;
@@ -655,7 +678,7 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
   double* pb = s.partials + kRB;
   CGState* cs = static_cast<CGState*>(s.state);
   // 1) r = rhs - A x
-  DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, tmp, 0, st));
+  DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, tmp, s.op_flags, st));
   k_sub_norm<<<kRB, kRT, 0, st>>>(b, tmp, r, n, pa, nullptr);
   k_cg_init<<<1, kRT, 0, st>>>(cs, pa, tol, max_iters);
   k_cg_init_p<<<kRB, kRT, 0, st>>>(cs, r, p, x, n);
@@ -664,7 +687,7 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
   const int* done = &cs->done;
   auto chunk = [&](cudaStream_t q) -> int {
     for (int kk = 0; kk < kCheckEvery; ++kk) {
-      DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, 0, q, done));
+      DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, s.op_flags, q, done));
       k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(p), static_cast<const double*>(tmp), n, pa, done);
       k_cg_update<<<kRB, kRT, 0, q>>>(kk, cs, x, r, p, tmp, n, pa, pb);
       k_cg_finish<<<kRB, kRT, 0, q>>>(kk, cs, r, p, n, pb);
@@ -699,7 +722,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   const int* done = &gs->done;
   const int* inactive = &gs->inactive;
   auto residual = [&](int phase, cudaStream_t q) -> int {
-    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, 0, q, done));
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w, s.op_flags, q, done));
     k_sub_norm<<<kRB, kRT, 0, q>>>(b, w, V, n, pa, done);
     k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, phase);
     DGOP_CUDA_S(cudaGetLastError());
@@ -710,7 +733,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
     for (int j = 0; j < m; ++j) {
       double* vj = V + (int64_t)j * n;
-      DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, 0, q, inactive));
+      DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, s.op_flags, q, inactive));
       k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(V), static_cast<const double*>(w), n, pa, inactive);
       double* pin = pa;
       double* pout = pb;
@@ -751,11 +774,11 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
 // The padding entries are zero from creation on and stay zero.
 int64_t ir_stride(int64_t n) { return (n + 63) / 64 * 64; }
 
-int apply_inner(dgop_operator* op, const float* x, float* y, cudaStream_t st, const int* skip) {
-  return launch_f32(op, 1.0f, x, 0.0f, y, kLinear, st, skip);
+int apply_inner(dgop_operator* op, const float* x, float* y, int flags, cudaStream_t st, const int* skip) {
+  return launch_f32(op, 1.0f, x, 0.0f, y, kLinear | flags, st, skip);
 }
-int apply_inner(dgop_operator* op, const double* x, double* y, cudaStream_t st, const int* skip) {
-  return launch_f64(op, 1.0, x, 0.0, y, kLinear, st, skip);
+int apply_inner(dgop_operator* op, const double* x, double* y, int flags, cudaStream_t st, const int* skip) {
+  return launch_f64(op, 1.0, x, 0.0, y, kLinear | flags, st, skip);
 }
 
 // GMRES with iterative refinement: every restart cycle solves the correction equation A d = r
@@ -786,7 +809,7 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
   const int* done = &gs->done;
   const int* inactive = &gs->inactive;
   auto residual = [&](int phase, cudaStream_t q) -> int {
-    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, 0, q, done));
+    DGOP_TRY(launch_f64(s.op, 1.0, x, 0.0, w64, s.op_flags, q, done));
     k_sub_norm<<<kRB, kRT, 0, q>>>(b, w64, r64, n, pa, done);
     k_gm_resid<<<1, kRT, 0, q>>>(gs, pa, phase);
     DGOP_CUDA_S(cudaGetLastError());
@@ -798,7 +821,7 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
     for (int j = 0; j < m; ++j) {
       T* vj = V + (int64_t)j * ld;
       T* vn = vj + ld;
-      DGOP_TRY(apply_inner(s.op, vj, w, q, inactive));
+      DGOP_TRY(apply_inner(s.op, vj, w, s.op_flags, q, inactive));
       const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
       k_gs_dots<T><<<dgrid, kRT, 0, q>>>(gs, V, ld, j, w, s.wide);
       k_gs_h<<<j + 1, kRT, 0, q>>>(gs, j, m, H, s.wide);
@@ -951,6 +974,29 @@ int dgop_solver_set_graphs(dgop_solver* sv, int enable) {
     return DGOP_ERR_ARG;
   }
   sv->s.use_graphs = enable != 0;
+  return DGOP_OK;
+}
+
+int dgop_solver_set_transpose(dgop_solver* sv, int transpose) {
+  if (!sv) {
+    set_error("dgop_solver_set_transpose: null solver");
+    return DGOP_ERR_ARG;
+  }
+  sv->s.op_flags = transpose ? kTranspose : 0;
+  return DGOP_OK;
+}
+
+int dgop_element_dot(const dgop_operator* op, const double* a, const double* b, const double* scale, double* out,
+                     void* stream) {
+  if (!op || !a || !b || !out) {
+    set_error("dgop_element_dot: null argument");
+    return DGOP_ERR_ARG;
+  }
+  const int64_t nelem = op->sp.nelem, nd = op->sp.ndofs / op->sp.nelem;
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((nelem + kRT / 32 - 1) / (kRT / 32), 4 * kRB));
+  k_element_dot<<<(unsigned)blocks, kRT, 0, (cudaStream_t)stream>>>(a, b, scale, out, nelem, nd);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "dgop_element_dot launch");
   return DGOP_OK;
 }
 

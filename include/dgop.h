@@ -162,6 +162,17 @@ int dgop_solver_destroy(dgop_solver* solver);
  * change (tolerance and iteration limit live in device memory).  enable = 0 launches every kernel directly instead (same results, bit for
  * bit).  No reference counterpart. */
 int dgop_solver_set_graphs(dgop_solver* solver, int enable);
+/* transpose != 0: the solver solves A^T x = b (the adjoint of the operator's linear part, inflow
+ * value 0; dgop_apply_transpose) with the same algorithm; used by adjoint solves.  No reference
+ * counterpart. */
+int dgop_solver_set_transpose(dgop_solver* solver, int transpose);
+
+/* Per-element inner products: out[e] = scale[e] * sum over the DoFs i of element e of a_i b_i
+ * (scale NULL: 1), for the vectors of op's space (device pointers).  With a the adjoint state and
+ * b = (dA/dc_e) u this is the gradient of a solve-based loss with respect to per-element
+ * coefficient factors c_e.  No reference counterpart. */
+int dgop_element_dot(const dgop_operator* op, const double* a, const double* b, const double* scale, double* out,
+                     void* stream);
 
 /* CG without any allocation at call time (no counterpart in the reference).  For callers that
  * must not let a library allocate device memory: a host framework that owns all device memory
