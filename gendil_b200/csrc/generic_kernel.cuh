@@ -366,8 +366,23 @@ __global__ void __launch_bounds__(256) generic_kernel(const __grid_constant__ Op
           if (!transpose) {
             up = (dot > Real(0)) ? dot * own : dot * other;
           } else {
-            const Real lin_other = interior ? other : Real(0);
-            up = (dot > Real(0)) ? dot * (own - lin_other) : Real(0);
+            // row e of A^T on this face: e's own outflow term, plus the neighbour's inflow term
+            // when the neighbour takes e's trace, with the neighbour's velocity (its own
+            // coefficient and per-element factor; equal to -dot for a continuous field)
+            up = (dot > Real(0)) ? dot * own : Real(0);
+            if (interior) {
+              int cn[D], jn[D];
+#pragma unroll
+              for (int k = 0; k < D; ++k) {
+                cn[k] = sidx[b * D + k];
+                jn[k] = j[k];
+              }
+              const int na = (int)P.sizes[a];
+              cn[a] = s ? (cn[a] + 1 == na ? 0 : cn[a] + 1) : (cn[a] == 0 ? na - 1 : cn[a] - 1);
+              jn[a] = Q + 1 - s;
+              const Real dot_nb = -coef_eval<D>(P.beta[a], P.tab, P.tab_ld, cn, jn, nb) * nrm;
+              if (!(dot_nb > Real(0))) up += dot_nb * other;
+            }
           }
           *own_p = (D == 1 ? detJ : weight * detJ) * up;
         }

@@ -897,6 +897,7 @@ struct OperatorPlan {
   std::shared_ptr<const detail::VectorField> beta;
   std::shared_ptr<const detail::ScalarField> outflow;  // boundary indicator (null: 1)
   std::shared_ptr<const detail::ScalarField> inflow;   // legacy bc(X) (null: 0 or no boundary)
+  const Real* beta_factor = nullptr;  // per-element velocity factor (device, num_elements; null: 1)
   std::string describe() const {
     std::ostringstream s;
     s << (mass ? "mass" : "") << (mass && cell ? "+" : "") << (cell ? "cell" : "") << (interior ? "+interior" : "")
@@ -1100,14 +1101,15 @@ class Operator {
   const OperatorPlan& plan() const { return plan_; }
   std::string KernelName() const { return dgop_operator_kernel(op_.get()) == DGOP_KERNEL_KRON ? "kron" : "generic"; }
 
-  // device-resident solvers, created once per (kind, restart, inner precision)
+  // device-resident solvers, created once per (kind, restart, inner precision); kind 0 CG,
+  // 1 GMRES, 2 refinement GMRES, 3 a second GMRES handle (the adjoint solve's)
   dgop_solver* solver(int kind, int restart, int inner) const {
     const auto key = std::make_tuple(kind, restart, inner);
     auto it = solvers_.find(key);
     if (it != solvers_.end()) return it->second->get();
     dgop_solver* s = nullptr;
     if (kind == 0) detail::check(dgop_cg_create(op_.get(), &s), "ConjugateGradient");
-    else if (kind == 1) detail::check(dgop_gmres_create(op_.get(), restart, &s), "GMRES");
+    else if (kind == 1 || kind == 3) detail::check(dgop_gmres_create(op_.get(), restart, &s), "GMRES");
     else detail::check(dgop_gmres_ir_create(op_.get(), restart, inner, &s), "refinement GMRES");
     auto h = std::make_shared<SolverHandle>(s);
     solvers_[key] = h;
@@ -1161,6 +1163,7 @@ class Operator {
             },
             "velocity '" + bf->name + "' component " + std::to_string(c));
         bsep[c].fill(beta[c]);
+        beta[c].element_factor = plan_.beta_factor;
       }
       if (plan_.boundary) g_in = check_boundary(g);
     }
@@ -1310,5 +1313,81 @@ IterativeSolverResult RefinedGMRES(const Operator<D>& A, const Vector& rhs, Inte
                                    Real tol, Vector& x, bool fp32_inner = true) {
   return detail::solve(A.solver(2, (int)restart, fp32_inner ? DGOP_FP32 : DGOP_FP64), rhs, x, max_iters, tol);
 }
+
+// ------------------------------------------------------------------------- adjoint gradients
+// Forward/backward pair for u = S(theta)^{-1} b with S(theta) = M_sigma + A(theta_e beta(X)) and
+// inflow value bc (one constant): theta holds one velocity factor per element.  Backward gives,
+// for an upstream gradient dJ/du, dJ/db = S^{-T} dJ/du and
+//   dJ/dtheta_e = -s_e (dJ/db)_e . (A(s beta) u)_e,   s_e = sign(theta_e),
+// because the rows of element e depend on theta_e alone (own cell term and own face fluxes).
+// Forward and adjoint solves run GMRES(restart) on the device; no Krylov iterate is stored.  No
+// reference counterpart.
+template <Integer D>
+class AdvectionSolveFunction {
+ public:
+  template <typename Sigma, typename Adv, typename BC>
+  AdvectionSolveFunction(const FiniteElementSpace<D>& fes, const IntegrationRule<D>& ir, const Sigma& sigma,
+                         const Adv& adv, const BC& bc, Integer restart = 30, Real tol = 1e-12,
+                         Integer max_iters = 20000)
+      : fes_(fes), ir_(ir), restart_(restart), tol_(tol), max_iters_(max_iters) {
+    plan_.mass = plan_.cell = plan_.interior = plan_.boundary = true;
+    plan_.sigma = detail::make_scalar(sigma, "sigma");
+    plan_.beta = detail::make_vector(adv, "adv");
+    plan_.inflow = detail::make_scalar(bc, "boundary value");
+  }
+
+  IterativeSolverResult Forward(const Vector& theta, const Vector& b, Vector& u) {
+    theta_ = theta;
+    u_ = Vector(b.Size());
+    u_ = 0.0;
+    op_ = std::make_unique<Operator<D>>(fes_, ir_, with_factor(plan_, theta_.ReadDeviceData()));
+    const IterativeSolverResult r =
+        detail::solve(op_->solver(1, (int)restart_, 0), b, u_, max_iters_, tol_);
+    u = u_;
+    return r;
+  }
+
+  IterativeSolverResult Backward(const Vector& grad_u, Vector& grad_theta, Vector& grad_b) {
+    if (!op_) throw Error("AdvectionSolveFunction: Backward before Forward");
+    dgop_solver* adj = op_->solver(3, (int)restart_, 0);
+    grad_b = Vector(grad_u.Size());
+    grad_b = 0.0;
+    detail::check(dgop_solver_set_transpose(adj, 1), "adjoint solve");
+    const IterativeSolverResult r = detail::solve(adj, grad_u, grad_b, max_iters_, tol_);
+    // s = sign(theta) and the advection part with element factors s
+    const Integer ne = fes_.GetNumberOfFiniteElements();
+    Vector s(ne);
+    {
+      const Real* t = theta_.ReadHostData();
+      Real* sp = s.WriteHostData();
+      for (Integer e = 0; e < ne; ++e) sp[e] = t[e] < 0.0 ? -1.0 : 1.0;
+    }
+    OperatorPlan adv = plan_;
+    adv.mass = false;
+    Operator<D> A(fes_, ir_, with_factor(adv, s.ReadDeviceData()));
+    Vector w(u_.Size());
+    A(u_, w);
+    grad_theta = Vector(ne);
+    detail::check(dgop_element_dot(A.handle(), grad_b.ReadDeviceData(), w.ReadDeviceData(), s.ReadDeviceData(),
+                                   grad_theta.WriteDeviceData(), nullptr),
+                  "element products");
+    grad_theta *= -1.0;
+    return r;
+  }
+
+ private:
+  static OperatorPlan with_factor(OperatorPlan p, const Real* factor) {
+    p.beta_factor = factor;
+    return p;
+  }
+  FiniteElementSpace<D> fes_;
+  IntegrationRule<D> ir_;
+  Integer restart_;
+  Real tol_;
+  Integer max_iters_;
+  OperatorPlan plan_;
+  Vector theta_, u_;
+  std::unique_ptr<Operator<D>> op_;
+};
 
 }  // namespace gendil_b200

@@ -241,6 +241,43 @@ int run_mode(const char* path) {
     report("G_refined", RefinedGMRES(A, b, 5000, 30, 1e-10, x));
     record("G_refined_x", x);
   }
+  {  // H: adjoint gradient of J = |u - u*|^2 / 2 w.r.t. per-element velocity factors, with
+     // central differences through the forward solve
+    CartesianMesh<3> mesh({3, 3, 2}, {1.0 / 3, 1.0 / 3, 0.5}, {0.0, 0.0, 0.0});
+    auto fes = MakeFiniteElementSpace(mesh, MakeLobattoFiniteElement(FiniteElementOrders<2, 2, 2>{}));
+    auto ir = MakeIntegrationRule(IntegrationRuleNumPoints<3, 3, 3>{});
+    auto sigma = [](const std::array<Real, 3>&) { return 20.0; };
+    auto g_in = [](const std::array<Real, 3>&) { return 0.3; };
+    AdvectionSolveFunction<3> fn(fes, ir, sigma, adv_sincos, g_in, 30, 1e-14);
+    const Integer ne = fes.GetNumberOfFiniteElements();
+    Vector theta(ne), b(fes), target(fes), u(fes);
+    FillRandom(theta, 11, 0.5, 1.5);
+    FillRandom(b, 5);
+    FillRandom(target, 6);
+    auto loss = [&](const Vector& th) {
+      Vector uu(fes);
+      fn.Forward(th, b, uu);
+      Real J = 0.0;
+      for (Integer i = 0; i < uu.Size(); ++i) J += 0.5 * (uu[i] - target[i]) * (uu[i] - target[i]);
+      return J;
+    };
+    report("H_forward", fn.Forward(theta, b, u));
+    Vector grad_u(fes), grad_theta, grad_b;
+    for (Integer i = 0; i < u.Size(); ++i) grad_u[i] = u[i] - target[i];
+    report("H_adjoint", fn.Backward(grad_u, grad_theta, grad_b));
+    Real gmax = 0.0, worst = 0.0;
+    for (Integer e = 0; e < ne; ++e) gmax = std::max(gmax, std::fabs(grad_theta[e]));
+    const Real eps = 1e-6;
+    for (Integer e : {Integer(0), Integer(5), Integer(9), ne - 1}) {
+      Vector tp = theta, tm = theta;
+      tp[e] += eps;
+      tm[e] -= eps;
+      const Real fd = (loss(tp) - loss(tm)) / (2 * eps);
+      worst = std::max(worst, std::fabs(fd - grad_theta[e]));
+    }
+    std::printf("check H_fd %.6g\n", worst / gmax);
+    record("H_grad_theta", grad_theta);
+  }
   std::fclose(g_out);
   return 0;
 }

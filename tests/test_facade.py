@@ -83,11 +83,14 @@ def test_facade_operators_and_solvers_match_the_oracle(facade_bin, tmp_path):
     r = subprocess.run([facade_bin, "run", out], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     vec = _read_records(out)
-    solves = {}
+    solves, checks = {}, {}
     for line in r.stdout.splitlines():
         if line.startswith("solve "):
             _, name, ok, it, rel = line.split()
             solves[name] = {"success": ok == "1", "iterations": int(it), "relative_error": float(rel)}
+        elif line.startswith("check "):
+            _, name, val = line.split()
+            checks[name] = float(val)
     o = oracle()
     fr = lambda case, seed: o.fill_random(int(np.prod(case["sizes"])) * (case["P"] + 1) ** case["D"], seed)
 
@@ -131,3 +134,7 @@ def test_facade_operators_and_solvers_match_the_oracle(facade_bin, tmp_path):
     assert rel_max(vec["G_gmres_x"], arr["gm1_x"]) < 1e-8
     assert solves["G_refined"]["success"] and solves["G_refined"]["relative_error"] <= 1e-10
     assert rel_max(vec["G_refined_x"], arr["gm1_x"]) < 1e-8
+
+    # adjoint gradient (AdvectionSolveFunction) against central differences
+    assert solves["H_forward"]["success"] and solves["H_adjoint"]["success"]
+    assert checks["H_fd"] <= 1e-6
