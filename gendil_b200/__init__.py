@@ -235,15 +235,16 @@ class _Operator:
 
     @property
     def kernel(self):
-        """'generic' (sum-factorized) or 'kron' (register-resident Kronecker form)."""
-        return ("generic", "kron")[lib().dgop_operator_kernel(self.handle)]
+        """'generic' (sum-factorized), 'kron' (register-resident 3D Kronecker form) or 'kronnd'
+        (shared-memory Kronecker form, any dimension)."""
+        return ("generic", "kron", "kronnd")[lib().dgop_operator_kernel(self.handle)]
 
     @property
     def kernel_note(self):
         return lib().dgop_operator_kernel_note(self.handle).decode()
 
     def select_kernel(self, name):
-        check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1}[name]))
+        check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1, "kronnd": 2}[name]))
 
     VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl")
 

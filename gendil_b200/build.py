@@ -75,6 +75,9 @@ def _jobs(fast):
         path = os.path.join(CSRC, src)
         if os.path.exists(path):
             jobs.append((src, path, []))
+    gnd = os.path.join(CSRC, "gen_kronnd.cu")
+    for d in range(1, 7):
+        jobs.append((f"gen_kronnd_d{d}.cu", gnd, [f"-DDGOP_GEN_D={d}"]))
     gen = os.path.join(CSRC, "gen_generic.cu")
     for d in range(1, 7):
         for n in range(1, 9):

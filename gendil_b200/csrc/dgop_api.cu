@@ -453,6 +453,126 @@ int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
   return DGOP_OK;
 }
 
+// Any-dimension Kronecker kernel: matrix tables, face tables and launch shape.
+template <typename Real>
+int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan, const double* elem_sigma,
+                 const double* const* elem_beta) {
+  const dgop_space& s = op->sp;
+  const int D = s.D, N = s.n;
+  const KronNDEntry<Real>* entry = nullptr;
+  if constexpr (sizeof(Real) == 8) entry = &kronnd_slot_f64(D, N);
+  else entry = &kronnd_slot_f32(D, N);
+  if (!entry->launch) {
+    set_error("no any-dimension Kronecker kernel for this shape");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  K.entry = entry;
+  KronNDParams<Real>& p = K.params;
+  std::memset(&p, 0, sizeof(p));
+  p.nelem = s.nelem;
+  int64_t stride = 1;
+  for (int k = 0; k < D; ++k) {
+    p.sizes[k] = s.sizes[k];
+    p.estride[k] = stride;
+    stride *= s.sizes[k];
+    p.periodic[k] = s.periodic[k];
+  }
+  p.flags = op->flags;
+  p.has_adv = plan.has_adv;
+  p.has_mass = plan.has_mass;
+  p.mass_merged = plan.mass_merged;
+  p.g = (Real)op->g;
+  int rc = upload<Real>(&K.d_mats, plan.mats.data(), plan.mats.size());
+  if (rc) return rc;
+  p.mats = K.d_mats;
+  for (int a = 0; a < kMaxDim; ++a) {
+    for (int k = 0; k < kMaxDim; ++k) p.slot[a][k] = KronMat{};
+    p.mslot[a] = KronMat{};
+  }
+  if (plan.has_adv) {
+    for (int a = 0; a < D; ++a)
+      for (int k = 0; k < D; ++k) p.slot[a][k] = (k == a) ? plan.D[a] : plan.T[a][k];
+    std::vector<double> phi;
+    std::vector<signed char> sg;
+    size_t phi_off[kMaxDim], sg_off[kMaxDim][kMaxDim];
+    for (int a = 0; a < D; ++a) {
+      phi_off[a] = phi.size();
+      phi.insert(phi.end(), plan.phi[a].begin(), plan.phi[a].end());
+      for (int k = 0; k < D; ++k) {
+        sg_off[a][k] = sg.size();
+        sg.insert(sg.end(), plan.sgn[a][k].begin(), plan.sgn[a][k].end());
+      }
+    }
+    rc = upload<Real>(&K.d_phi, phi.data(), phi.size());
+    if (rc) return rc;
+    DGOP_CUDA(cudaMalloc(&K.d_sgn, sg.size() ? sg.size() : 1));
+    if (!sg.empty()) DGOP_CUDA(cudaMemcpy(K.d_sgn, sg.data(), sg.size(), cudaMemcpyHostToDevice));
+    for (int a = 0; a < D; ++a) {
+      p.phi[a] = K.d_phi + phi_off[a];
+      for (int k = 0; k < D; ++k) p.sgn[a][k] = (k == a) ? nullptr : K.d_sgn + sg_off[a][k];
+    }
+  }
+  if (plan.has_mass && !(plan.has_adv && plan.mass_merged)) {
+    p.mslot[D - 1] = plan.MD;
+    for (int k = 0; k < D - 1; ++k) p.mslot[k] = plan.MT[k];
+  }
+  auto elem_ptr = [&](const double* src, int slot, const Real** dst) -> int {
+    *dst = nullptr;
+    if (!src) return DGOP_OK;
+    if constexpr (sizeof(Real) == 8) {
+      *dst = src;
+    } else {
+      DGOP_CUDA(cudaMalloc(&K.d_elem[slot], sizeof(Real) * s.nelem));
+      convert_kernel<Real><<<256, 256>>>(src, K.d_elem[slot], s.nelem);
+      DGOP_CUDA(cudaGetLastError());
+      *dst = K.d_elem[slot];
+    }
+    return DGOP_OK;
+  };
+  for (int a = 0; a < D; ++a)
+    if ((rc = elem_ptr(plan.has_adv ? elem_beta[a] : nullptr, a, &p.elem[a]))) return rc;
+  if ((rc = elem_ptr(plan.has_mass ? elem_sigma : nullptr, kMaxDim, &p.elem_mass))) return rc;
+  // elements per CTA: as many as fit in ~96 KB (at most 64), one at least
+  const size_t per = (size_t)entry->per_elem * sizeof(Real);
+  int eb = (int)std::max<size_t>(1, std::min<size_t>(64, (96 * 1024) / per));
+  const int64_t lines = (int64_t)(s.ndofs / s.nelem) / N;
+  while (eb > 1 && (int64_t)(eb / 2) * lines >= 4 * kKronNDThreads) eb /= 2;  // enough work, more CTAs
+  int max_smem = 0;
+  DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+  while (eb > 1 && per * eb > (size_t)max_smem) --eb;
+  if (per * eb > (size_t)max_smem) {
+    set_error("element does not fit in shared memory");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  p.eb = eb;
+  K.params_t = p;
+  if (plan.has_adv)
+    for (int a = 0; a < D; ++a) K.params_t.slot[a][a] = plan.Dt[a];
+  K.block = dim3(kKronNDThreads);
+  K.smem = per * eb;
+  DGOP_CUDA(cudaFuncSetAttribute(entry->func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  int per_sm = 0;
+  DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, entry->func, kKronNDThreads, K.smem));
+  if (per_sm < 1) {
+    set_error("any-dimension Kronecker kernel cannot be resident");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  const int64_t ctas = std::min<int64_t>((s.nelem + eb - 1) / eb, (int64_t)device_sm_count(op->device) * per_sm);
+  K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+  K.ready = true;
+  return DGOP_OK;
+}
+
+template <typename Real>
+void free_kronnd(KronNDCfg<Real>& K) {
+  if (K.d_mats) cudaFree(K.d_mats);
+  if (K.d_phi) cudaFree(K.d_phi);
+  if (K.d_sgn) cudaFree(K.d_sgn);
+  for (auto* p : K.d_elem)
+    if (p) cudaFree(p);
+  K = KronNDCfg<Real>{};
+}
+
 template <typename Real>
 void free_kron(KronCfg<Real>& K) {
   if (K.d_mats) cudaFree(K.d_mats);
@@ -555,6 +675,19 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
       in.beta[k] = sep_of(adv ? &beta[k] : nullptr);
       elem_beta[k] = adv ? beta[k].element_factor : nullptr;
     }
+    // any-dimension kernel: every shape the Kronecker form covers (also the 3D register kernel's,
+    // where it is an alternative the caller may select)
+    KronPlanHost plan_nd = plan_kron(in);
+    if (plan_nd.ok && (int64_t)op->sp.nelem < (int64_t(1) << 40)) {
+      const double* es = sg ? sg->element_factor : nullptr;
+      if (setup_kronnd<double>(op, op->n64, plan_nd, es, elem_beta) == DGOP_OK) {
+        if (setup_kronnd<float>(op, op->n32, plan_nd, es, elem_beta) != DGOP_OK) free_kronnd(op->n32);
+        op->kernel = DGOP_KERNEL_KRONND;
+      } else {
+        free_kronnd(op->n64);
+      }
+      set_error("");
+    }
     KronPlanHost plan = plan_kron3d(in);
     if (plan.ok) {
       const double* es = sg ? sg->element_factor : nullptr;
@@ -573,9 +706,10 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
       op->kron_why = plan.why;
     }
   }
-  if (!op->f64.ready && !op->k64.ready) {
+  if (!op->f64.ready && !op->k64.ready && !op->n64.ready) {
     free_launch(op->f32);
     free_kron(op->k32);
+    free_kronnd(op->n32);
     delete op;
     set_error(generic_err.empty() ? std::string("no kernel for this operator") : generic_err);
     return DGOP_ERR_UNSUPPORTED;
@@ -587,9 +721,9 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 }  // namespace
 
 template <typename Real>
-static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, Real alpha, const Real* x, Real beta_y,
-                       Real* y, int extra_flags, cudaStream_t s, const int* skip, int64_t e_begin = 0,
-                       int64_t e_end = -1) {
+static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, KronNDCfg<Real>& KN, Real alpha,
+                       const Real* x, Real beta_y, Real* y, int extra_flags, cudaStream_t s, const int* skip,
+                       int64_t e_begin = 0, int64_t e_end = -1) {
   if (e_end < 0) e_end = op->sp.nelem;
   if (!x || !y) {
     set_error("null vector");
@@ -613,6 +747,22 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   }
   const bool linear = (extra_flags & kLinear) != 0;
   extra_flags &= ~kLinear;
+  if (op->kernel == DGOP_KERNEL_KRONND && KN.ready) {
+    KronNDParams<Real> p = (extra_flags & kTranspose) ? KN.params_t : KN.params;
+    p.x = x;
+    p.y = y;
+    p.alpha = alpha;
+    p.beta_y = beta_y;
+    p.flags = op->flags | extra_flags;
+    p.skip = skip;
+    p.e_begin = e_begin;
+    p.nelem = e_end;
+    if (linear) p.g = Real(0);
+    KN.entry->launch(p, KN.grid, KN.block, KN.smem, s);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
+    return DGOP_OK;
+  }
   if (op->kernel == DGOP_KERNEL_KRON && K.ready && aligned16) {
     KronParams<Real> p = (extra_flags & kTranspose) ? K.params_t : K.params;
     p.x = x;
@@ -652,16 +802,16 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
 
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
                cudaStream_t s, const int* skip) {
-  return launch_impl<double>(op, op->f64, op->k64, alpha, x, beta_y, y, extra_flags, s, skip);
+  return launch_impl<double>(op, op->f64, op->k64, op->n64, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s, const int* skip) {
-  return launch_impl<float>(op, op->f32, op->k32, alpha, x, beta_y, y, extra_flags, s, skip);
+  return launch_impl<float>(op, op->f32, op->k32, op->n32, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s) {
-  return launch_impl<double>(op, op->f64, op->k64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
+  return launch_impl<double>(op, op->f64, op->k64, op->n64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
 }
 
 }  // namespace dgop
@@ -795,6 +945,8 @@ int dgop_operator_destroy(dgop_operator* op) {
   free_launch(op->f32);
   free_kron(op->k64);
   free_kron(op->k32);
+  free_kronnd(op->n64);
+  free_kronnd(op->n32);
   delete op;
   return DGOP_OK;
 }
@@ -806,12 +958,16 @@ int dgop_operator_kernel(const dgop_operator* op) { return op ? op->kernel : -1;
 const char* dgop_operator_kernel_note(const dgop_operator* op) { return op ? op->kron_why : ""; }
 
 int dgop_operator_select_kernel(dgop_operator* op, int kernel) {
-  if (!op || (kernel != DGOP_KERNEL_GENERIC && kernel != DGOP_KERNEL_KRON)) {
+  if (!op || (kernel != DGOP_KERNEL_GENERIC && kernel != DGOP_KERNEL_KRON && kernel != DGOP_KERNEL_KRONND)) {
     set_error("dgop_operator_select_kernel: bad arguments");
     return DGOP_ERR_ARG;
   }
   if (kernel == DGOP_KERNEL_KRON && !op->k64.ready) {
     set_error(std::string("Kronecker kernel unavailable: ") + op->kron_why);
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (kernel == DGOP_KERNEL_KRONND && !op->n64.ready) {
+    set_error("any-dimension Kronecker kernel unavailable for this operator");
     return DGOP_ERR_UNSUPPORTED;
   }
   if (kernel == DGOP_KERNEL_GENERIC && !op->f64.ready) {

@@ -54,6 +54,20 @@ struct KronCfg {
   Real* d_elem[4] = {};  // converted per-element factors (FP32 only)
 };
 
+template <typename Real>
+struct KronNDCfg {
+  bool ready = false;
+  const KronNDEntry<Real>* entry = nullptr;
+  KronNDParams<Real> params{};    // forward operator
+  KronNDParams<Real> params_t{};  // transposed operator
+  dim3 grid, block;
+  size_t smem = 0;
+  Real* d_mats = nullptr;
+  Real* d_phi = nullptr;
+  signed char* d_sgn = nullptr;
+  Real* d_elem[kMaxDim + 1] = {};  // converted per-element factors (FP32 only)
+};
+
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
@@ -72,6 +86,8 @@ struct dgop_operator {
   dgop::LaunchCfg<float> f32;
   dgop::KronCfg<double> k64;
   dgop::KronCfg<float> k32;
+  dgop::KronNDCfg<double> n64;
+  dgop::KronNDCfg<float> n32;
 };
 
 namespace dgop {

@@ -1,0 +1,46 @@
+// Instantiation unit of the any-dimension Kronecker kernel, compiled once per dimension with
+// -DDGOP_GEN_D=<dim>: every N = 1..8 whose element (U, W, Y, matrices) fits in shared memory.
+#include "kron_registry.h"
+#include "kronnd_kernel.cuh"
+
+#ifndef DGOP_GEN_D
+#error "DGOP_GEN_D must be defined"
+#endif
+
+#define DGOP_CAT2_(a, b) a##b
+#define DGOP_CAT2(a, b) DGOP_CAT2_(a, b)
+
+namespace dgop {
+
+namespace {
+template <int D, int N, typename Real>
+void launch_kronnd(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
+}
+
+// one element must fit in 200 KB of shared memory
+template <int D, int N, typename Real>
+constexpr bool fits() {
+  return (int64_t)KronNDShape<D, N>::PER_ELEM * (int64_t)sizeof(Real) <= 200 * 1024;
+}
+
+template <int D, int N, typename Real>
+void fill(KronNDEntry<Real>& d) {
+  if constexpr (fits<D, N, Real>()) {
+    d.launch = &launch_kronnd<D, N, Real>;
+    d.func = reinterpret_cast<const void*>(&kronnd_kernel<D, N, Real>);
+    d.per_elem = KronNDShape<D, N>::PER_ELEM;
+  }
+}
+}  // namespace
+
+void DGOP_CAT2(register_kronnd_d, DGOP_GEN_D)() {
+  constexpr int D = DGOP_GEN_D;
+  static_for<1, kMaxN + 1>([&](auto nc) {
+    constexpr int N = decltype(nc)::value;
+    fill<D, N, double>(kronnd_slot_f64(D, N));
+    fill<D, N, float>(kronnd_slot_f32(D, N));
+  });
+}
+
+}  // namespace dgop

@@ -79,14 +79,40 @@ struct KronParams {
   const int* skip;               // device word; the launch does nothing when it is non-zero
 };
 
+// Launch parameters of the any-dimension kernel (kronnd_kernel.cuh).
+template <typename Real>
+struct KronNDParams {
+  int64_t nelem;    // the launch processes elements [e_begin, nelem)
+  int64_t e_begin;
+  int64_t sizes[kMaxDim];
+  int64_t estride[kMaxDim];  // element index = sum_k c_k estride[k]
+  int periodic[kMaxDim];
+  int flags;        // OpFlags
+  int has_adv, has_mass, mass_merged;
+  int eb;           // elements per CTA
+  Real g, alpha, beta_y;
+  const Real* x;
+  Real* y;
+  const Real* mats;              // matrix tables (device)
+  KronMat slot[kMaxDim][kMaxDim];  // [a][k]: term a's matrix along k (k == a: D, or D^T when transposed)
+  KronMat mslot[kMaxDim];          // separate mass term: matrix along k
+  const Real* phi[kMaxDim];        // phi[a][e_a * 2 + s]
+  const signed char* sgn[kMaxDim][kMaxDim];
+  const Real* elem[kMaxDim];
+  const Real* elem_mass;
+  const int* skip;
+};
+
 struct KronPlanHost {
   bool ok = false;
   const char* why = "";
-  int N = 0;
+  int N = 0, dim = 0;
   std::vector<double> mats;               // all matrices, row-major N x N each
-  std::vector<double> phi[3];             // per axis, e * 2 + s
-  std::vector<signed char> sgn[3][3];
-  KronMat D[3], Dt[3], T[3][3], MD, MT[3];
+  std::vector<double> phi[kMaxDim];       // per axis, e * 2 + s
+  std::vector<signed char> sgn[kMaxDim][kMaxDim];
+  // term a: D[a] (Dt[a] transposed) along a, T[a][k] along k != a; a separate mass term: MD along
+  // the last axis, MT[k] along the others
+  KronMat D[kMaxDim], Dt[kMaxDim], T[kMaxDim][kMaxDim], MD, MT[kMaxDim];
   int has_adv = 0, has_mass = 0, mass_merged = 0;
 };
 

@@ -39,7 +39,7 @@ KronMat add_grad(std::vector<double>& mats, const KronInputs& in, int axis, cons
   m.off = (int64_t)mats.size();
   m.stride = varies ? N * N : 0;
   for (int64_t e = 0; e < count; ++e) {
-    double G[kKronMaxN][kKronMaxN];
+    double G[kMaxN][kMaxN];
     for (int j = 0; j < N; ++j)
       for (int c = 0; c < N; ++c) {
         double s = 0.0;
@@ -82,23 +82,15 @@ bool sign_table(const KronInputs& in, int axis, const double* tab, std::vector<s
 
 }  // namespace
 
-KronPlanHost plan_kron3d(const KronInputs& in) {
+// The Kronecker form for any dimension (see kron.h): eligibility of the coefficients and the
+// per-axis matrix tables.  Dimension- and size-specific limits are the callers'.
+KronPlanHost plan_kron(const KronInputs& in) {
   KronPlanHost p;
   p.N = in.N;
-  if (in.D != 3) {
-    p.why = "dimension != 3";
-    return p;
-  }
+  p.dim = in.D;
+  const int Dm = in.D;
   if (!in.gll) {
     p.why = "basis is not GLL";
-    return p;
-  }
-  if (in.N > 4) {  // the FP64 register kernel spills above N = 4
-    p.why = "order above 3 (register kernel limit)";
-    return p;
-  }
-  if ((uint64_t)in.sizes[0] * in.sizes[1] * in.sizes[2] >= (uint64_t(1) << 32)) {
-    p.why = "more than 2^32 elements";
     return p;
   }
   const bool adv = (in.flags & kAdvCell) != 0;
@@ -108,7 +100,7 @@ KronPlanHost plan_kron3d(const KronInputs& in) {
     return p;
   }
   if (adv)
-    for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < Dm; ++a)
       if (!in.beta[a].separable) {
         p.why = "velocity component is not a single separable product";
         return p;
@@ -118,23 +110,26 @@ KronPlanHost plan_kron3d(const KronInputs& in) {
     return p;
   }
   double detJ = 1.0;
-  for (int k = 0; k < 3; ++k) detJ *= in.h[k];
+  for (int k = 0; k < Dm; ++k) detJ *= in.h[k];
   p.has_adv = adv;
   p.has_mass = mass;
   auto& M = p.mats;
+  const int last = Dm - 1;
   if (adv) {
-    const SepCoef& bz = in.beta[2];
-    p.mass_merged = mass && !in.sigma.has_elem && !bz.has_elem && in.sigma.tab[0] == bz.tab[0] &&
-                    in.sigma.tab[1] == bz.tab[1];
-    for (int a = 0; a < 3; ++a) {
+    // the mass term merges into the last axis' term when its other factors equal that term's
+    const SepCoef& bl = in.beta[last];
+    bool same = mass && !in.sigma.has_elem && !bl.has_elem;
+    for (int k = 0; k < last && same; ++k) same = in.sigma.tab[k] == bl.tab[k];
+    p.mass_merged = same;
+    for (int a = 0; a < Dm; ++a) {
       const SepCoef& b = in.beta[a];
       const double invh = 1.0 / in.h[a];
       const double s_a = -b.c * detJ * invh;
-      const bool merge = p.mass_merged && a == 2;
+      const bool merge = p.mass_merged && a == last;
       const double s_m = in.sigma.c * detJ;
-      p.D[a] = add_grad(M, in, a, b.tab[a], s_a, false, in.sigma.tab[2], s_m, merge);
-      p.Dt[a] = add_grad(M, in, a, b.tab[a], s_a, true, in.sigma.tab[2], s_m, merge);
-      for (int k = 0; k < 3; ++k) {
+      p.D[a] = add_grad(M, in, a, b.tab[a], s_a, false, in.sigma.tab[last], s_m, merge);
+      p.Dt[a] = add_grad(M, in, a, b.tab[a], s_a, true, in.sigma.tab[last], s_m, merge);
+      for (int k = 0; k < Dm; ++k) {
         if (k == a) continue;
         p.T[a][k] = add_mass(M, in, k, b.tab[k], 1.0);
         if (!sign_table(in, k, b.tab[k], p.sgn[a][k])) {
@@ -154,12 +149,29 @@ KronPlanHost plan_kron3d(const KronInputs& in) {
   }
   if (mass && !p.mass_merged) {
     const double s_m = in.sigma.c * detJ;
-    p.MD = add_mass(M, in, 2, in.sigma.tab[2], s_m);
-    p.MT[0] = add_mass(M, in, 0, in.sigma.tab[0], 1.0);
-    p.MT[1] = add_mass(M, in, 1, in.sigma.tab[1], 1.0);
+    p.MD = add_mass(M, in, last, in.sigma.tab[last], s_m);
+    for (int k = 0; k < last; ++k) p.MT[k] = add_mass(M, in, k, in.sigma.tab[k], 1.0);
   }
   p.ok = true;
   return p;
+}
+
+KronPlanHost plan_kron3d(const KronInputs& in) {
+  KronPlanHost p;
+  p.N = in.N;
+  if (in.D != 3) {
+    p.why = "dimension != 3";
+    return p;
+  }
+  if (in.N > 4) {  // the FP64 register kernel spills above N = 4
+    p.why = "order above 3 (register kernel limit)";
+    return p;
+  }
+  if ((uint64_t)in.sizes[0] * in.sizes[1] * in.sizes[2] >= (uint64_t(1) << 32)) {
+    p.why = "more than 2^32 elements";
+    return p;
+  }
+  return plan_kron(in);
 }
 
 }  // namespace dgop

@@ -18,6 +18,9 @@ struct KronInputs {
   SepCoef beta[kMaxDim];
 };
 
+// Any dimension (dimension- and size-specific limits are the callers').
+KronPlanHost plan_kron(const KronInputs& in);
+// The 3D register kernel's plan: D = 3, N <= 4, fewer than 2^32 elements.
 KronPlanHost plan_kron3d(const KronInputs& in);
 
 }  // namespace dgop

@@ -8,6 +8,7 @@
 namespace dgop {
 
 constexpr int kKronThreads = 128;
+constexpr int kKronNDThreads = 256;  // threads per CTA of the any-dimension kernel
 
 // Kernel variants of one (N, precision); the autotuner picks one per operator.
 //   0: two staging stages, exchanges through the shared tile
@@ -33,5 +34,21 @@ struct KronEntry {
 KronEntry<double>& kron3d_slot_f64(int N);
 KronEntry<float>& kron3d_slot_f32(int N);
 void register_kron3d();
+
+// Kronecker form, any dimension, shared-memory kernel (kronnd_kernel.cuh).
+template <typename Real>
+struct KronNDEntry {
+  void (*launch)(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func = nullptr;
+  int per_elem = 0;  // Real values of shared memory per element
+};
+KronNDEntry<double>& kronnd_slot_f64(int D, int N);
+KronNDEntry<float>& kronnd_slot_f32(int D, int N);
+void register_kronnd_d1();
+void register_kronnd_d2();
+void register_kronnd_d3();
+void register_kronnd_d4();
+void register_kronnd_d5();
+void register_kronnd_d6();
 
 }  // namespace dgop

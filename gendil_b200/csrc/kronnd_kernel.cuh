@@ -1,0 +1,303 @@
+// Kronecker-form DG operator kernel for any dimension D and order (N = p + 1), shared memory.
+//
+// The operator is the sum of D terms (plus a separate mass term when it does not merge), each a
+// tensor product of per-axis N x N matrices (kron.h):
+//
+//   y_e = sum_a  (x)_{k != a} T_ak  [ D_a u_e + faces_a ]
+//
+// A CTA holds EB elements in shared memory: the input U, one work array W and the accumulator Y.
+// Every factor is one pass over the element's N^(D-1) lines along its axis, one line per thread,
+// read into registers and written back in place (lines are disjoint, so W needs no second
+// buffer); the last tangential pass of a term accumulates into Y.  The face terms of axis a are
+// added to the faces' slices of D_a U before the tangential passes (GLL: the trace is the slice),
+// with the upwind neighbour's trace read from global memory.  Matrices (constant or depending on
+// the element's coordinate along their axis) are copied per element into shared memory.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dgop_params.h"
+#include "generic_kernel.cuh"
+#include "kron.h"
+
+namespace dgop {
+
+
+__host__ __device__ constexpr int kpow(int b, int e) { return e == 0 ? 1 : b * kpow(b, e - 1); }
+
+template <int D, int N>
+struct KronNDShape {
+  static constexpr int ND = kpow(N, D);  // DoFs per element
+  static constexpr int NL = ND / N;      // lines per pass
+  static constexpr int NS = D * D + D;   // matrix slots: D terms x D axes, plus the mass term
+  static constexpr int MAT = N * N;
+  // per element: U, W, Y, the slot matrices, and 2D face records (corner, neighbour / inflow
+  // coefficient) + flags
+  static constexpr int REC = 4 * D + 2;
+  static constexpr int PER_ELEM = 3 * ND + NS * MAT + REC;
+};
+
+// One pass along axis A over a batch of ne elements: X <- M X (in place) or Y += M X.
+template <int D, int N, int A, bool ACC, typename Real>
+__device__ __forceinline__ void nd_pass(Real* base, int ne, int slot, bool scale_elem, const Real* escale) {
+  using S = KronNDShape<D, N>;
+  constexpr int INNER = kpow(N, A);
+  const int total = ne * S::NL;
+  for (int l = threadIdx.x; l < total; l += blockDim.x) {
+    const int b = l / S::NL;
+    const int r = l - b * S::NL;
+    const int o = r / INNER;
+    const int t = r - o * INNER;
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    const Real* W = el + S::ND;
+    Real* out = ACC ? el + 2 * S::ND : el + S::ND;
+    const Real* m = el + 3 * S::ND + slot * S::MAT;
+    const int off = o * N * INNER + t;
+    Real v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = W[off + i * INNER];
+    const Real f = scale_elem ? escale[b] : Real(1);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      Real s = m[j * N] * v[0];
+#pragma unroll
+      for (int i = 1; i < N; ++i) s += m[j * N + i] * v[i];
+      if (ACC) out[off + j * INNER] += s;
+      else out[off + j * INNER] = scale_elem ? s * f : s;
+    }
+  }
+}
+
+// The D-matrix pass of term a: W <- M U along axis A.
+template <int D, int N, int A, typename Real>
+__device__ __forceinline__ void nd_first_pass(Real* base, int ne, int slot, const Real* escale) {
+  using S = KronNDShape<D, N>;
+  constexpr int INNER = kpow(N, A);
+  const int total = ne * S::NL;
+  for (int l = threadIdx.x; l < total; l += blockDim.x) {
+    const int b = l / S::NL;
+    const int r = l - b * S::NL;
+    const int o = r / INNER;
+    const int t = r - o * INNER;
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    const Real* U = el;
+    Real* W = el + S::ND;
+    const Real* m = el + 3 * S::ND + slot * S::MAT;
+    const int off = o * N * INNER + t;
+    Real v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = U[off + i * INNER];
+    const Real f = escale ? escale[b] : Real(1);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      Real s = m[j * N] * v[0];
+#pragma unroll
+      for (int i = 1; i < N; ++i) s += m[j * N + i] * v[i];
+      W[off + j * INNER] = escale ? s * f : s;
+    }
+  }
+}
+
+// Face records of element e (one thread per element): for face f = a * 2 + s, rec[2 f] is the
+// own-trace (corner) coefficient, rec[2 f + 1] the neighbour / inflow coefficient, and bits of
+// the flag word (5 per face): 1 corner, 2 neighbour trace, 4 inflow value.  Follows the upwind
+// rule of advectionoperator.hpp:379-386 / 422-428 per element, as the 3D kernel does.
+template <int D, typename Real>
+__device__ __forceinline__ void nd_face_records(const KronNDParams<Real>& P, int64_t e, const int64_t (&c)[kMaxDim],
+                                                Real* rec, uint32_t* flags_out) {
+  uint32_t flags = 0;
+  const bool transpose = (P.flags & kTranspose) != 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    Real tsign = Real(1);
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (k != a) tsign *= (Real)P.sgn[a][k][c[k]];
+    const Real el = P.elem[a] ? P.elem[a][e] : Real(1);
+    const int64_t n = P.sizes[a];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const bool interior = s == 0 ? (c[a] > 0 || P.periodic[a]) : (c[a] + 1 < n || P.periodic[a]);
+      const bool active = interior ? (P.flags & kFaceInt) : (P.flags & kFaceBnd);
+      const Real phi = P.phi[a][c[a] * 2 + s];
+      Real coef = Real(0);
+      uint32_t bits = 0;
+      if (active) {
+        if (phi * tsign * el > Real(0)) bits |= 1u;
+        if (!transpose) {
+          if (!(phi * tsign * el > Real(0))) {
+            coef = phi * el;
+            bits |= interior ? 2u : 4u;
+          }
+        } else if (interior) {
+          // transposed coupling: the neighbour's row, taken when its face 1 - s is inflow for it
+          const int64_t cn = s ? (c[a] + 1 == n ? 0 : c[a] + 1) : (c[a] == 0 ? n - 1 : c[a] - 1);
+          const int64_t en = e + (cn - c[a]) * P.estride[a];
+          const Real phin = P.phi[a][cn * 2 + (1 - s)];
+          const Real eln = P.elem[a] ? P.elem[a][en] : Real(1);
+          if (!(phin * tsign * eln > Real(0))) {
+            coef = phin * eln;
+            bits |= 2u;
+          }
+        }
+      }
+      rec[2 * (a * 2 + s)] = phi * el;
+      rec[2 * (a * 2 + s) + 1] = coef;
+      flags |= bits << (5 * (a * 2 + s));
+    }
+  }
+  *flags_out = flags;
+}
+
+// Face terms of axis A added to W (= D_A U) on the two slices of that axis.
+template <int D, int N, int A, typename Real>
+__device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base, int ne, int64_t e0,
+                                         const int (*ecoord)[kMaxDim]) {
+  using S = KronNDShape<D, N>;
+  constexpr int INNER = kpow(N, A);
+  const int total = ne * 2 * S::NL;  // slice points of both sides
+  for (int l = threadIdx.x; l < total; l += blockDim.x) {
+    const int b = l / (2 * S::NL);
+    const int r = l - b * 2 * S::NL;
+    const int s = r / S::NL;
+    const int p = r - s * S::NL;  // point of the slice: (o, t) with the axis index removed
+    const int o = p / INNER, t = p - o * INNER;
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+    const uint32_t f = (reinterpret_cast<const uint32_t*>(rec + 4 * D)[0] >> (5 * (A * 2 + s))) & 31u;
+    if (!f) continue;
+    const int sl = s ? N - 1 : 0;
+    const int idx = o * N * INNER + sl * INNER + t;
+    Real add = Real(0);
+    if (f & 1u) add += rec[2 * (A * 2 + s)] * el[idx];  // own trace
+    if (f & 2u) {
+      // the neighbour's opposite slice at the same tangential point
+      const int64_t e = e0 + b;
+      const int64_t n = P.sizes[A];
+      const int64_t ca = ecoord[b][A];
+      const int64_t cn = s ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
+      const int64_t en = e + (cn - ca) * P.estride[A];
+      const int nidx = o * N * INNER + (N - 1 - sl) * INNER + t;
+      add += rec[2 * (A * 2 + s) + 1] * P.x[en * S::ND + nidx];
+    } else if (f & 4u) {
+      add += rec[2 * (A * 2 + s) + 1] * P.g;
+    }
+    el[S::ND + idx] += add;
+  }
+}
+
+template <int D, int N, typename Real>
+__global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_constant__ KronNDParams<Real> P) {
+  using S = KronNDShape<D, N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* base = reinterpret_cast<Real*>(smem_raw);
+  __shared__ Real escale[64];          // per-element factor of the pass being run (EB <= 64)
+  __shared__ int ecoord[64][kMaxDim];  // element coordinates
+  if (P.skip && *P.skip) return;
+  const int EB = P.eb;
+  const bool adv = P.has_adv != 0;
+  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    __syncthreads();
+    // input, accumulator
+    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+      const int b = l / S::ND, i = l - b * S::ND;
+      Real* el = base + (size_t)b * S::PER_ELEM;
+      el[i] = P.x[e0 * S::ND + l];
+      el[2 * S::ND + i] = Real(0);
+    }
+    if (threadIdx.x < ne) {
+      const int64_t e = e0 + threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < D; ++k) ecoord[threadIdx.x][k] = (int)((e / P.estride[k]) % P.sizes[k]);
+    }
+    __syncthreads();
+    // per element: slot matrices and face records
+    for (int l = threadIdx.x; l < ne * S::NS * S::MAT; l += blockDim.x) {
+      const int b = l / (S::NS * S::MAT);
+      const int r = l - b * (S::NS * S::MAT);
+      const int sl = r / S::MAT, q = r - sl * S::MAT;
+      const int a = sl / D, k = sl - a * D;  // a == D: the mass term
+      const KronMat m = a < D ? P.slot[a][k] : P.mslot[k];
+      Real v = Real(0);
+      if (m.off >= 0) v = P.mats[m.off + (int64_t)ecoord[b][k] * m.stride + q];
+      base[(size_t)b * S::PER_ELEM + 3 * S::ND + r] = v;
+    }
+    if (adv && threadIdx.x < ne) {
+      const int b = threadIdx.x;
+      const int64_t e = e0 + b;
+      int64_t c[kMaxDim];
+#pragma unroll
+      for (int k = 0; k < D; ++k) c[k] = ecoord[b][k];
+      Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
+      uint32_t fl;
+      nd_face_records<D>(P, e, c, rec, &fl);
+      reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl;
+    }
+    __syncthreads();
+    if (adv) {
+      static_for<0, D>([&](auto ac) {
+        constexpr int a = decltype(ac)::value;
+        if (P.elem[a]) {
+          if (threadIdx.x < ne) escale[threadIdx.x] = P.elem[a][e0 + threadIdx.x];
+          __syncthreads();
+        }
+        nd_first_pass<D, N, a>(base, ne, a * D + a, P.elem[a] ? escale : (const Real*)nullptr);
+        __syncthreads();
+        nd_faces<D, N, a>(P, base, ne, e0, ecoord);
+        __syncthreads();
+        // tangential passes in increasing axis order; the last accumulates into Y
+        static_for<0, D>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          if constexpr (k != a) {
+            constexpr int lastk = (a == D - 1) ? D - 2 : D - 1;
+            nd_pass<D, N, k, k == lastk>(base, ne, a * D + k, false, escale);
+            __syncthreads();
+          }
+        });
+        if constexpr (D == 1) {
+          // no tangential pass: the term goes straight to Y
+          for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+            const int b = l / S::ND, i = l - b * S::ND;
+            Real* el = base + (size_t)b * S::PER_ELEM;
+            el[2 * S::ND + i] += el[S::ND + i];
+          }
+          __syncthreads();
+        }
+      });
+    }
+    if (P.has_mass && !(adv && P.mass_merged)) {
+      // separate mass term: along the last axis (scaled), then the others
+      if (P.elem_mass) {
+        if (threadIdx.x < ne) escale[threadIdx.x] = P.elem_mass[e0 + threadIdx.x];
+        __syncthreads();
+      }
+      nd_first_pass<D, N, D - 1>(base, ne, D * D + D - 1, P.elem_mass ? escale : (const Real*)nullptr);
+      __syncthreads();
+      static_for<0, D - 1>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        nd_pass<D, N, k, k == D - 2>(base, ne, D * D + k, false, escale);
+        __syncthreads();
+      });
+      if constexpr (D == 1) {
+        for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+          const int b = l / S::ND, i = l - b * S::ND;
+          Real* el = base + (size_t)b * S::PER_ELEM;
+          el[2 * S::ND + i] += el[S::ND + i];
+        }
+        __syncthreads();
+      }
+    }
+    // y = alpha Y + beta_y y
+    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+      const int b = l / S::ND, i = l - b * S::ND;
+      const Real v = base[(size_t)b * S::PER_ELEM + 2 * S::ND + i];
+      Real* dst = P.y + e0 * S::ND + l;
+      *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
+    }
+  }
+}
+
+}  // namespace dgop

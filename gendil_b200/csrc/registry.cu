@@ -12,10 +12,14 @@ GenericEntry<float> g_f32[kMaxDim][kMaxN][kMaxQ];
 std::once_flag g_once;
 KronEntry<double> g_k64[kKronMaxN + 1];
 KronEntry<float> g_k32[kKronMaxN + 1];
+KronNDEntry<double> g_n64[kMaxDim][kMaxN];
+KronNDEntry<float> g_n32[kMaxDim][kMaxN];
 }  // namespace
 
 KronEntry<double>& kron3d_slot_f64(int N) { return g_k64[N]; }
 KronEntry<float>& kron3d_slot_f32(int N) { return g_k32[N]; }
+KronNDEntry<double>& kronnd_slot_f64(int D, int N) { return g_n64[D - 1][N - 1]; }
+KronNDEntry<float>& kronnd_slot_f32(int D, int N) { return g_n32[D - 1][N - 1]; }
 
 GenericEntry<double>& generic_slot_f64(int D, int N, int Q) { return g_f64[D - 1][N - 1][Q - 1]; }
 GenericEntry<float>& generic_slot_f32(int D, int N, int Q) { return g_f32[D - 1][N - 1][Q - 1]; }
@@ -36,6 +40,12 @@ void ensure_registry() {
   DGOP_CALL_N(D, 5) DGOP_CALL_N(D, 6) DGOP_CALL_N(D, 7) DGOP_CALL_N(D, 8)
     DGOP_CALL_D(1) DGOP_CALL_D(2) DGOP_CALL_D(3) DGOP_CALL_D(4) DGOP_CALL_D(5) DGOP_CALL_D(6)
     register_kron3d();
+    register_kronnd_d1();
+    register_kronnd_d2();
+    register_kronnd_d3();
+    register_kronnd_d4();
+    register_kronnd_d5();
+    register_kronnd_d6();
 #undef DGOP_CALL_D
 #undef DGOP_CALL_N
   });

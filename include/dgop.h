@@ -81,9 +81,12 @@ int64_t dgop_operator_num_dofs(const dgop_operator* op);
 /* Kernel family used by an operator (no reference counterpart; diagnostics and testing):
  * DGOP_KERNEL_GENERIC is the sum-factorized kernel that follows the reference's element
  * algorithm for every shape; DGOP_KERNEL_KRON is the register-resident Kronecker-form kernel
- * (3D, GLL, orders 0..3, separable coefficients), chosen automatically when eligible.
+ * (3D, GLL, orders 0..3, separable coefficients), chosen automatically when eligible;
+ * DGOP_KERNEL_KRONND is the shared-memory Kronecker-form kernel for any dimension and order
+ * (GLL, separable coefficients, element within shared memory), chosen when the register kernel
+ * does not apply.
  * dgop_operator_kernel_note() says why the Kronecker form was not chosen. */
-enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1 };
+enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1, DGOP_KERNEL_KRONND = 2 };
 int dgop_operator_kernel(const dgop_operator* op);
 const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);

@@ -1,7 +1,8 @@
 """GPU: the sm_100a operators against the reference's golden outputs and the oracle.
 
 FP64 applies must match to APPLY_TOL = 1e-13 relative in max norm per apply.  Every case runs on
-the generic sum-factorized kernel and, where eligible, on the Kronecker-form kernel."""
+the generic sum-factorized kernel and, where eligible, on the Kronecker-form kernels (the 3D
+register kernel and the any-dimension shared-memory kernel)."""
 import numpy as np
 import pytest
 
@@ -9,12 +10,18 @@ from helpers import APPLY_TOL, cuda_apply, golden, inputs, make_operator, oracle
 
 pytestmark = pytest.mark.gpu
 CASES, ARR = golden()
-KERNELS = ["generic", "kron"]
+KERNELS = ["generic", "kron", "kronnd"]
 
 
 def _select(op, kernel):
     if kernel == "kron" and op.kernel != "kron":
         pytest.skip(f"not eligible for the Kronecker kernel: {op.kernel_note}")
+    if kernel == "kronnd" and op.kernel != "kronnd":
+        import gendil_b200 as g
+        try:
+            op.select_kernel("kronnd")
+        except g.DGOPError as exc:
+            pytest.skip(f"not eligible for the any-dimension Kronecker kernel: {exc}")
     if kernel == "generic" and op.kernel != "generic":
         import gendil_b200 as g
         try:
@@ -54,6 +61,27 @@ def test_transpose_adjoint_identity(case, mode, kernel):
     atz = cuda_apply(op, z, transpose=True)
     lhs, rhs = float(ax @ z), float(x @ atz)
     assert abs(lhs - rhs) <= 1e-12 * (np.abs(ax).sum() * np.abs(z).max() + 1e-300)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("case", CASES["advection"], ids=lambda c: c["id"])
+def test_transpose_kronnd_agrees_with_generic(case, mode):
+    """The any-dimension Kronecker kernel and the generic kernel give the same A^T x."""
+    import gendil_b200 as g
+    case = dict(case, g=0.0)
+    op = make_operator(case, "adv", mode)
+    try:
+        op.select_kernel("kronnd")
+    except g.DGOPError:
+        pytest.skip("not eligible for the any-dimension Kronecker kernel")
+    x = inputs(case, seed=7)
+    yk = cuda_apply(op, x, transpose=True)
+    try:
+        op.select_kernel("generic")
+    except g.DGOPError:
+        pytest.skip("generic kernel not built for this shape")
+    yg = cuda_apply(op, x, transpose=True)
+    assert rel_max(yk, yg) <= APPLY_TOL
 
 
 @pytest.mark.parametrize("mode", [0, 1, 2])
