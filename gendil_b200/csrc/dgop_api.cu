@@ -539,6 +539,9 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
   while (eb > 1 && (int64_t)(eb / 2) * lines >= 4 * kKronNDThreads) eb /= 2;  // enough work, more CTAs
   int max_smem = 0;
   DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+  cudaFuncAttributes fa{};
+  DGOP_CUDA(cudaFuncGetAttributes(&fa, entry->func));
+  max_smem -= (int)fa.sharedSizeBytes;  // the kernel's static shared memory counts against the limit
   while (eb > 1 && per * eb > (size_t)max_smem) --eb;
   if (per * eb > (size_t)max_smem) {
     set_error("element does not fit in shared memory");
