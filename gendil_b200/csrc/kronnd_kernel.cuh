@@ -151,40 +151,43 @@ __device__ __forceinline__ void nd_face_records(const KronNDParams<Real>& P, int
   *flags_out = flags;
 }
 
-// Face terms of axis A added to W (= D_A U) on the two slices of that axis.
+// Face terms of axis A added to W (= D_A U) on the two slices of that axis.  One thread takes a
+// tangential point and both sides (for N = 1 the two slices are the same point).
 template <int D, int N, int A, typename Real>
 __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base, int ne, int64_t e0,
                                          const int (*ecoord)[kMaxDim]) {
   using S = KronNDShape<D, N>;
   constexpr int INNER = kpow(N, A);
-  const int total = ne * 2 * S::NL;  // slice points of both sides
+  const int total = ne * S::NL;
   for (int l = threadIdx.x; l < total; l += blockDim.x) {
-    const int b = l / (2 * S::NL);
-    const int r = l - b * 2 * S::NL;
-    const int s = r / S::NL;
-    const int p = r - s * S::NL;  // point of the slice: (o, t) with the axis index removed
+    const int b = l / S::NL;
+    const int p = l - b * S::NL;  // point of the slice: (o, t) with the axis index removed
     const int o = p / INNER, t = p - o * INNER;
     Real* el = base + (size_t)b * S::PER_ELEM;
     const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
-    const uint32_t f = (reinterpret_cast<const uint32_t*>(rec + 4 * D)[0] >> (5 * (A * 2 + s))) & 31u;
-    if (!f) continue;
-    const int sl = s ? N - 1 : 0;
-    const int idx = o * N * INNER + sl * INNER + t;
-    Real add = Real(0);
-    if (f & 1u) add += rec[2 * (A * 2 + s)] * el[idx];  // own trace
-    if (f & 2u) {
-      // the neighbour's opposite slice at the same tangential point
-      const int64_t e = e0 + b;
-      const int64_t n = P.sizes[A];
-      const int64_t ca = ecoord[b][A];
-      const int64_t cn = s ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
-      const int64_t en = e + (cn - ca) * P.estride[A];
-      const int nidx = o * N * INNER + (N - 1 - sl) * INNER + t;
-      add += rec[2 * (A * 2 + s) + 1] * P.x[en * S::ND + nidx];
-    } else if (f & 4u) {
-      add += rec[2 * (A * 2 + s) + 1] * P.g;
+    const uint32_t fw = reinterpret_cast<const uint32_t*>(rec + 4 * D)[0];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const uint32_t f = (fw >> (5 * (A * 2 + s))) & 31u;
+      if (!f) continue;
+      const int sl = s ? N - 1 : 0;
+      const int idx = o * N * INNER + sl * INNER + t;
+      Real add = Real(0);
+      if (f & 1u) add += rec[2 * (A * 2 + s)] * el[idx];  // own trace
+      if (f & 2u) {
+        // the neighbour's opposite slice at the same tangential point
+        const int64_t e = e0 + b;
+        const int64_t n = P.sizes[A];
+        const int64_t ca = ecoord[b][A];
+        const int64_t cn = s ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
+        const int64_t en = e + (cn - ca) * P.estride[A];
+        const int nidx = o * N * INNER + (N - 1 - sl) * INNER + t;
+        add += rec[2 * (A * 2 + s) + 1] * P.x[en * S::ND + nidx];
+      } else if (f & 4u) {
+        add += rec[2 * (A * 2 + s) + 1] * P.g;
+      }
+      el[S::ND + idx] += add;
     }
-    el[S::ND + idx] += add;
   }
 }
 
