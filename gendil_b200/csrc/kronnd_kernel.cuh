@@ -107,7 +107,8 @@ __device__ __forceinline__ void nd_first_pass(Real* base, int ne, int slot, cons
 template <int D, typename Real>
 __device__ __forceinline__ void nd_face_records(const KronNDParams<Real>& P, int64_t e, const int64_t (&c)[kMaxDim],
                                                 Real* rec, uint32_t* flags_out) {
-  uint32_t flags = 0;
+  // 5 bits per face, six faces per 32-bit word: faces 0..5 in word 0, 6..11 in word 1
+  uint32_t flags[2] = {0u, 0u};
   const bool transpose = (P.flags & kTranspose) != 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
@@ -145,10 +146,12 @@ __device__ __forceinline__ void nd_face_records(const KronNDParams<Real>& P, int
       }
       rec[2 * (a * 2 + s)] = phi * el;
       rec[2 * (a * 2 + s) + 1] = coef;
-      flags |= bits << (5 * (a * 2 + s));
+      const int fi = a * 2 + s;
+      flags[fi / 6] |= bits << (5 * (fi % 6));
     }
   }
-  *flags_out = flags;
+  flags_out[0] = flags[0];
+  flags_out[1] = flags[1];
 }
 
 // Face terms of axis A added to W (= D_A U) on the two slices of that axis.  One thread takes a
@@ -165,10 +168,11 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
     const int o = p / INNER, t = p - o * INNER;
     Real* el = base + (size_t)b * S::PER_ELEM;
     const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
-    const uint32_t fw = reinterpret_cast<const uint32_t*>(rec + 4 * D)[0];
+    const uint32_t* fw = reinterpret_cast<const uint32_t*>(rec + 4 * D);
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      const uint32_t f = (fw >> (5 * (A * 2 + s))) & 31u;
+      const int fi = A * 2 + s;
+      const uint32_t f = (fw[fi / 6] >> (5 * (fi % 6))) & 31u;
       if (!f) continue;
       const int sl = s ? N - 1 : 0;
       const int idx = o * N * INNER + sl * INNER + t;
@@ -235,9 +239,10 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
 #pragma unroll
       for (int k = 0; k < D; ++k) c[k] = ecoord[b][k];
       Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
-      uint32_t fl;
-      nd_face_records<D>(P, e, c, rec, &fl);
-      reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl;
+      uint32_t fl[2];
+      nd_face_records<D>(P, e, c, rec, fl);
+      reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl[0];
+      reinterpret_cast<uint32_t*>(rec + 4 * D)[1] = fl[1];
     }
     __syncthreads();
     if (adv) {
