@@ -532,17 +532,19 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
   for (int a = 0; a < D; ++a)
     if ((rc = elem_ptr(plan.has_adv ? elem_beta[a] : nullptr, a, &p.elem[a]))) return rc;
   if ((rc = elem_ptr(plan.has_mass ? elem_sigma : nullptr, kMaxDim, &p.elem_mass))) return rc;
-  // elements per CTA: as many as fit in ~96 KB (at most 64), one at least
+  // elements per CTA: a power of two (the CTA's threads split into equal groups, one per element)
+  // as large as fits in ~96 KB, at most 64, and no larger than needed to give every thread a line
   const size_t per = (size_t)entry->per_elem * sizeof(Real);
-  int eb = (int)std::max<size_t>(1, std::min<size_t>(64, (96 * 1024) / per));
+  int eb = 1;
+  while (eb < 64 && per * (eb * 2) <= 96 * 1024) eb *= 2;
   const int64_t lines = (int64_t)(s.ndofs / s.nelem) / N;
-  while (eb > 1 && (int64_t)(eb / 2) * lines >= 4 * kKronNDThreads) eb /= 2;  // enough work, more CTAs
+  while (eb > 1 && (int64_t)(eb / 2) * lines >= kKronNDThreads) eb /= 2;
   int max_smem = 0;
   DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
   cudaFuncAttributes fa{};
   DGOP_CUDA(cudaFuncGetAttributes(&fa, entry->func));
   max_smem -= (int)fa.sharedSizeBytes;  // the kernel's static shared memory counts against the limit
-  while (eb > 1 && per * eb > (size_t)max_smem) --eb;
+  while (eb > 1 && per * eb > (size_t)max_smem) eb /= 2;
   if (per * eb > (size_t)max_smem) {
     set_error("element does not fit in shared memory");
     return DGOP_ERR_UNSUPPORTED;

@@ -39,63 +39,56 @@ struct KronNDShape {
   static constexpr int PER_ELEM = 3 * ND + NS * MAT + REC;
 };
 
-// One pass along axis A over a batch of ne elements: X <- M X (in place) or Y += M X.
-template <int D, int N, int A, bool ACC, typename Real>
-__device__ __forceinline__ void nd_pass(Real* base, int ne, int slot, bool scale_elem, const Real* escale) {
-  using S = KronNDShape<D, N>;
-  constexpr int INNER = kpow(N, A);
-  const int total = ne * S::NL;
-  for (int l = threadIdx.x; l < total; l += blockDim.x) {
-    const int b = l / S::NL;
-    const int r = l - b * S::NL;
-    const int o = r / INNER;
-    const int t = r - o * INNER;
-    Real* el = base + (size_t)b * S::PER_ELEM;
-    const Real* W = el + S::ND;
-    Real* out = ACC ? el + 2 * S::ND : el + S::ND;
-    const Real* m = el + 3 * S::ND + slot * S::MAT;
-    const int off = o * N * INNER + t;
-    Real v[N];
+// Matrix of a pass: in registers for N <= 4 (loaded once per pass), read from shared memory
+// otherwise.
+template <int N, typename Real, bool REG = (N <= 4)>
+struct PassMat;
+template <int N, typename Real>
+struct PassMat<N, Real, true> {
+  Real a[N * N];
+  __device__ __forceinline__ explicit PassMat(const Real* m) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) v[i] = W[off + i * INNER];
-    const Real f = scale_elem ? escale[b] : Real(1);
-#pragma unroll
-    for (int j = 0; j < N; ++j) {
-      Real s = m[j * N] * v[0];
-#pragma unroll
-      for (int i = 1; i < N; ++i) s += m[j * N + i] * v[i];
-      if (ACC) out[off + j * INNER] += s;
-      else out[off + j * INNER] = scale_elem ? s * f : s;
-    }
+    for (int i = 0; i < N * N; ++i) a[i] = m[i];
   }
-}
+  __device__ __forceinline__ Real operator()(int j, int i) const { return a[j * N + i]; }
+};
+template <int N, typename Real>
+struct PassMat<N, Real, false> {
+  const Real* m;
+  __device__ __forceinline__ explicit PassMat(const Real* p) : m(p) {}
+  __device__ __forceinline__ Real operator()(int j, int i) const { return m[j * N + i]; }
+};
 
-// The D-matrix pass of term a: W <- M U along axis A.
-template <int D, int N, int A, typename Real>
-__device__ __forceinline__ void nd_first_pass(Real* base, int ne, int slot, const Real* escale) {
+// One pass along axis A over the batch: the CTA's threads form EB groups of blockDim / EB, group
+// b runs the lines of element b with the element's matrix held in registers.
+//   FIRST: W <- M U (times the element factor when escale is given)
+//   ACC:   Y += M W            otherwise: W <- M W in place
+template <int D, int N, int A, bool FIRST, bool ACC, typename Real>
+__device__ __forceinline__ void nd_pass(Real* base, int ne, int eb, int slot, const Real* escale) {
   using S = KronNDShape<D, N>;
   constexpr int INNER = kpow(N, A);
-  const int total = ne * S::NL;
-  for (int l = threadIdx.x; l < total; l += blockDim.x) {
-    const int b = l / S::NL;
-    const int r = l - b * S::NL;
+  const int tpe = blockDim.x / eb;
+  const int b = threadIdx.x / tpe;
+  if (b >= ne) return;
+  Real* el = base + (size_t)b * S::PER_ELEM;
+  const Real* in = FIRST ? el : el + S::ND;
+  Real* out = ACC ? el + 2 * S::ND : el + S::ND;
+  const PassMat<N, Real> m(el + 3 * S::ND + slot * S::MAT);
+  const Real f = (FIRST && escale) ? escale[b] : Real(1);
+  for (int r = threadIdx.x - b * tpe; r < S::NL; r += tpe) {
     const int o = r / INNER;
     const int t = r - o * INNER;
-    Real* el = base + (size_t)b * S::PER_ELEM;
-    const Real* U = el;
-    Real* W = el + S::ND;
-    const Real* m = el + 3 * S::ND + slot * S::MAT;
     const int off = o * N * INNER + t;
     Real v[N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) v[i] = U[off + i * INNER];
-    const Real f = escale ? escale[b] : Real(1);
+    for (int i = 0; i < N; ++i) v[i] = in[off + i * INNER];
 #pragma unroll
     for (int j = 0; j < N; ++j) {
-      Real s = m[j * N] * v[0];
+      Real s = m(j, 0) * v[0];
 #pragma unroll
-      for (int i = 1; i < N; ++i) s += m[j * N + i] * v[i];
-      W[off + j * INNER] = escale ? s * f : s;
+      for (int i = 1; i < N; ++i) s += m(j, i) * v[i];
+      if (ACC) out[off + j * INNER] += s;
+      else out[off + j * INNER] = (FIRST && escale) ? s * f : s;
     }
   }
 }
@@ -252,7 +245,7 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
           if (threadIdx.x < ne) escale[threadIdx.x] = P.elem[a][e0 + threadIdx.x];
           __syncthreads();
         }
-        nd_first_pass<D, N, a>(base, ne, a * D + a, P.elem[a] ? escale : (const Real*)nullptr);
+        nd_pass<D, N, a, true, false>(base, ne, EB, a * D + a, P.elem[a] ? escale : (const Real*)nullptr);
         __syncthreads();
         nd_faces<D, N, a>(P, base, ne, e0, ecoord);
         __syncthreads();
@@ -261,7 +254,7 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
           constexpr int k = decltype(kc)::value;
           if constexpr (k != a) {
             constexpr int lastk = (a == D - 1) ? D - 2 : D - 1;
-            nd_pass<D, N, k, k == lastk>(base, ne, a * D + k, false, escale);
+            nd_pass<D, N, k, false, k == lastk>(base, ne, EB, a * D + k, (const Real*)nullptr);
             __syncthreads();
           }
         });
@@ -282,11 +275,11 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
         if (threadIdx.x < ne) escale[threadIdx.x] = P.elem_mass[e0 + threadIdx.x];
         __syncthreads();
       }
-      nd_first_pass<D, N, D - 1>(base, ne, D * D + D - 1, P.elem_mass ? escale : (const Real*)nullptr);
+      nd_pass<D, N, D - 1, true, false>(base, ne, EB, D * D + D - 1, P.elem_mass ? escale : (const Real*)nullptr);
       __syncthreads();
       static_for<0, D - 1>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        nd_pass<D, N, k, k == D - 2>(base, ne, D * D + k, false, escale);
+        nd_pass<D, N, k, false, k == D - 2>(base, ne, EB, D * D + k, (const Real*)nullptr);
         __syncthreads();
       });
       if constexpr (D == 1) {
