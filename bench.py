@@ -33,6 +33,8 @@ sys.path.insert(0, ROOT)
 N_AXIS, ORDER, NQ = 64, 3, 4
 METRIC = "GDoF/s per operator apply vs HBM roofline; mixed vs FP64 solve time @1e-10"
 WORKLOAD = "fp64 upwind DG advection apply, 3D 64^3 hex, p=3 GLL, q=4 GL, sin/cos velocity, inflow 0"
+WORKLOAD_6D = ("fp64 upwind DG advection apply, 6D phase space 8^6 hypercubes on [0,1]^3 x [-1,1]^3, p=2 GLL, "
+               "q=3 GL, beta = (v, -x + 0.5), inflow 0")
 FALLBACK_HBM_GBS = 6650.0
 HOST_SLABS = 16  # pipeline depth of the host-vector apply (slabs of z planes)
 # DRAM bytes (read + write) of one launch measured by ncu on the 64^3 workload, by kernel family
@@ -185,18 +187,19 @@ def run_reference(args):
     return 0
 
 
-def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10):
-    """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed 2), GMRES(restart) to tol
+def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2):
+    """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed), GMRES(restart) to tol
     relative FP64 residual from x0 = 0, timed on the device (CUDA events around the whole solve):
     FP64 GMRES with the reference's modified Gram-Schmidt, then the refinement solver with FP64
     and with FP32 inner cycles (fused classical Gram-Schmidt, FP64 residual and update).  Each leg reports the
     residual it reached, recomputed here with the FP64 operator, and the mixed leg its max-norm
     distance to the FP64 solution."""
     import torch
-    A = g.SystemOperator(space, NQ, C.velocity_sincos(3), sigma=1.0 / dt, bc=g.BC_INFLOW, g=0.0)
-    b = torch.from_numpy(g.fill_random(space.num_dofs, 2)).to(dev)
+    A = g.SystemOperator(space, q or NQ, beta or C.velocity_sincos(3), sigma=1.0 / dt, bc=g.BC_INFLOW, g=0.0)
+    b = torch.from_numpy(g.fill_random(space.num_dofs, seed)).to(dev)
     bnorm = torch.linalg.vector_norm(b).item()
-    out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, x0 = 0, b = FillRandom(seed 2)"}
+    out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, x0 = 0, b = FillRandom(seed {seed})",
+           "kernel": A.kernel}
     sols = {}
     legs = (("fp64_gmres", lambda: g.GMRESSolver(A, restart)),
             ("fp64_gmres_ir", lambda: g.GMRESIRSolver(A, restart, inner="fp64")),
@@ -244,8 +247,15 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    space = g.Space(3, [args.size] * 3, order=ORDER)
-    op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
+    six = args.workload == "6d"
+    if six:
+        # configuration 3: 8^6 elements on [0,1]^3 x [-1,1]^3, p = 2, q = 3, beta = (v, -x + 0.5)
+        n6 = 8
+        space = g.Space(6, [n6] * 6, [1.0 / n6] * 3 + [2.0 / n6] * 3, [0.0] * 3 + [-1.0] * 3, None, 2)
+        op = g.AdvectionOperator(space, 3, C.velocity_phase_space(6), bc=g.BC_INFLOW, g=0.0)
+    else:
+        space = g.Space(3, [args.size] * 3, order=ORDER)
+        op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
     if args.variant and op.kernel == "kron":
         op.set_variant(args.variant)  # a fixed kernel for profiling; the autotuner's pick otherwise
     nd = space.num_dofs
@@ -304,15 +314,16 @@ def run_ours(args):
     alg_bytes = 16.0 * nd
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
     # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu, summarized under profiles/)
-    traffic = TRAFFIC_BYTES.get((op.kernel, args.size))
+    traffic = None if six else TRAFFIC_BYTES.get((op.kernel, args.size))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)",
-                "config": {"workload": WORKLOAD, "dofs": nd, "elements": space.num_elements,
+                "config": {"workload": WORKLOAD_6D if six else WORKLOAD, "dofs": nd,
+                           "elements": space.num_elements,
                            "parallelism": f"replicas{world}" if world > 1 else "single",
-                           "l2": "inputs larger than L2 (x, y 134 MB each)"},
+                           "l2": f"inputs larger than L2 (x, y {8 * nd / 1e6:.0f} MB each)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                              "algorithmic_bytes_per_launch": alg_bytes},
@@ -321,21 +332,30 @@ def run_ours(args):
                         "path": f"dgop_host_io_apply (pinned host vectors, {HOST_SLABS} slabs)"},
                 "gpu_launches": args.steps,
                 "clocks": clocks.summary()}
-        if op.kernel == "kron":
+        if op.kernel in ("kron", "kronnd"):
+            # FP64 work: D^2 n x n passes (D terms x D axes), n FMA per DoF each, 2 flop per FMA
+            D, n = space.dim, space.order + 1
+            flop = D * D * n * 2
             peak64 = fp64_gemm_peak(torch, dev)
-            a64 = KRON_FLOP_PER_DOF * nd / (ms_step * 1e-3) / 1e12
+            a64 = flop * nd / (ms_step * 1e-3) / 1e12
             line["roofline_fp64"] = {"bound": "fp64", "achieved": a64, "peak": peak64, "unit": "TFLOP/s",
-                                     "frac": a64 / peak64, "flop_per_dof": KRON_FLOP_PER_DOF,
+                                     "frac": a64 / peak64, "flop_per_dof": flop,
                                      "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch), best of 3"}
         line["config"]["kernel"] = op.kernel
         if op.variant:
             line["config"]["kernel_variant"] = op.variant
             line["config"]["autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in op.variant_times().items() if v}
-        if args.size != N_AXIS:
+        if args.size != N_AXIS and not six:
             line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
         if world == 1 and not args.no_solve:
-            line["solve"] = solve_leg(g, C, space, dev)
-        if world == 1 and not args.no_cpu_baseline and args.size == N_AXIS:
+            if six:  # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3
+                line["solve"] = solve_leg(g, C, space, dev, dt=5e-3, restart=20, q=3,
+                                          beta=C.velocity_phase_space(6), seed=3)
+            else:
+                line["solve"] = solve_leg(g, C, space, dev)
+        if six:
+            line["cpu_baseline"] = {"unavailable": "the reference timing driver is built for the 3D workload only"}
+        if world == 1 and not args.no_cpu_baseline and args.size == N_AXIS and not six:
             try:
                 line["cpu_baseline"] = cpu_baseline(x_np)
             except Exception as exc:  # the baseline is reported, never required
@@ -356,6 +376,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=N_AXIS, help="elements per axis (profiling runs only)")
     ap.add_argument("--variant", default=None, help="force a Kronecker-kernel variant (profiling runs only)")
+    ap.add_argument("--workload", choices=["3d", "6d"], default="3d",
+                    help="3d: the 64^3 p=3 advection apply (default); 6d: the 8^6 p=2 phase-space configuration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
