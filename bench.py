@@ -187,7 +187,7 @@ def run_reference(args):
     return 0
 
 
-def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2):
+def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2, max_iters=20000):
     """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed), GMRES(restart) to tol
     relative FP64 residual from x0 = 0, timed on the device (CUDA events around the whole solve):
     FP64 GMRES with the reference's modified Gram-Schmidt, then the refinement solver with FP64
@@ -198,8 +198,8 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
     A = g.SystemOperator(space, q or NQ, beta or C.velocity_sincos(3), sigma=1.0 / dt, bc=g.BC_INFLOW, g=0.0)
     b = torch.from_numpy(g.fill_random(space.num_dofs, seed)).to(dev)
     bnorm = torch.linalg.vector_norm(b).item()
-    out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, x0 = 0, b = FillRandom(seed {seed})",
-           "kernel": A.kernel}
+    out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, at most {max_iters} iterations, x0 = 0, "
+                     f"b = FillRandom(seed {seed})", "kernel": A.kernel}
     sols = {}
     legs = (("fp64_gmres", lambda: g.GMRESSolver(A, restart)),
             ("fp64_gmres_ir", lambda: g.GMRESIRSolver(A, restart, inner="fp64")),
@@ -212,7 +212,7 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        info = solver.solve(b, x, 20000, tol)
+        info = solver.solve(b, x, max_iters, tol)
         e1.record()
         torch.cuda.synchronize()
         ax = torch.empty_like(x)
@@ -348,9 +348,13 @@ def run_ours(args):
         if args.size != N_AXIS and not six:
             line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
         if world == 1 and not args.no_solve:
-            if six:  # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3
+            if six:
+                # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3.  The unpreconditioned
+                # system's tensor-product mass matrix is ill-conditioned in 6D (GMRES(20) needs far
+                # more than 10^4 iterations to reach 1e-10), so both legs run the same bounded
+                # iteration budget and report the residual they reached.
                 line["solve"] = solve_leg(g, C, space, dev, dt=5e-3, restart=20, q=3,
-                                          beta=C.velocity_phase_space(6), seed=3)
+                                          beta=C.velocity_phase_space(6), seed=3, max_iters=200)
             else:
                 line["solve"] = solve_leg(g, C, space, dev)
         if six:
