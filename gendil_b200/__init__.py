@@ -95,6 +95,8 @@ def lib():
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
         L.dgop_solver_set_graphs.argtypes = [vp, i]
         L.dgop_solver_set_transpose.argtypes = [vp, i]
+        L.dgop_solver_set_preconditioner.argtypes = [vp, vp]
+        L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
         L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_host_io_apply.argtypes = [vp, vp, vp, vp]
@@ -290,6 +292,16 @@ class MassOperator(_Operator):
         self.handle = h
 
 
+class MassInverseOperator(_Operator):
+    """y = M_sigma^{-1} x (inverse of the block-diagonal DG mass matrix; Kronecker kernels only)."""
+
+    def __init__(self, space, q, sigma=1.0):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        check(lib().dgop_mass_inverse_create(space.handle, q, ctypes.byref(self._coef(sigma)), ctypes.byref(h)))
+        self.handle = h
+
+
 class AdvectionOperator(_Operator):
     """y = A x, upwind DG advection (AdvectionOperator, advectionoperator.hpp:1005).
 
@@ -342,6 +354,12 @@ class _Solver:
         check(lib().dgop_solver_solve(self.handle, _ptr(b), _ptr(x), int(max_iters), float(tol), ctypes.byref(res),
                                       _stream(stream)))
         return {"success": bool(res.success), "iterations": res.iterations, "relative_error": res.relative_error}
+
+    def precondition(self, prec):
+        """Right preconditioner P (an operator on the same space, e.g. MassInverseOperator), or None."""
+        check(lib().dgop_solver_set_preconditioner(self.handle, None if prec is None else prec.handle))
+        self._prec = prec  # keep it alive while the solver uses it
+        return self
 
     def transpose(self, enable=True):
         """Solve with the transposed operator A^T (adjoint solves)."""

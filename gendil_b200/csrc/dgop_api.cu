@@ -637,7 +637,9 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
   for (int k = 0; rc == DGOP_OK && k < op->sp.D; ++k)
     rc = pack_coef(op->sp, q, (flags & (kAdvCell | kFaceInt | kFaceBnd)) ? &beta[k] : nullptr, pack, bet[k]);
   std::string generic_err;
-  if (rc == DGOP_OK) {
+  if (rc == DGOP_OK && (flags & kInvMass)) {
+    generic_err = "the mass inverse needs the Kronecker form (GLL basis, separable density, no per-element factor)";
+  } else if (rc == DGOP_OK) {
     rc = setup_launch<double>(op, op->f64, t, pack, sig, bet);
     if (rc == DGOP_ERR_UNSUPPORTED) {
       // no generic instantiation for this shape: acceptable when the Kronecker kernel covers it
@@ -674,6 +676,7 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
     in.wq = t.wq;
     const dgop_coef* sg = (flags & kMass) ? (sigma ? sigma : &one) : nullptr;
     in.sigma = sep_of(sg);
+    in.inverse_mass = (flags & kInvMass) != 0;
     const bool adv = (flags & (kAdvCell | kFaceInt | kFaceBnd)) != 0;
     const double* elem_beta[kMaxDim] = {};
     for (int k = 0; k < op->sp.D; ++k) {
@@ -917,6 +920,10 @@ int dgop_space_coordinates(const dgop_space* space, int q, int axis, double* coo
 
 int dgop_mass_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out) {
   return create_operator(space, q, sigma, nullptr, kMass, 0.0, out);
+}
+
+int dgop_mass_inverse_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out) {
+  return create_operator(space, q, sigma, nullptr, kMass | kInvMass, 0.0, out);
 }
 
 int dgop_advection_create(const dgop_space* space, int q, const dgop_coef* beta, int bc, double bc_value,

@@ -18,6 +18,7 @@ enum OpFlags : int {
   kFaceBnd = 1 << 3,    // upwind flux on boundary faces, inflow value g (advectionoperator.hpp:391-438)
   kTranspose = 1 << 4,  // apply the transposed (adjoint) operator
   kLinear = 1 << 5,     // host-side launch option: inflow value taken as 0 (the linear part)
+  kInvMass = 1 << 6,    // operator is the inverse of the element mass matrices (Kronecker kernels only)
 };
 
 // A scalar coefficient c(X) = constant + sum_t prod_k T_{t,k}(X_k), optionally multiplied by a

@@ -1,6 +1,7 @@
 // Host planner for the Kronecker form (see kron.h): eligibility and per-axis matrix tables.
 #include "kron_plan.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -80,6 +81,47 @@ bool sign_table(const KronInputs& in, int axis, const double* tab, std::vector<s
   return true;
 }
 
+// In-place inverse of one N x N block (Gauss-Jordan with partial pivoting); false if singular.
+bool invert_block(double* a, int N) {
+  double inv[kMaxN * kMaxN];
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) inv[i * N + j] = i == j ? 1.0 : 0.0;
+  for (int c = 0; c < N; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < N; ++r)
+      if (std::fabs(a[r * N + c]) > std::fabs(a[piv * N + c])) piv = r;
+    if (!(std::fabs(a[piv * N + c]) > 0.0)) return false;
+    if (piv != c)
+      for (int j = 0; j < N; ++j) {
+        std::swap(a[c * N + j], a[piv * N + j]);
+        std::swap(inv[c * N + j], inv[piv * N + j]);
+      }
+    const double d = 1.0 / a[c * N + c];
+    for (int j = 0; j < N; ++j) {
+      a[c * N + j] *= d;
+      inv[c * N + j] *= d;
+    }
+    for (int r = 0; r < N; ++r) {
+      if (r == c) continue;
+      const double f = a[r * N + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < N; ++j) {
+        a[r * N + j] -= f * a[c * N + j];
+        inv[r * N + j] -= f * inv[c * N + j];
+      }
+    }
+  }
+  for (int i = 0; i < N * N; ++i) a[i] = inv[i];
+  return true;
+}
+
+// Invert every block of a matrix table in place.
+bool invert_table(std::vector<double>& mats, const KronMat& m, int64_t count, int N) {
+  for (int64_t e = 0; e < count; ++e)
+    if (!invert_block(mats.data() + m.off + e * m.stride, N)) return false;
+  return true;
+}
+
 }  // namespace
 
 // The Kronecker form for any dimension (see kron.h): eligibility of the coefficients and the
@@ -97,6 +139,10 @@ KronPlanHost plan_kron(const KronInputs& in) {
   const bool mass = (in.flags & kMass) != 0;
   if (!adv && !mass) {
     p.why = "empty operator";
+    return p;
+  }
+  if (in.inverse_mass && (adv || !mass || in.sigma.has_elem)) {
+    p.why = "the mass inverse takes a density without per-element factor and no advection";
     return p;
   }
   if (adv)
@@ -151,6 +197,15 @@ KronPlanHost plan_kron(const KronInputs& in) {
     const double s_m = in.sigma.c * detJ;
     p.MD = add_mass(M, in, last, in.sigma.tab[last], s_m);
     for (int k = 0; k < last; ++k) p.MT[k] = add_mass(M, in, k, in.sigma.tab[k], 1.0);
+    if (in.inverse_mass) {
+      // (x)_k A_k is inverted factor by factor: every block of every table
+      bool ok = invert_table(M, p.MD, p.MD.stride ? in.sizes[last] : 1, in.N);
+      for (int k = 0; k < last && ok; ++k) ok = invert_table(M, p.MT[k], p.MT[k].stride ? in.sizes[k] : 1, in.N);
+      if (!ok) {
+        p.why = "singular element mass matrix";
+        return p;
+      }
+    }
   }
   p.ok = true;
   return p;

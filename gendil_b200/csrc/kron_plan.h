@@ -16,6 +16,7 @@ struct KronInputs {
   const double* wq = nullptr;  // Q
   SepCoef sigma;
   SepCoef beta[kMaxDim];
+  bool inverse_mass = false;  // plan the inverse of the (mass-only) operator
 };
 
 // Any dimension (dimension- and size-specific limits are the callers').

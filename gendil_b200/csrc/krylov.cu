@@ -548,6 +548,13 @@ struct SolverImpl {
   const void* key_x = nullptr;
   int key_version = -1, key_flags = -1;
   int op_flags = 0;  // extra operator flags of every apply (kTranspose: solve with A^T)
+  // right preconditioner (GMRES): A P z = b, x = P z; scratch vectors z (inner precision, stride
+  // ir_stride(n) for the refinement solver) and t (FP64)
+  dgop_operator* prec = nullptr;
+  void* pz = nullptr;
+  double* pt = nullptr;
+  const dgop_operator* key_prec = nullptr;
+  int key_prec_version = -1;
   // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -595,6 +602,8 @@ void solver_free(dgop_solver* sv) {
   if (s.small) cudaFree(s.small);
   if (s.h_flag) cudaFreeHost(s.h_flag);
   if (s.wide) cudaFree(s.wide);
+  if (s.pz) cudaFree(s.pz);
+  if (s.pt) cudaFree(s.pt);
   if (s.exec) cudaGraphExecDestroy(s.exec);
   if (s.cap) cudaStreamDestroy(s.cap);
   for (auto e : s.ev)
@@ -608,7 +617,8 @@ template <typename F>
 int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&& enqueue) {
   if (!s.use_graphs) return enqueue(st);
   const bool same =
-      s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version && s.key_flags == s.op_flags;
+      s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version && s.key_flags == s.op_flags &&
+      s.key_prec == s.prec && (!s.prec || s.key_prec_version == s.prec->version);
   if (!same) {
     if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
     DGOP_CUDA_S(cudaStreamBeginCapture(s.cap, cudaStreamCaptureModeThreadLocal));
@@ -632,6 +642,8 @@ int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&
     s.key_x = x;
     s.key_version = s.op->version;
     s.key_flags = s.op_flags;
+    s.key_prec = s.prec;
+    s.key_prec_version = s.prec ? s.prec->version : -1;
   }
   DGOP_CUDA_S(cudaGraphLaunch(s.exec, st));
   return DGOP_OK;
@@ -733,7 +745,13 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
     for (int j = 0; j < m; ++j) {
       double* vj = V + (int64_t)j * n;
-      DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, s.op_flags, q, inactive));
+      if (s.prec) {
+        double* z = static_cast<double*>(s.pz);
+        DGOP_TRY(launch_f64(s.prec, 1.0, vj, 0.0, z, 0, q, inactive));
+        DGOP_TRY(launch_f64(s.op, 1.0, z, 0.0, w, s.op_flags, q, inactive));
+      } else {
+        DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, s.op_flags, q, inactive));
+      }
       k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(V), static_cast<const double*>(w), n, pa, inactive);
       double* pin = pa;
       double* pout = pb;
@@ -748,7 +766,14 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
       DGOP_CUDA_S(cudaGetLastError());
     }
     k_gm_backsub<<<1, 1, 0, q>>>(gs, H, e1, y, m);
-    k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const double*>(V), n, y, n);
+    if (s.prec) {
+      // x += P (sum_i y_i V_i)
+      DGOP_CUDA_S(cudaMemsetAsync(s.pt, 0, sizeof(double) * n, q));
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, s.pt, static_cast<const double*>(V), n, y, n);
+      DGOP_TRY(launch_f64(s.prec, 1.0, s.pt, 1.0, x, 0, q, done));
+    } else {
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const double*>(V), n, y, n);
+    }
     return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
@@ -821,7 +846,13 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
     for (int j = 0; j < m; ++j) {
       T* vj = V + (int64_t)j * ld;
       T* vn = vj + ld;
-      DGOP_TRY(apply_inner(s.op, vj, w, s.op_flags, q, inactive));
+      if (s.prec) {
+        T* z = static_cast<T*>(s.pz);
+        DGOP_TRY(apply_inner(s.prec, vj, z, 0, q, inactive));
+        DGOP_TRY(apply_inner(s.op, z, w, s.op_flags, q, inactive));
+      } else {
+        DGOP_TRY(apply_inner(s.op, vj, w, s.op_flags, q, inactive));
+      }
       const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
       k_gs_dots<T><<<dgrid, kRT, 0, q>>>(gs, V, ld, j, w, s.wide);
       k_gs_h<<<j + 1, kRT, 0, q>>>(gs, j, m, H, s.wide);
@@ -831,7 +862,13 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
       DGOP_CUDA_S(cudaGetLastError());
     }
     k_gm_backsub<<<1, 1, 0, q>>>(gs, H, e1, y, m);
-    k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const T*>(V), ld, y, n);
+    if (s.prec) {
+      DGOP_CUDA_S(cudaMemsetAsync(s.pt, 0, sizeof(double) * n, q));
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, s.pt, static_cast<const T*>(V), ld, y, n);
+      DGOP_TRY(launch_f64(s.prec, 1.0, s.pt, 1.0, x, 0, q, done));
+    } else {
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const T*>(V), ld, y, n);
+    }
     return residual(1, q);
   };
   k_dot<<<kRB, kRT, 0, st>>>(b, b, n, pa, nullptr);
@@ -974,6 +1011,35 @@ int dgop_solver_set_graphs(dgop_solver* sv, int enable) {
     return DGOP_ERR_ARG;
   }
   sv->s.use_graphs = enable != 0;
+  return DGOP_OK;
+}
+
+int dgop_solver_set_preconditioner(dgop_solver* sv, dgop_operator* prec) {
+  if (!sv) {
+    set_error("dgop_solver_set_preconditioner: null solver");
+    return DGOP_ERR_ARG;
+  }
+  SolverImpl& s = sv->s;
+  if (prec && s.kind == 0) {
+    set_error("dgop_solver_set_preconditioner: GMRES solvers only");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (prec && prec->sp.ndofs != s.n) {
+    set_error("dgop_solver_set_preconditioner: the preconditioner acts on another space");
+    return DGOP_ERR_ARG;
+  }
+  if (prec && s.kind == 2 && s.inner == DGOP_FP32 && !prec->f32.ready && !prec->k32.ready && !prec->n32.ready) {
+    set_error("dgop_solver_set_preconditioner: the preconditioner has no FP32 kernel");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (prec && !s.pz) {
+    const size_t zbytes = s.kind == 2 ? (size_t)ir_stride(s.n) * (s.inner == DGOP_FP32 ? 4 : 8) : sizeof(double) * s.n;
+    cudaError_t e = cudaMalloc(&s.pz, zbytes);
+    if (e == cudaSuccess) e = cudaMemset(s.pz, 0, zbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&s.pt, sizeof(double) * s.n);
+    if (e != cudaSuccess) return cuda_fail(e, "preconditioner workspace");
+  }
+  s.prec = prec;
   return DGOP_OK;
 }
 

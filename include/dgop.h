@@ -75,6 +75,11 @@ int dgop_mass_advection_create(const dgop_space* space, int q, const dgop_coef* 
                                dgop_operator** out);
 int dgop_system_create(const dgop_space* space, int q, const dgop_coef* sigma, const dgop_coef* beta, int bc,
                        double bc_value, dgop_operator** out);
+/* mass_inverse:    y = M_sigma^{-1} x, the inverse of the block-diagonal DG mass matrix, applied as
+ *                  the tensor product of inverted per-axis factors (no reference counterpart; the
+ *                  preconditioner of dgop_solver_set_preconditioner).  Needs the Kronecker form:
+ *                  GLL basis, a density that is one separable product, no per-element factor. */
+int dgop_mass_inverse_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out);
 int dgop_operator_destroy(dgop_operator* op);
 int64_t dgop_operator_num_dofs(const dgop_operator* op);
 
@@ -169,6 +174,13 @@ int dgop_solver_set_graphs(dgop_solver* solver, int enable);
  * value 0; dgop_apply_transpose) with the same algorithm; used by adjoint solves.  No reference
  * counterpart. */
 int dgop_solver_set_transpose(dgop_solver* solver, int transpose);
+/* Right preconditioning of a GMRES or refinement-GMRES solver: it solves A P z = b and returns
+ * x = P z, so the stopping test and `relative_error` stay those of the unpreconditioned system
+ * (|b - A x| / |b|).  P is an operator on the same space, typically dgop_mass_inverse_create's
+ * (for mass-dominated implicit systems, whose tensor-product mass matrix conditions badly in high
+ * dimension).  NULL removes it.  The workspace (two vectors) is allocated here.  No reference
+ * counterpart. */
+int dgop_solver_set_preconditioner(dgop_solver* solver, dgop_operator* prec);
 
 /* Per-element inner products: out[e] = scale[e] * sum over the DoFs i of element e of a_i b_i
  * (scale NULL: 1), for the vectors of op's space (device pointers).  With a the adjoint state and
