@@ -187,7 +187,8 @@ def run_reference(args):
     return 0
 
 
-def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2, max_iters=20000):
+def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2, max_iters=20000,
+              plain=True):
     """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed), GMRES(restart) to tol
     relative FP64 residual from x0 = 0, timed on the device (CUDA events around the whole solve):
     FP64 GMRES with the reference's modified Gram-Schmidt, then the refinement solver with FP64
@@ -201,9 +202,14 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
     out = {"system": f"M/dt + A, dt={dt}, GMRES({restart}), tol {tol}, at most {max_iters} iterations, x0 = 0, "
                      f"b = FillRandom(seed {seed})", "kernel": A.kernel}
     sols = {}
-    legs = (("fp64_gmres", lambda: g.GMRESSolver(A, restart)),
+    P = g.MassInverseOperator(space, q or NQ, 1.0 / dt)  # element mass inverse (right preconditioner)
+    legs = [("fp64_gmres", lambda: g.GMRESSolver(A, restart)),
             ("fp64_gmres_ir", lambda: g.GMRESIRSolver(A, restart, inner="fp64")),
-            ("mixed_gmres_ir", lambda: g.GMRESIRSolver(A, restart, inner="fp32")))
+            ("mixed_gmres_ir", lambda: g.GMRESIRSolver(A, restart, inner="fp32"))]
+    if not plain:
+        legs = []
+    legs += [("fp64_gmres_massprec", lambda: g.GMRESSolver(A, restart).precondition(P)),
+             ("mixed_gmres_ir_massprec", lambda: g.GMRESIRSolver(A, restart, inner="fp32").precondition(P))]
     for name, make in legs:
         solver = make()
         x = torch.zeros_like(b)
@@ -223,11 +229,17 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
                      "converged": info["success"]}
         sols[name] = x
         solver.close()
-    for name in ("fp64_gmres_ir", "mixed_gmres_ir"):
-        d = (sols[name] - sols["fp64_gmres"]).abs().max() / sols["fp64_gmres"].abs().max()
-        out[name]["rel_max_diff_vs_fp64_gmres"] = d.item()
-    out["fp64_over_mixed_time"] = out["fp64_gmres"]["seconds"] / out["mixed_gmres_ir"]["seconds"]
+    ref = "fp64_gmres" if plain else "fp64_gmres_massprec"
+    for name in sols:
+        if name != ref:
+            d = (sols[name] - sols[ref]).abs().max() / sols[ref].abs().max()
+            out[name][f"rel_max_diff_vs_{ref}"] = d.item()
+    if plain:
+        out["fp64_over_mixed_time"] = out["fp64_gmres"]["seconds"] / out["mixed_gmres_ir"]["seconds"]
+    out["fp64_over_mixed_time_massprec"] = (out["fp64_gmres_massprec"]["seconds"] /
+                                            out["mixed_gmres_ir_massprec"]["seconds"])
     A.close()
+    P.close()
     return out
 
 
@@ -350,11 +362,11 @@ def run_ours(args):
         if world == 1 and not args.no_solve:
             if six:
                 # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3.  The unpreconditioned
-                # system's tensor-product mass matrix is ill-conditioned in 6D (GMRES(20) needs far
-                # more than 10^4 iterations to reach 1e-10), so both legs run the same bounded
-                # iteration budget and report the residual they reached.
+                # system's tensor-product mass matrix is ill-conditioned in 6D (GMRES(20) stands at
+                # a relative residual of 0.12 after 200 iterations), so the legs solve it with the
+                # element mass inverse as right preconditioner (same 1e-10 on |b - A x| / |b|).
                 line["solve"] = solve_leg(g, C, space, dev, dt=5e-3, restart=20, q=3,
-                                          beta=C.velocity_phase_space(6), seed=3, max_iters=200)
+                                          beta=C.velocity_phase_space(6), seed=3, max_iters=2000, plain=False)
             else:
                 line["solve"] = solve_leg(g, C, space, dev)
         if six:
