@@ -99,6 +99,10 @@ def lib():
         L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
         L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.dgop_batch_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
+        L.dgop_batch_groups.argtypes = [vp]
+        L.dgop_batch_apply.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
+        L.dgop_batch_destroy.argtypes = [vp]
         L.dgop_host_io_apply.argtypes = [vp, vp, vp, vp]
         L.dgop_host_io_destroy.argtypes = [vp]
         L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
@@ -415,6 +419,38 @@ class GMRESIRSolver(_Solver):
         h = ctypes.c_void_p()
         check(lib().dgop_gmres_ir_create(op.handle, int(restart), prec, ctypes.byref(h)))
         self.handle = h
+
+
+class Batch:
+    """Independent operators applied together: one persistent launch per (dimension, order) group
+    of any-dimension Kronecker operators, one launch each for the rest (dgop_batch_apply)."""
+
+    def __init__(self, ops):
+        self.ops = list(ops)
+        arr = (ctypes.c_void_p * len(self.ops))(*[o.handle for o in self.ops])
+        h = ctypes.c_void_p()
+        check(lib().dgop_batch_create(arr, len(self.ops), ctypes.byref(h)))
+        self.handle = h
+
+    @property
+    def groups(self):
+        return int(lib().dgop_batch_groups(self.handle))
+
+    def apply(self, xs, ys, stream=None):
+        xa = (ctypes.c_void_p * len(xs))(*[_ptr(x) for x in xs])
+        ya = (ctypes.c_void_p * len(ys))(*[_ptr(y) for y in ys])
+        check(lib().dgop_batch_apply(self.handle, xa, ya, _stream(stream)))
+
+    def close(self):
+        if self.handle:
+            lib().dgop_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class HostIO:

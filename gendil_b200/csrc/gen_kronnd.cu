@@ -18,6 +18,12 @@ void launch_kronnd(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t sm
   kronnd_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
 }
 
+template <int D, int N, typename Real>
+void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, int count, int eb, dim3 grid,
+                         dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_batch_kernel<D, N, Real><<<grid, block, smem, s>>>(table, first, count, eb);
+}
+
 // one element must fit in 200 KB of shared memory
 template <int D, int N, typename Real>
 constexpr bool fits() {
@@ -29,6 +35,8 @@ void fill(KronNDEntry<Real>& d) {
   if constexpr (fits<D, N, Real>()) {
     d.launch = &launch_kronnd<D, N, Real>;
     d.func = reinterpret_cast<const void*>(&kronnd_kernel<D, N, Real>);
+    d.launch_batch = &launch_kronnd_batch<D, N, Real>;
+    d.func_batch = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, Real>);
     d.per_elem = KronNDShape<D, N>::PER_ELEM;
   }
 }

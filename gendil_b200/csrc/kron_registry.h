@@ -40,6 +40,10 @@ template <typename Real>
 struct KronNDEntry {
   void (*launch)(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func = nullptr;
+  // many operators of this (D, N) in one launch (dgop_batch_apply)
+  void (*launch_batch)(const KronNDParams<Real>* table, const int64_t* first, int count, int eb, dim3 grid,
+                       dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func_batch = nullptr;
   int per_elem = 0;  // Real values of shared memory per element
 };
 KronNDEntry<double>& kronnd_slot_f64(int D, int N);

@@ -188,101 +188,74 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
   }
 }
 
+// One batch of ne elements starting at e0 (the CTA's shared memory holds them); x / y are the
+// instance's vectors.
 template <int D, int N, typename Real>
-__global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_constant__ KronNDParams<Real> P) {
+__device__ __forceinline__ void kronnd_block(const KronNDParams<Real>& P, const Real* __restrict__ xin,
+                                             Real* __restrict__ yout, int64_t e0, int ne, int EB, Real* base,
+                                             Real* escale, int (*ecoord)[kMaxDim]) {
   using S = KronNDShape<D, N>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Real* base = reinterpret_cast<Real*>(smem_raw);
-  __shared__ Real escale[64];          // per-element factor of the pass being run (EB <= 64)
-  __shared__ int ecoord[64][kMaxDim];  // element coordinates
-  if (P.skip && *P.skip) return;
-  const int EB = P.eb;
   const bool adv = P.has_adv != 0;
-  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
-    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
-    __syncthreads();
-    // input, accumulator
-    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-      const int b = l / S::ND, i = l - b * S::ND;
-      Real* el = base + (size_t)b * S::PER_ELEM;
-      el[i] = P.x[e0 * S::ND + l];
-      el[2 * S::ND + i] = Real(0);
-    }
-    if (threadIdx.x < ne) {
-      const int64_t e = e0 + threadIdx.x;
+  __syncthreads();
+  // input, accumulator
+  for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+    const int b = l / S::ND, i = l - b * S::ND;
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    el[i] = xin[e0 * S::ND + l];
+    el[2 * S::ND + i] = Real(0);
+  }
+  if (threadIdx.x < ne) {
+    const int64_t e = e0 + threadIdx.x;
 #pragma unroll
-      for (int k = 0; k < D; ++k) ecoord[threadIdx.x][k] = (int)((e / P.estride[k]) % P.sizes[k]);
-    }
-    __syncthreads();
-    // per element: slot matrices and face records
-    for (int l = threadIdx.x; l < ne * S::NS * S::MAT; l += blockDim.x) {
-      const int b = l / (S::NS * S::MAT);
-      const int r = l - b * (S::NS * S::MAT);
-      const int sl = r / S::MAT, q = r - sl * S::MAT;
-      const int a = sl / D, k = sl - a * D;  // a == D: the mass term
-      const KronMat m = a < D ? P.slot[a][k] : P.mslot[k];
-      Real v = Real(0);
-      if (m.off >= 0) v = P.mats[m.off + (int64_t)ecoord[b][k] * m.stride + q];
-      base[(size_t)b * S::PER_ELEM + 3 * S::ND + r] = v;
-    }
-    if (adv && threadIdx.x < ne) {
-      const int b = threadIdx.x;
-      const int64_t e = e0 + b;
-      int64_t c[kMaxDim];
+    for (int k = 0; k < D; ++k) ecoord[threadIdx.x][k] = (int)((e / P.estride[k]) % P.sizes[k]);
+  }
+  __syncthreads();
+  // per element: slot matrices and face records
+  for (int l = threadIdx.x; l < ne * S::NS * S::MAT; l += blockDim.x) {
+    const int b = l / (S::NS * S::MAT);
+    const int r = l - b * (S::NS * S::MAT);
+    const int sl = r / S::MAT, q = r - sl * S::MAT;
+    const int a = sl / D, k = sl - a * D;  // a == D: the mass term
+    const KronMat m = a < D ? P.slot[a][k] : P.mslot[k];
+    Real v = Real(0);
+    if (m.off >= 0) v = P.mats[m.off + (int64_t)ecoord[b][k] * m.stride + q];
+    base[(size_t)b * S::PER_ELEM + 3 * S::ND + r] = v;
+  }
+  if (adv && threadIdx.x < ne) {
+    const int b = threadIdx.x;
+    const int64_t e = e0 + b;
+    int64_t c[kMaxDim];
 #pragma unroll
-      for (int k = 0; k < D; ++k) c[k] = ecoord[b][k];
-      Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
-      uint32_t fl[2];
-      nd_face_records<D>(P, e, c, rec, fl);
-      reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl[0];
-      reinterpret_cast<uint32_t*>(rec + 4 * D)[1] = fl[1];
-    }
-    __syncthreads();
-    if (adv) {
-      static_for<0, D>([&](auto ac) {
-        constexpr int a = decltype(ac)::value;
-        if (P.elem[a]) {
-          if (threadIdx.x < ne) escale[threadIdx.x] = P.elem[a][e0 + threadIdx.x];
-          __syncthreads();
-        }
-        nd_pass<D, N, a, true, false>(base, ne, EB, a * D + a, P.elem[a] ? escale : (const Real*)nullptr);
-        __syncthreads();
-        nd_faces<D, N, a>(P, base, ne, e0, ecoord);
-        __syncthreads();
-        // tangential passes in increasing axis order; the last accumulates into Y
-        static_for<0, D>([&](auto kc) {
-          constexpr int k = decltype(kc)::value;
-          if constexpr (k != a) {
-            constexpr int lastk = (a == D - 1) ? D - 2 : D - 1;
-            nd_pass<D, N, k, false, k == lastk>(base, ne, EB, a * D + k, (const Real*)nullptr);
-            __syncthreads();
-          }
-        });
-        if constexpr (D == 1) {
-          // no tangential pass: the term goes straight to Y
-          for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-            const int b = l / S::ND, i = l - b * S::ND;
-            Real* el = base + (size_t)b * S::PER_ELEM;
-            el[2 * S::ND + i] += el[S::ND + i];
-          }
-          __syncthreads();
-        }
-      });
-    }
-    if (P.has_mass && !(adv && P.mass_merged)) {
-      // separate mass term: along the last axis (scaled), then the others
-      if (P.elem_mass) {
-        if (threadIdx.x < ne) escale[threadIdx.x] = P.elem_mass[e0 + threadIdx.x];
+    for (int k = 0; k < D; ++k) c[k] = ecoord[b][k];
+    Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
+    uint32_t fl[2];
+    nd_face_records<D>(P, e, c, rec, fl);
+    reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl[0];
+    reinterpret_cast<uint32_t*>(rec + 4 * D)[1] = fl[1];
+  }
+  __syncthreads();
+  if (adv) {
+    static_for<0, D>([&](auto ac) {
+      constexpr int a = decltype(ac)::value;
+      if (P.elem[a]) {
+        if (threadIdx.x < ne) escale[threadIdx.x] = P.elem[a][e0 + threadIdx.x];
         __syncthreads();
       }
-      nd_pass<D, N, D - 1, true, false>(base, ne, EB, D * D + D - 1, P.elem_mass ? escale : (const Real*)nullptr);
+      nd_pass<D, N, a, true, false>(base, ne, EB, a * D + a, P.elem[a] ? escale : (const Real*)nullptr);
       __syncthreads();
-      static_for<0, D - 1>([&](auto kc) {
+      nd_faces<D, N, a>(P, base, ne, e0, ecoord);
+      __syncthreads();
+      // tangential passes in increasing axis order; the last accumulates into Y
+      static_for<0, D>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        nd_pass<D, N, k, false, k == D - 2>(base, ne, EB, D * D + k, (const Real*)nullptr);
-        __syncthreads();
+        if constexpr (k != a) {
+          constexpr int lastk = (a == D - 1) ? D - 2 : D - 1;
+          nd_pass<D, N, k, false, k == lastk>(base, ne, EB, a * D + k, (const Real*)nullptr);
+          __syncthreads();
+        }
       });
       if constexpr (D == 1) {
+        // no tangential pass: the term goes straight to Y
         for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
           const int b = l / S::ND, i = l - b * S::ND;
           Real* el = base + (size_t)b * S::PER_ELEM;
@@ -290,14 +263,76 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
         }
         __syncthreads();
       }
+    });
+  }
+  if (P.has_mass && !(adv && P.mass_merged)) {
+    // separate mass term: along the last axis (scaled), then the others
+    if (P.elem_mass) {
+      if (threadIdx.x < ne) escale[threadIdx.x] = P.elem_mass[e0 + threadIdx.x];
+      __syncthreads();
     }
-    // y = alpha Y + beta_y y
-    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-      const int b = l / S::ND, i = l - b * S::ND;
-      const Real v = base[(size_t)b * S::PER_ELEM + 2 * S::ND + i];
-      Real* dst = P.y + e0 * S::ND + l;
-      *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
+    nd_pass<D, N, D - 1, true, false>(base, ne, EB, D * D + D - 1, P.elem_mass ? escale : (const Real*)nullptr);
+    __syncthreads();
+    static_for<0, D - 1>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      nd_pass<D, N, k, false, k == D - 2>(base, ne, EB, D * D + k, (const Real*)nullptr);
+      __syncthreads();
+    });
+    if constexpr (D == 1) {
+      for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+        const int b = l / S::ND, i = l - b * S::ND;
+        Real* el = base + (size_t)b * S::PER_ELEM;
+        el[2 * S::ND + i] += el[S::ND + i];
+      }
+      __syncthreads();
     }
+  }
+  // y = alpha Y + beta_y y
+  for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+    const int b = l / S::ND, i = l - b * S::ND;
+    const Real v = base[(size_t)b * S::PER_ELEM + 2 * S::ND + i];
+    Real* dst = yout + e0 * S::ND + l;
+    *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
+  }
+}
+
+template <int D, int N, typename Real>
+__global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_constant__ KronNDParams<Real> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* base = reinterpret_cast<Real*>(smem_raw);
+  __shared__ Real escale[64];          // per-element factor of the pass being run (EB <= 64)
+  __shared__ int ecoord[64][kMaxDim];  // element coordinates
+  if (P.skip && *P.skip) return;
+  const int EB = P.eb;
+  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
+  }
+}
+
+// Many operators of one (D, N) in one persistent launch: table[i] holds instance i's parameters
+// (forward operator, x / y set per apply), its element batches are the global batch indices
+// [first[i], first[i + 1]); every CTA walks the global batches.
+template <int D, int N, typename Real>
+__global__ void __launch_bounds__(kKronNDThreads)
+    kronnd_batch_kernel(const KronNDParams<Real>* __restrict__ table, const int64_t* __restrict__ first, int count,
+                        int EB) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* base = reinterpret_cast<Real*>(smem_raw);
+  __shared__ Real escale[64];
+  __shared__ int ecoord[64][kMaxDim];
+  const int64_t total = first[count];
+  for (int64_t gb = blockIdx.x; gb < total; gb += gridDim.x) {
+    int lo = 0, hi = count;  // instance: the last i with first[i] <= gb
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (first[mid] <= gb) lo = mid;
+      else hi = mid;
+    }
+    const KronNDParams<Real>& P = table[lo];
+    const int64_t e0 = (gb - first[lo]) * EB;
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
   }
 }
 

@@ -120,6 +120,17 @@ int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* st
 /* FP32 apply of the same operator (tables rounded to FP32); no reference counterpart. */
 int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
 
+/* Batches of independent operators (no reference counterpart; configuration 5 of the benchmark
+ * plan): operators on the any-dimension Kronecker kernel are grouped by (dimension, order) and
+ * each group is applied by ONE persistent launch over all its operators' elements; the others are
+ * applied one launch each.  y[i] = A_i x[i] (device pointers), bit-identical to dgop_apply.  The
+ * operators must outlive the batch.  dgop_batch_groups gives the number of grouped launches. */
+typedef struct dgop_batch dgop_batch;
+int dgop_batch_create(dgop_operator* const* ops, int count, dgop_batch** out);
+int dgop_batch_groups(const dgop_batch* batch);
+int dgop_batch_apply(dgop_batch* batch, const double* const* x, double* const* y, void* stream);
+int dgop_batch_destroy(dgop_batch* batch);
+
 /* Applies on HOST vectors (the reference's operator() on a host-resident Vector,
  * massoperator.hpp:209, advectionoperator.hpp:1070, where the data lives in host memory):
  * y_host = A x_host.  The host-to-device copy, the apply and the device-to-host copy are pipelined
