@@ -455,6 +455,7 @@ def run_batch(args):
         ok = [False] * len(ops)
         order = sorted(range(len(ops)), key=lambda i: -dofs[i])  # largest first
         lock = threading.Lock()
+        errors = []
 
         def worker():
             st = torch.cuda.Stream()
@@ -465,17 +466,22 @@ def run_batch(args):
                             return
                         i = order.pop(0)
                     A, P, b = ops[i], precs[i], bs[i]
-                    s = (g.GMRESSolver(A, 20) if kind == "fp64" else g.GMRESIRSolver(A, 20, inner="fp32")).precondition(P)
-                    x = torch.zeros_like(b)
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record(st)
-                    info = s.solve(b, x, 2000, 1e-10, stream=st)
-                    e1.record(st)
-                    e1.synchronize()
-                    times[i] = e0.elapsed_time(e1) * 1e-3
-                    iters[i], ok[i] = info["iterations"], info["success"]
-                    s.close()
-                    del x
+                    try:
+                        s = (g.GMRESSolver(A, 20) if kind == "fp64" else
+                             g.GMRESIRSolver(A, 20, inner="fp32")).precondition(P)
+                        x = torch.zeros_like(b)
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(st)
+                        info = s.solve(b, x, 2000, 1e-10, stream=st)
+                        e1.record(st)
+                        e1.synchronize()
+                        times[i] = e0.elapsed_time(e1) * 1e-3
+                        iters[i], ok[i] = info["iterations"], info["success"]
+                        s.close()
+                        del x
+                    except Exception as exc:  # reported as an unconverged instance
+                        with lock:
+                            errors.append(f"instance {i}: {exc}")
 
         torch.cuda.synchronize()
         w0 = time.time()
@@ -488,6 +494,7 @@ def run_batch(args):
         wall = time.time() - w0
         ts = np.array(times)
         return {"wall_s": wall, "solved_gdofs_per_s": total / wall / 1e9, "converged": int(sum(ok)),
+                "errors": errors[:3],
                 "iterations_median": float(np.median(iters)), "iterations_max": int(max(iters)),
                 "instance_s": {"p50": float(np.percentile(ts, 50)), "p90": float(np.percentile(ts, 90)),
                                "p99": float(np.percentile(ts, 99)), "max": float(ts.max())}}

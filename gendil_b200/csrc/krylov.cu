@@ -29,6 +29,11 @@ constexpr int kRB = 592;  // reduction blocks (4 per SM on 148 SMs)
 constexpr int kRT = 256;  // threads per reduction block
 constexpr int kCheckEvery = 8;  // CG iterations per chunk (even)
 
+// Stride of the solvers' workspace vectors: n rounded up to 64 entries, so every vector starts
+// 256-byte aligned (the operator kernels stage elements with 16-byte copies).  Padding entries
+// are zero from creation on and stay zero.
+inline int64_t vec_stride(int64_t n) { return (n + 63) / 64 * 64; }
+
 // Sum over the block in a fixed order; the result is valid in thread 0.
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double ws[kRT / 32];
@@ -684,8 +689,8 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
              cudaStream_t st) {
   const int64_t n = s.n;
   double* tmp = s.work;
-  double* r = s.work + n;
-  double* p = s.work + 2 * n;
+  double* r = s.work + vec_stride(n);
+  double* p = s.work + 2 * vec_stride(n);
   double* pa = s.partials;
   double* pb = s.partials + kRB;
   CGState* cs = static_cast<CGState*>(s.state);
@@ -722,7 +727,8 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   const int64_t n = s.n;
   const int m = s.restart;
   double* w = s.work;
-  double* V = s.work + n;  // m + 1 basis vectors
+  const int64_t ld = vec_stride(n);
+  double* V = s.work + ld;  // m + 1 basis vectors, stride ld
   double* pa = s.partials;
   double* pb = s.partials + kRB;
   double* H = s.small;
@@ -744,7 +750,7 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m);
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
     for (int j = 0; j < m; ++j) {
-      double* vj = V + (int64_t)j * n;
+      double* vj = V + (int64_t)j * ld;
       if (s.prec) {
         double* z = static_cast<double*>(s.pz);
         DGOP_TRY(launch_f64(s.prec, 1.0, vj, 0.0, z, 0, q, inactive));
@@ -756,13 +762,13 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
       double* pin = pa;
       double* pout = pb;
       for (int i = 0; i <= j; ++i) {
-        const double* next = (i < j) ? V + (int64_t)(i + 1) * n : w;
-        k_gm_mgs<<<kRB, kRT, 0, q>>>(gs, i, j, m, static_cast<const double*>(V + (int64_t)i * n), next, w, n, H,
+        const double* next = (i < j) ? V + (int64_t)(i + 1) * ld : w;
+        k_gm_mgs<<<kRB, kRT, 0, q>>>(gs, i, j, m, static_cast<const double*>(V + (int64_t)i * ld), next, w, n, H,
                                      pin, pout);
         std::swap(pin, pout);
       }
       k_gm_column<<<1, kRT, 0, q>>>(gs, j, m, H, csv, snv, e1, pin);
-      k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(w), V + (int64_t)(j + 1) * n, n, j);
+      k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(w), V + (int64_t)(j + 1) * ld, n, j);
       DGOP_CUDA_S(cudaGetLastError());
     }
     k_gm_backsub<<<1, 1, 0, q>>>(gs, H, e1, y, m);
@@ -794,10 +800,8 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   return finish<GMState>(s, st, res);
 }
 
-// Vector stride of the refinement solver's inner workspace: n rounded up to 64 entries
-// (256 bytes for FP32), so every inner vector starts 16-byte aligned for 128-bit accesses.
-// The padding entries are zero from creation on and stay zero.
-int64_t ir_stride(int64_t n) { return (n + 63) / 64 * 64; }
+// Vector stride of the refinement solver's inner workspace (the same rounding as vec_stride).
+int64_t ir_stride(int64_t n) { return vec_stride(n); }
 
 int apply_inner(dgop_operator* op, const float* x, float* y, int flags, cudaStream_t st, const int* skip) {
   return launch_f32(op, 1.0f, x, 0.0f, y, kLinear | flags, st, skip);
@@ -821,8 +825,8 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
   const int m = s.restart;
   const int64_t ld = ir_stride(n);
   double* w64 = s.work;
-  double* r64 = s.work + n;
-  T* w = reinterpret_cast<T*>(s.work + 2 * n);
+  double* r64 = s.work + vec_stride(n);
+  T* w = reinterpret_cast<T*>(s.work + 2 * vec_stride(n));
   T* V = w + ld;  // m + 1 inner basis vectors, stride ld
   double* pa = s.partials;
   double* H = s.small;
@@ -921,7 +925,7 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dg
   // two FP64 vectors (A x, residual), then restart + 2 inner vectors (w and the basis) at stride
   // ir_stride(n); the padding entries must read as zero, so the workspace starts zeroed
   const size_t inner_words = (size_t)ir_stride(s.n) * (inner_precision == DGOP_FP32 ? 4 : 8) / 8;
-  const size_t words = 2 * (size_t)s.n + (size_t)(restart + 2) * inner_words;
+  const size_t words = 2 * (size_t)vec_stride(s.n) + (size_t)(restart + 2) * inner_words;
   int rc = solver_alloc(sv, words, sizeof(GMState), small);
   if (rc == DGOP_OK) {
     cudaError_t e = cudaMemset(s.work, 0, sizeof(double) * words);
@@ -951,7 +955,7 @@ int dgop_cg_create(dgop_operator* op, dgop_solver** out) {
   sv->s.kind = 0;
   sv->s.op = op;
   sv->s.n = op->sp.ndofs;
-  const int rc = solver_alloc(sv, 3 * (size_t)sv->s.n, sizeof(CGState), 0);
+  const int rc = solver_alloc(sv, 3 * (size_t)vec_stride(sv->s.n), sizeof(CGState), 0);
   if (rc != DGOP_OK) {
     solver_free(sv);
     delete sv;
@@ -977,7 +981,7 @@ int dgop_gmres_create(dgop_operator* op, int restart, dgop_solver** out) {
   sv->s.n = op->sp.ndofs;
   sv->s.restart = restart;
   const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
-  const int rc = solver_alloc(sv, (size_t)(restart + 2) * sv->s.n, sizeof(GMState), small);
+  const int rc = solver_alloc(sv, (size_t)(restart + 2) * vec_stride(sv->s.n), sizeof(GMState), small);
   if (rc != DGOP_OK) {
     solver_free(sv);
     delete sv;
