@@ -775,10 +775,10 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     if (s.prec) {
       // x += P (sum_i y_i V_i)
       DGOP_CUDA_S(cudaMemsetAsync(s.pt, 0, sizeof(double) * n, q));
-      k_gm_update<<<kRB, kRT, 0, q>>>(gs, s.pt, static_cast<const double*>(V), n, y, n);
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, s.pt, static_cast<const double*>(V), ld, y, n);
       DGOP_TRY(launch_f64(s.prec, 1.0, s.pt, 1.0, x, 0, q, done));
     } else {
-      k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const double*>(V), n, y, n);
+      k_gm_update<<<kRB, kRT, 0, q>>>(gs, x, static_cast<const double*>(V), ld, y, n);
     }
     return residual(1, q);
   };
