@@ -249,15 +249,11 @@ def run_ours(args):
     import gendil_b200 as g
     from gendil_b200 import coefficients as C
 
+    from gendil_b200.replicas import Replicas
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    reps = Replicas("nccl")  # independent replicas: only barriers and the max-over-ranks timing
 
     six = args.workload == "6d"
     if six:
@@ -276,10 +272,7 @@ def run_ours(args):
     y = torch.empty_like(x)
     stream = torch.cuda.current_stream()
 
-    def barrier():
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
+    barrier = reps.barrier
 
     for _ in range(args.warmup):
         op(x, y)
@@ -291,13 +284,9 @@ def run_ours(args):
             op(x, y)
         stop.record(stream)
         barrier()
-    ms = start.elapsed_time(stop)
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reps.max(start.elapsed_time(stop))
     ms_step = ms / args.steps
-    value = world * nd * args.steps / (ms * 1e-3) / 1e9
+    value = reps.throughput(nd * args.steps, ms) / 1e9
 
     # end to end through the C ABI on host vectors (dgop_host_io_apply): pinned host input ->
     # device -> apply -> host result, upload / apply / download pipelined over slabs of z planes
@@ -315,12 +304,8 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     io.close()
-    ems = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([ems], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e_value = world * nd * e_steps / (ems * 1e-3) / 1e9
+    ems = reps.max(e0.elapsed_time(e1))
+    e2e_value = reps.throughput(nd * e_steps, ems) / 1e9
 
     hbm, peak_kind = peaks()
     alg_bytes = 16.0 * nd
@@ -377,8 +362,7 @@ def run_ours(args):
             except Exception as exc:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"unavailable": str(exc)}
         print(json.dumps(line))
-    if pg:
-        pg.destroy_process_group()
+    reps.close()
     return 0
 
 
