@@ -96,6 +96,7 @@ def lib():
         L.dgop_solver_set_graphs.argtypes = [vp, i]
         L.dgop_solver_set_transpose.argtypes = [vp, i]
         L.dgop_solver_set_preconditioner.argtypes = [vp, vp]
+        L.dgop_sipdg_create.argtypes = [vp, i, vp, ctypes.c_double, ctypes.c_double, i, ctypes.POINTER(vp)]
         L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
         L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
@@ -243,7 +244,7 @@ class _Operator:
     def kernel(self):
         """'generic' (sum-factorized), 'kron' (register-resident 3D Kronecker form) or 'kronnd'
         (shared-memory Kronecker form, any dimension)."""
-        return ("generic", "kron", "kronnd")[lib().dgop_operator_kernel(self.handle)]
+        return ("generic", "kron", "kronnd", "diffusion")[lib().dgop_operator_kernel(self.handle)]
 
     @property
     def kernel_note(self):
@@ -293,6 +294,22 @@ class MassOperator(_Operator):
         super().__init__(space, q)
         h = ctypes.c_void_p()
         check(lib().dgop_mass_create(space.handle, q, ctypes.byref(self._coef(sigma)), ctypes.byref(h)))
+        self.handle = h
+
+
+class SIPDGOperator(_Operator):
+    """Interior-penalty DG diffusion (the reference's SIPDG weak form): mu one diffusivity per
+    element (FP64 device tensor, kept alive here), tau = kappa / h, sigma = -1 symmetric (SIPG),
+    +1 NIPG, 0 IIPG; Dirichlet-0 boundary terms when `boundary`."""
+
+    def __init__(self, space, q, mu, sigma=-1.0, kappa=None, boundary=True):
+        super().__init__(space, q)
+        if kappa is None:
+            kappa = 10.0 * (space.order + 1) ** 2
+        self.mu = mu
+        h = ctypes.c_void_p()
+        check(lib().dgop_sipdg_create(space.handle, q, _ptr(mu), float(sigma), float(kappa), 1 if boundary else 0,
+                                      ctypes.byref(h)))
         self.handle = h
 
 

@@ -91,6 +91,10 @@ int pack_coef(const dgop_space& s, int q, const dgop_coef* c, std::vector<double
   return DGOP_OK;
 }
 
+int device_sm_count(int dev);
+}  // namespace
+int device_sms(int dev) { return device_sm_count(dev); }
+namespace {
 int device_sm_count(int dev) {
   static int cache[64] = {};
   if (dev < 0 || dev >= 64) return 148;
@@ -729,9 +733,9 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 }  // namespace
 
 template <typename Real>
-static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, KronNDCfg<Real>& KN, Real alpha,
-                       const Real* x, Real beta_y, Real* y, int extra_flags, cudaStream_t s, const int* skip,
-                       int64_t e_begin = 0, int64_t e_end = -1) {
+static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, KronNDCfg<Real>& KN,
+                       KronDiffCfg<Real>& SD, Real alpha, const Real* x, Real beta_y, Real* y, int extra_flags,
+                       cudaStream_t s, const int* skip, int64_t e_begin = 0, int64_t e_end = -1) {
   if (e_end < 0) e_end = op->sp.nelem;
   if (!x || !y) {
     set_error("null vector");
@@ -755,6 +759,28 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   }
   const bool linear = (extra_flags & kLinear) != 0;
   extra_flags &= ~kLinear;
+  if (op->kernel == DGOP_KERNEL_DIFF) {
+    if (!SD.ready) {
+      set_error("the diffusion operator has no kernel for this precision");
+      return DGOP_ERR_UNSUPPORTED;
+    }
+    if ((extra_flags & kTranspose) && op->ip_sigma != -1.0) {
+      set_error("the transposed interior-penalty operator is provided for the symmetric form (sigma = -1) only");
+      return DGOP_ERR_UNSUPPORTED;
+    }
+    KronDiffParams<Real> p = SD.params;  // symmetric for sigma = -1: the transpose is the operator
+    p.x = x;
+    p.y = y;
+    p.alpha = alpha;
+    p.beta_y = beta_y;
+    p.skip = skip;
+    p.e_begin = e_begin;
+    p.nelem = e_end;
+    SD.entry->launch_diff(p, SD.grid, SD.block, SD.smem, s);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
+    return DGOP_OK;
+  }
   if (op->kernel == DGOP_KERNEL_KRONND && KN.ready) {
     KronNDParams<Real> p = (extra_flags & kTranspose) ? KN.params_t : KN.params;
     p.x = x;
@@ -810,16 +836,16 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
 
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
                cudaStream_t s, const int* skip) {
-  return launch_impl<double>(op, op->f64, op->k64, op->n64, alpha, x, beta_y, y, extra_flags, s, skip);
+  return launch_impl<double>(op, op->f64, op->k64, op->n64, op->s64, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s, const int* skip) {
-  return launch_impl<float>(op, op->f32, op->k32, op->n32, alpha, x, beta_y, y, extra_flags, s, skip);
+  return launch_impl<float>(op, op->f32, op->k32, op->n32, op->s32, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
 int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s) {
-  return launch_impl<double>(op, op->f64, op->k64, op->n64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
+  return launch_impl<double>(op, op->f64, op->k64, op->n64, op->s64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
 }
 
 }  // namespace dgop
@@ -959,6 +985,8 @@ int dgop_operator_destroy(dgop_operator* op) {
   free_kron(op->k32);
   free_kronnd(op->n64);
   free_kronnd(op->n32);
+  free_diff(op->s64);
+  free_diff(op->s32);
   delete op;
   return DGOP_OK;
 }

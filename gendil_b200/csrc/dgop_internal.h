@@ -68,6 +68,17 @@ struct KronNDCfg {
   Real* d_elem[kMaxDim + 1] = {};  // converted per-element factors (FP32 only)
 };
 
+template <typename Real>
+struct KronDiffCfg {
+  bool ready = false;
+  const KronNDEntry<Real>* entry = nullptr;
+  KronDiffParams<Real> params{};
+  dim3 grid, block;
+  size_t smem = 0;
+  Real* d_mats = nullptr;
+  Real* d_mu = nullptr;  // FP32 copy of the per-element diffusivity
+};
+
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
@@ -88,6 +99,9 @@ struct dgop_operator {
   dgop::KronCfg<float> k32;
   dgop::KronNDCfg<double> n64;
   dgop::KronNDCfg<float> n32;
+  dgop::KronDiffCfg<double> s64;  // interior-penalty diffusion (dgop_sipdg_create)
+  dgop::KronDiffCfg<float> s32;
+  double ip_sigma = 0.0;
 };
 
 namespace dgop {
@@ -99,4 +113,7 @@ int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, flo
                cudaStream_t s, const int* skip = nullptr);
 // y = Op(x) on the elements [e_begin, e_end) only (y elsewhere untouched; x read around them)
 int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s);
+int device_sms(int dev);
+template <typename Real>
+void free_diff(KronDiffCfg<Real>& K);
 }  // namespace dgop

@@ -19,6 +19,7 @@ enum OpFlags : int {
   kTranspose = 1 << 4,  // apply the transposed (adjoint) operator
   kLinear = 1 << 5,     // host-side launch option: inflow value taken as 0 (the linear part)
   kInvMass = 1 << 6,    // operator is the inverse of the element mass matrices (Kronecker kernels only)
+  kDiffusion = 1 << 7,  // interior-penalty diffusion operator (dgop_sipdg_create)
 };
 
 // A scalar coefficient c(X) = constant + sum_t prod_k T_{t,k}(X_k), optionally multiplied by a

@@ -1,6 +1,7 @@
 // Instantiation unit of the any-dimension Kronecker kernel, compiled once per dimension with
 // -DDGOP_GEN_D=<dim>: every N = 1..8 whose element (U, W, Y, matrices) fits in shared memory.
 #include "kron_registry.h"
+#include "kronnd_diff_kernel.cuh"
 #include "kronnd_kernel.cuh"
 
 #ifndef DGOP_GEN_D
@@ -24,6 +25,11 @@ void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, 
   kronnd_batch_kernel<D, N, Real><<<grid, block, smem, s>>>(table, first, count, eb);
 }
 
+template <int D, int N, typename Real>
+void launch_kronnd_diff(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_diff_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
+}
+
 // one element must fit in 200 KB of shared memory
 template <int D, int N, typename Real>
 constexpr bool fits() {
@@ -38,6 +44,11 @@ void fill(KronNDEntry<Real>& d) {
     d.launch_batch = &launch_kronnd_batch<D, N, Real>;
     d.func_batch = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, Real>);
     d.per_elem = KronNDShape<D, N>::PER_ELEM;
+  }
+  if constexpr ((int64_t)KronDiffShape<D, N>::PER_ELEM * (int64_t)sizeof(Real) <= 200 * 1024) {
+    d.launch_diff = &launch_kronnd_diff<D, N, Real>;
+    d.func_diff = reinterpret_cast<const void*>(&kronnd_diff_kernel<D, N, Real>);
+    d.per_elem_diff = KronDiffShape<D, N>::PER_ELEM;
   }
 }
 }  // namespace

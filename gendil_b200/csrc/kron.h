@@ -103,6 +103,37 @@ struct KronNDParams {
   const int* skip;
 };
 
+// Interior-penalty diffusion (kronnd_diff_kernel.cuh, sipdg.cu).
+// Base matrix k of axis a in the table: mats[(a * kDiffMats + k) * N * N]
+enum DiffMat : int {
+  kDK = 0,    // Khat
+  kDP1 = 1,   // P1_0, P1_1
+  kDP2 = 3,   // P2_0, P2_1
+  kDP3 = 5,   // P3_0, P3_1
+  kDQ1 = 7,   // Q1_0, Q1_1
+  kDQ2 = 9,   // Q2_0, Q2_1
+  kDQ3 = 11,  // Q3_0, Q3_1
+  kDM = 13,   // reference mass M_a (tangential factor)
+  kDiffMats = 14
+};
+
+template <typename Real>
+struct KronDiffParams {
+  int64_t nelem, e_begin;
+  int64_t sizes[kMaxDim];
+  int64_t estride[kMaxDim];
+  int periodic[kMaxDim];
+  int boundary;  // Dirichlet-0 boundary terms
+  int eb;        // elements per CTA
+  Real sigma;    // -1 SIPG, +1 NIPG, 0 IIPG
+  Real alpha, beta_y;
+  const Real* x;
+  Real* y;
+  const Real* mu;    // per element (device)
+  const Real* mats;  // D x kDiffMats base matrices, N x N each (device)
+  const int* skip;
+};
+
 struct KronPlanHost {
   bool ok = false;
   const char* why = "";

@@ -45,6 +45,10 @@ struct KronNDEntry {
                        dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_batch = nullptr;
   int per_elem = 0;  // Real values of shared memory per element
+  // interior-penalty diffusion (kronnd_diff_kernel.cuh)
+  void (*launch_diff)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func_diff = nullptr;
+  int per_elem_diff = 0;
 };
 KronNDEntry<double>& kronnd_slot_f64(int D, int N);
 KronNDEntry<float>& kronnd_slot_f32(int D, int N);

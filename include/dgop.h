@@ -80,6 +80,17 @@ int dgop_system_create(const dgop_space* space, int q, const dgop_coef* sigma, c
  *                  preconditioner of dgop_solver_set_preconditioner).  Needs the Kronecker form:
  *                  GLL basis, a density that is one separable product, no per-element factor. */
 int dgop_mass_inverse_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out);
+/* sipdg:           y = A x for the interior-penalty DG diffusion form of the reference's weak-form
+ *                  DSL (README "Weak Form DSL"; test-sipdg-coefficient-field-inputs.cpp:560-569):
+ *                  integrate(cells, mu grad u . grad v) + integrate(interior_facets,
+ *                  -{mu grad u . n}[v] + sigma [u]{mu grad v . n} + tau {mu}[u][v]) and, when
+ *                  `boundary`, integrate(boundary_facets, -mu grad u . n v + sigma u mu grad v . n
+ *                  + tau mu u v) (Dirichlet 0).  mu: DEVICE array, one diffusivity per element (kept,
+ *                  not copied); tau = kappa / h on each face (InverseFacetSize); sigma = -1 gives the
+ *                  symmetric form (SIPG), +1 NIPG, 0 IIPG.  Any dimension, any basis; the element must
+ *                  fit in shared memory (kernel DGOP_KERNEL_DIFF). */
+int dgop_sipdg_create(const dgop_space* space, int q, const double* mu, double sigma, double kappa, int boundary,
+                      dgop_operator** out);
 int dgop_operator_destroy(dgop_operator* op);
 int64_t dgop_operator_num_dofs(const dgop_operator* op);
 
@@ -91,7 +102,7 @@ int64_t dgop_operator_num_dofs(const dgop_operator* op);
  * (GLL, separable coefficients, element within shared memory), chosen when the register kernel
  * does not apply.
  * dgop_operator_kernel_note() says why the Kronecker form was not chosen. */
-enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1, DGOP_KERNEL_KRONND = 2 };
+enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1, DGOP_KERNEL_KRONND = 2, DGOP_KERNEL_DIFF = 3 };
 int dgop_operator_kernel(const dgop_operator* op);
 const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);

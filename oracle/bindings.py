@@ -141,6 +141,19 @@ class Reference(_Lib):
     def num_threads(self):
         return int(self.lib.gref_num_threads())
 
+    def sipdg_apply(self, case, mu_elem, sigma, kappa, boundary, x):
+        """The reference's generic SIPDG form (part_sipdg.cpp): mu per element, tau = kappa / h,
+        sigma = -1 SIPG / +1 NIPG / 0 IIPG, Dirichlet-0 boundary terms when `boundary`."""
+        sizes, h, origin, periodic = self._mesh(case)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        mu = np.ascontiguousarray(mu_elem, dtype=np.float64)
+        y = np.zeros_like(x)
+        rc = self.lib.gref_sipdg_apply(case["D"], case["P"], case["Q"], _p(sizes), _p(h), _p(origin), _p(periodic),
+                                       _p(mu), _cd(sigma), _cd(kappa), int(boundary), _p(x), _p(y))
+        if rc != 0:
+            raise NotImplementedError("sipdg_apply: case not instantiated")
+        return y
+
     def time_advection(self, case, x, pairs):
         """Seconds per apply of the reference advection operator (inflow value case['g'])."""
         sizes, h, origin, _ = self._mesh(case)

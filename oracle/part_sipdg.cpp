@@ -1,0 +1,74 @@
+// Test infrastructure only (CPU oracle): the reference's generic SIPDG diffusion weak form
+// (README.md "Weak Form DSL", tests/integration/gendil/test-sipdg-coefficient-field-inputs.cpp:
+// 547-575): mu a finite-element field (here constant on each element: every node of element e
+// holds mu_e), tau = kappa * InverseFacetSize, sigma = -1 (SIPG), +1 (NIPG) or 0 (IIPG), and
+// optionally the Dirichlet-0 boundary terms of the README form with the same sigma.
+#include "ref_impl.hpp"
+
+namespace gref {
+
+template < int D, int P, int Q >
+void SipdgApply( const MeshArgs & m, const double * mu_elem, double sigma, double kappa, int boundary,
+                 const double * x, double * y )
+{
+   WithSpace< D, P, Q, 0 >( m, [&]( auto & fes, auto & ir )
+   {
+      const size_t n = fes.GetNumberOfFiniteElementDofs();
+      const size_t ne = fes.GetNumberOfFiniteElements();
+      const size_t nd = n / ne;
+      Vector vx( n ), vy( n ), vmu( n );
+      CopyIn( vx, x );
+      Real * md = vmu.WriteHostData();
+      for ( size_t e = 0; e < ne; ++e )
+         for ( size_t i = 0; i < nd; ++i ) md[ e * nd + i ] = mu_elem[ e ];
+      auto mu_view = MakeReadOnlyElementTensorView< SerialKernelConfiguration >( fes, vmu );
+      TrialSpace< "u" > u;
+      TestSpace< "u" > v;
+      Cells< "mesh" > cells;
+      InteriorFacets< "mesh" > interior_facets;
+      BoundaryFacets< "mesh" > boundary_facets;
+      auto mu = MakeCoefficient< "diffusivity", FieldValue< "mu" > >(
+         [] GENDIL_HOST_DEVICE ( const Real mu_q ) -> Real { return mu_q; } );
+      auto tau = MakeCoefficient< "penalty", InverseFacetSize >(
+         [=] GENDIL_HOST_DEVICE ( const Real h_inv ) -> Real { return kappa * h_inv; } );
+      auto interior = integrate( cells, mu * dot( grad( u ), grad( v ) ) ) +
+                      integrate( interior_facets,
+                                 - average( mu * dot( grad( u ), Normal{} ) ) * jump( v )
+                                 + sigma * jump( u ) * average( mu * dot( grad( v ), Normal{} ) )
+                                 + tau * average( mu ) * jump( u ) * jump( v ) );
+      auto ctx = MakeWeakFormContext( MakeTrialField< "u" >( fes ), MakeFiniteElementField< "mu" >( fes, mu_view ),
+                                      MakeIntegrationDomain< "mesh" >( fes ) );
+      vy = 0.0;
+      if ( boundary )
+      {
+         auto form = interior + integrate( boundary_facets,
+                                           - mu * dot( grad( u ), Normal{} ) * v
+                                           + sigma * u * mu * dot( grad( v ), Normal{} )
+                                           + tau * mu * u * v );
+         auto op = MakeGenericOperator< SerialKernelConfiguration >( form, ctx, ir );
+         op( vx, vy );
+      }
+      else
+      {
+         auto op = MakeGenericOperator< SerialKernelConfiguration >( interior, ctx, ir );
+         op( vx, vy );
+      }
+      CopyOut( vy, y );
+   } );
+}
+
+}  // namespace gref
+
+#define GREF_SIPDG_LIST( X ) X( 2, 1, 3 ) X( 2, 2, 4 ) X( 3, 1, 3 ) X( 3, 2, 4 ) X( 3, 3, 5 ) X( 3, 4, 6 )
+
+extern "C" int gref_sipdg_apply( int D, int P, int Q, const long * sizes, const double * h, const double * origin,
+                                 const int * periodic, const double * mu_elem, double sigma, double kappa,
+                                 int boundary, const double * x, double * y )
+{
+   gref::MeshArgs m{ sizes, h, origin, periodic };
+#define X( d, p, q ) \
+   if ( D == d && P == p && Q == q ) { gref::SipdgApply< d, p, q >( m, mu_elem, sigma, kappa, boundary, x, y ); return 0; }
+   GREF_SIPDG_LIST( X )
+#undef X
+   return gref::GREF_UNSUPPORTED;
+}

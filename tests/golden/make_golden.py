@@ -106,9 +106,23 @@ def adv_cases():
     return c
 
 
+def sipdg_cases():
+    """The reference's generic SIPDG form (oracle/part_sipdg.cpp): mu_e = exp(z_e), z_e normal
+    with standard deviation 0.5 from numpy seed 4 (configuration 4's field), kappa = 10 (p+1)^2."""
+    c = []
+    c.append(("s1", dict(cube(2, 0, 1, 3, sizes=[5, 4]), sigma=-1.0, boundary=1)))
+    c.append(("s2", dict(cube(2, 0, 2, 4, sizes=[3, 4], periodic=[1, 0]), sigma=-1.0, boundary=1)))
+    c.append(("s3", dict(cube(3, 0, 1, 3, sizes=[4, 3, 3]), sigma=-1.0, boundary=1)))
+    c.append(("s4", dict(cube(3, 0, 2, 4, sizes=[3, 3, 2]), sigma=-1.0, boundary=0)))
+    c.append(("s5", dict(cube(3, 0, 3, 5, sizes=[3, 2, 2]), sigma=1.0, boundary=1)))
+    c.append(("s6", dict(cube(3, 0, 4, 6, sizes=[2, 3, 2]), sigma=-1.0, boundary=1)))
+    c.append(("s7", dict(cube(3, 0, 4, 6, sizes=[3, 2, 2], h=[0.2, 0.5, 0.25]), sigma=0.0, boundary=1)))
+    return c
+
+
 def main():
     ref = Reference()
-    cases = {"mass": [], "advection": [], "cg": [], "gmres": []}
+    cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": []}
     arrays = {}
     for seed in (0, 1, 2, 3, 12345):
         arrays[f"rng_seed{seed}"] = ref.fill_random(256, seed)
@@ -128,6 +142,15 @@ def main():
         for mode in (0, 1, 2):
             arrays[f"{cid}_mode{mode}_y"] = ref.advection_apply(case, x, mode)
         cases["advection"].append({"id": cid, **case})
+    for cid, case in sipdg_cases():
+        ne = int(np.prod(case["sizes"]))
+        mu = np.exp(np.random.default_rng(4).normal(0.0, 0.5, ne))
+        kappa = 10.0 * (case["P"] + 1) ** 2
+        case = dict(case, seed=5, kappa=kappa)
+        x = ref.fill_random(num_dofs(case), case["seed"])
+        arrays[f"{cid}_mu"] = mu
+        arrays[f"{cid}_y"] = ref.sipdg_apply(case, mu, case["sigma"], kappa, case["boundary"], x)
+        cases["sipdg"].append({"id": cid, **case})
     # CG on the mass operator: b = M u (u from seed 0), x0 = 0 (conjugategradient.hpp:125)
     for cid, case, iters, tol in (("cg1", dict(cube(3, 4, 3, 4), sigma_kind=0, sigma_c=1.0), 20, 1e-6),
                                   ("cg2", dict(cube(3, 4, 3, 4), sigma_kind=1), 500, 1e-12),
