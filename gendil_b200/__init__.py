@@ -306,6 +306,8 @@ class SIPDGOperator(_Operator):
         super().__init__(space, q)
         if kappa is None:
             kappa = 10.0 * (space.order + 1) ** 2
+        if str(mu.dtype) != "torch.float64" or not mu.is_cuda or not mu.is_contiguous() or mu.numel() != space.num_elements:
+            raise ValueError("mu: one FP64 value per element, a contiguous CUDA tensor")
         self.mu = mu
         h = ctypes.c_void_p()
         check(lib().dgop_sipdg_create(space.handle, q, _ptr(mu), float(sigma), float(kappa), 1 if boundary else 0,
