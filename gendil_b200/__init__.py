@@ -99,6 +99,7 @@ def lib():
         L.dgop_sipdg_create.argtypes = [vp, i, vp, ctypes.c_double, ctypes.c_double, i, ctypes.POINTER(vp)]
         L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
         L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.dgop_sipdg_gradient.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_batch_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
         L.dgop_batch_groups.argtypes = [vp]
@@ -313,6 +314,16 @@ class SIPDGOperator(_Operator):
         check(lib().dgop_sipdg_create(space.handle, q, _ptr(mu), float(sigma), float(kappa), 1 if boundary else 0,
                                       ctypes.byref(h)))
         self.handle = h
+
+    def coefficient_gradient(self, u, lam, scale=None, out=None, stream=None):
+        """out[e] = scale[e] * lam^T (dA/dmu_e) u (one kernel; FP64 device tensors).  With lam the
+        adjoint state (A^T lam = dJ/du) of A u = f, dJ/dmu_e = -out[e]."""
+        import torch
+        if out is None:
+            out = torch.empty(self.space.num_elements, dtype=torch.float64, device=u.device)
+        check(lib().dgop_sipdg_gradient(self.handle, _ptr(u), _ptr(lam), None if scale is None else _ptr(scale),
+                                        _ptr(out), _stream(stream)))
+        return out
 
 
 class MassInverseOperator(_Operator):

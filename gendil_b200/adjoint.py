@@ -126,3 +126,79 @@ class _SolveFunction(torch.autograd.Function):
 def solve(system, theta, b, rho=None):
     """u = S(theta, rho)^{-1} b, differentiable in theta, rho and b (torch.autograd)."""
     return _SolveFunction.apply(theta, rho, b, system)
+
+
+class DiffusionSystem:
+    """A(mu) u = f for the symmetric interior-penalty DG diffusion operator (SIPG, sigma = -1) with
+    one diffusivity mu_e per element; FP64 CG (A is symmetric positive definite for kappa large
+    enough).  With J(u) and lambda = A^{-1} dJ/du (A^T = A),
+
+        dJ/dmu_e = -lambda^T (dA/dmu_e) u     (dgop_sipdg_gradient, one kernel)
+        dJ/df    =  lambda
+
+    and dJ/dz_e = mu_e dJ/dmu_e for mu = exp(z) follows by the chain rule (torch.autograd).
+    No reference counterpart; the checks are central finite differences and the reference
+    operator's one-hot derivative (tests/test_sipdg_gpu.py)."""
+
+    def __init__(self, space, q, kappa=None, boundary=True, tol=1e-12, max_iters=50000):
+        self.space, self.q = space, q
+        self.kappa = 10.0 * (space.order + 1) ** 2 if kappa is None else kappa
+        self.boundary = boundary
+        self.tol, self.max_iters = tol, max_iters
+        self.last_info = None
+
+    def operator(self, mu):
+        return g.SIPDGOperator(self.space, self.q, mu.detach().contiguous(), sigma=-1.0, kappa=self.kappa,
+                               boundary=self.boundary)
+
+    def _solve(self, op, rhs):
+        x = torch.zeros_like(rhs)
+        solver = g.CGSolver(op)
+        info = solver.solve(rhs, x, self.max_iters, self.tol)
+        solver.close()
+        if not info["success"]:
+            raise RuntimeError(f"CG did not converge: {info}")
+        self.last_info = info
+        return x
+
+    def solve(self, mu, f):
+        """u = A(mu)^{-1} f."""
+        op = self.operator(mu)
+        u = self._solve(op, f)
+        op.close()
+        return u
+
+    def adjoint(self, mu, grad_u):
+        """lambda = A(mu)^{-T} grad_u (= A(mu)^{-1} grad_u: the form is symmetric)."""
+        return self.solve(mu, grad_u)
+
+    def grad_mu(self, mu, u, lam):
+        """dJ/dmu_e = -lambda^T (dA/dmu_e) u."""
+        op = self.operator(mu)
+        out = op.coefficient_gradient(u, lam)
+        op.close()
+        return -out
+
+
+class _DiffusionSolveFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, mu, f, system):
+        mu = mu.detach().contiguous()
+        u = system.solve(mu, f.detach().contiguous())
+        ctx.system = system
+        ctx.save_for_backward(mu, u)
+        return u
+
+    @staticmethod
+    def backward(ctx, grad_u):
+        system = ctx.system
+        mu, u = ctx.saved_tensors
+        lam = system.adjoint(mu, grad_u.contiguous())
+        g_mu = system.grad_mu(mu, u, lam) if ctx.needs_input_grad[0] else None
+        g_f = lam if ctx.needs_input_grad[1] else None
+        return g_mu, g_f, None
+
+
+def solve_diffusion(system, mu, f):
+    """u = A(mu)^{-1} f, differentiable in mu and f (torch.autograd)."""
+    return _DiffusionSolveFunction.apply(mu, f, system)

@@ -77,6 +77,11 @@ struct KronDiffCfg {
   size_t smem = 0;
   Real* d_mats = nullptr;
   Real* d_mu = nullptr;  // FP32 copy of the per-element diffusivity
+  // coefficient-gradient kernel launch (FP64)
+  bool grad_ready = false;
+  int grad_eb = 0;
+  dim3 grad_grid;
+  size_t grad_smem = 0;
 };
 
 void set_error(const std::string& msg);

@@ -1,6 +1,7 @@
 // Instantiation unit of the any-dimension Kronecker kernel, compiled once per dimension with
 // -DDGOP_GEN_D=<dim>: every N = 1..8 whose element (U, W, Y, matrices) fits in shared memory.
 #include "kron_registry.h"
+#include "kronnd_diff_grad_kernel.cuh"
 #include "kronnd_diff_kernel.cuh"
 #include "kronnd_kernel.cuh"
 
@@ -30,6 +31,11 @@ void launch_kronnd_diff(const KronDiffParams<Real>& p, dim3 grid, dim3 block, si
   kronnd_diff_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
 }
 
+template <int D, int N, typename Real>
+void launch_kronnd_grad(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_diff_grad_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
+}
+
 // one element must fit in 200 KB of shared memory
 template <int D, int N, typename Real>
 constexpr bool fits() {
@@ -49,6 +55,14 @@ void fill(KronNDEntry<Real>& d) {
     d.launch_diff = &launch_kronnd_diff<D, N, Real>;
     d.func_diff = reinterpret_cast<const void*>(&kronnd_diff_kernel<D, N, Real>);
     d.per_elem_diff = KronDiffShape<D, N>::PER_ELEM;
+  }
+  if constexpr (sizeof(Real) == 8 &&
+                (int64_t)(KronDiffGradShape<D, N>::PER_ELEM + KronDiffGradShape<D, N>::HDR) * (int64_t)sizeof(Real) <=
+                    200 * 1024) {
+    d.launch_grad = &launch_kronnd_grad<D, N, Real>;
+    d.func_grad = reinterpret_cast<const void*>(&kronnd_diff_grad_kernel<D, N, Real>);
+    d.per_elem_grad = KronDiffGradShape<D, N>::PER_ELEM;
+    d.header_grad = KronDiffGradShape<D, N>::HDR;
   }
 }
 }  // namespace

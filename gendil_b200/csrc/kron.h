@@ -130,8 +130,15 @@ struct KronDiffParams {
   const Real* x;
   Real* y;
   const Real* mu;    // per element (device)
-  const Real* mats;  // D x kDiffMats base matrices, N x N each (device)
+  const Real* mats;  // D x kDiffMats base matrices, N x N each (device), then the trace rows
+                     // l(0), l(1), l'(0), l'(1) (N each)
   const int* skip;
+  // coefficient gradient (kronnd_diff_grad_kernel): gout[e] = gscale[e] lam^T (dA/dmu_e) x
+  const Real* lam;
+  Real* gout;
+  const Real* gscale;
+  Real kappa;
+  Real face_h[kMaxDim];  // detJ / h_a^2
 };
 
 struct KronPlanHost {

@@ -49,6 +49,10 @@ struct KronNDEntry {
   void (*launch_diff)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_diff = nullptr;
   int per_elem_diff = 0;
+  // its coefficient gradient (kronnd_diff_grad_kernel.cuh)
+  void (*launch_grad)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func_grad = nullptr;
+  int per_elem_grad = 0, header_grad = 0;
 };
 KronNDEntry<double>& kronnd_slot_f64(int D, int N);
 KronNDEntry<float>& kronnd_slot_f32(int D, int N);

@@ -35,7 +35,8 @@ __global__ void to_real(const double* in, Real* out, int64_t n) {
     out[i] = (Real)in[i];
 }
 
-// Base matrices of every axis (see kronnd_diff_kernel.cuh), row-major N x N, axis-major.
+// Base matrices of every axis (see kronnd_diff_kernel.cuh), row-major N x N, axis-major, then
+// the trace rows l(0), l(1), l'(0), l'(1) of the coefficient-gradient kernel.
 bool diff_tables(const dgop_space& s, int q, double kappa, std::vector<double>& mats) {
   const int N = s.n, D = s.D;
   double xq[kMaxQ], wq[kMaxQ], xn[kMaxN], wn[kMaxN];
@@ -54,7 +55,13 @@ bool diff_tables(const dgop_space& s, int q, double kappa, std::vector<double>& 
     }
   double detJ = 1.0;
   for (int k = 0; k < D; ++k) detJ *= s.h[k];
-  mats.assign((size_t)D * kDiffMats * N * N, 0.0);
+  mats.assign((size_t)D * kDiffMats * N * N + 4 * N, 0.0);
+  double* tv = mats.data() + (size_t)D * kDiffMats * N * N;
+  for (int j = 0; j < N; ++j)
+    for (int side = 0; side < 2; ++side) {
+      tv[side * N + j] = b[side][j];
+      tv[(2 + side) * N + j] = d[side][j];
+    }
   for (int a = 0; a < D; ++a) {
     const double h = s.h[a], fm = detJ / h;  // face measure
     auto M = [&](int k) { return mats.data() + ((size_t)a * kDiffMats + k) * N * N; };
@@ -82,9 +89,41 @@ bool diff_tables(const dgop_space& s, int q, double kappa, std::vector<double>& 
   return true;
 }
 
+// Launch shape of the coefficient-gradient kernel (FP64); leaves grad_ready false when the element
+// does not fit.
+int setup_grad(dgop_operator* op, KronDiffCfg<double>& K) {
+  const dgop_space& s = op->sp;
+  const KronNDEntry<double>* entry = K.entry;
+  if (!entry->launch_grad) return DGOP_OK;
+  const size_t per = (size_t)entry->per_elem_grad * sizeof(double);
+  const size_t hdr = (size_t)entry->header_grad * sizeof(double);
+  int eb = 1;
+  while (eb < 64 && hdr + per * (eb * 2) <= 96 * 1024) eb *= 2;
+  const int64_t lines = (int64_t)(s.ndofs / s.nelem) / s.n;
+  while (eb > 1 && (int64_t)(eb / 2) * lines >= kKronNDThreads) eb /= 2;
+  int max_smem = 0;
+  DGOP_CUDA_D(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+  cudaFuncAttributes fa{};
+  DGOP_CUDA_D(cudaFuncGetAttributes(&fa, entry->func_grad));
+  max_smem -= (int)fa.sharedSizeBytes;
+  while (eb > 1 && hdr + per * eb > (size_t)max_smem) eb /= 2;
+  if (hdr + per * eb > (size_t)max_smem) return DGOP_OK;
+  K.grad_eb = eb;
+  K.grad_smem = hdr + per * eb;
+  DGOP_CUDA_D(cudaFuncSetAttribute(entry->func_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  int per_sm = 0;
+  DGOP_CUDA_D(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, entry->func_grad, kKronNDThreads, K.grad_smem));
+  if (per_sm < 1) return DGOP_OK;
+  const int64_t ctas = std::min<int64_t>((s.nelem + eb - 1) / eb, (int64_t)device_sms(op->device) * per_sm);
+  K.grad_grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+  K.grad_ready = true;
+  return DGOP_OK;
+}
+
 template <typename Real>
 int setup_diff(dgop_operator* op, KronDiffCfg<Real>& K, const std::vector<double>& mats, const double* mu,
-               double sigma, int boundary) {
+               double sigma, double kappa, int boundary) {
   const dgop_space& s = op->sp;
   const KronNDEntry<Real>* entry = nullptr;
   if constexpr (sizeof(Real) == 8) entry = &kronnd_slot_f64(s.D, s.n);
@@ -106,6 +145,10 @@ int setup_diff(dgop_operator* op, KronDiffCfg<Real>& K, const std::vector<double
   }
   p.boundary = boundary;
   p.sigma = (Real)sigma;
+  p.kappa = (Real)kappa;
+  double detJ = 1.0;
+  for (int k = 0; k < s.D; ++k) detJ *= s.h[k];
+  for (int k = 0; k < s.D; ++k) p.face_h[k] = (Real)(detJ / (s.h[k] * s.h[k]));
   std::vector<Real> mr(mats.begin(), mats.end());
   Real* dm = nullptr;
   DGOP_CUDA_D(cudaMalloc(&dm, sizeof(Real) * mr.size()));
@@ -149,6 +192,7 @@ int setup_diff(dgop_operator* op, KronDiffCfg<Real>& K, const std::vector<double
   const int64_t ctas = std::min<int64_t>((s.nelem + eb - 1) / eb, (int64_t)device_sms(op->device) * per_sm);
   K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
   K.ready = true;
+  if constexpr (sizeof(Real) == 8) return setup_grad(op, K);
   return DGOP_OK;
 }
 
@@ -187,8 +231,8 @@ extern "C" int dgop_sipdg_create(const dgop_space* space, int q, const double* m
     set_error("basis tables");
     return DGOP_ERR_ARG;
   }
-  int rc = setup_diff<double>(op, op->s64, mats, mu, sigma, boundary);
-  if (rc == DGOP_OK && setup_diff<float>(op, op->s32, mats, mu, sigma, boundary) != DGOP_OK) {
+  int rc = setup_diff<double>(op, op->s64, mats, mu, sigma, kappa, boundary);
+  if (rc == DGOP_OK && setup_diff<float>(op, op->s32, mats, mu, sigma, kappa, boundary) != DGOP_OK) {
     free_diff(op->s32);
     set_error("");
   }
@@ -198,5 +242,34 @@ extern "C" int dgop_sipdg_create(const dgop_space* space, int q, const double* m
     return rc;
   }
   *out = op;
+  return DGOP_OK;
+}
+
+extern "C" int dgop_sipdg_gradient(const dgop_operator* op, const double* u, const double* lambda,
+                                   const double* scale, double* out, void* stream) {
+  if (!op || !u || !lambda || !out) {
+    set_error("dgop_sipdg_gradient: null argument");
+    return DGOP_ERR_ARG;
+  }
+  if (op->kernel != DGOP_KERNEL_DIFF) {
+    set_error("dgop_sipdg_gradient: not an interior-penalty diffusion operator");
+    return DGOP_ERR_ARG;
+  }
+  const KronDiffCfg<double>& K = op->s64;
+  if (!K.grad_ready) {
+    set_error("no coefficient-gradient kernel for this (dimension, order): the element exceeds shared memory");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  KronDiffParams<double> p = K.params;
+  p.x = u;
+  p.lam = lambda;
+  p.gout = out;
+  p.gscale = scale;
+  p.eb = K.grad_eb;
+  p.e_begin = 0;
+  p.skip = nullptr;
+  K.entry->launch_grad(p, K.grad_grid, K.block, K.grad_smem, (cudaStream_t)stream);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "coefficient-gradient kernel launch");
   return DGOP_OK;
 }

@@ -91,6 +91,12 @@ int dgop_mass_inverse_create(const dgop_space* space, int q, const dgop_coef* si
  *                  fit in shared memory (kernel DGOP_KERNEL_DIFF). */
 int dgop_sipdg_create(const dgop_space* space, int q, const double* mu, double sigma, double kappa, int boundary,
                       dgop_operator** out);
+/* sipdg_gradient:  out[e] = scale[e] * lambda^T (dA/dmu_e) u for an operator of dgop_sipdg_create
+ *                  (scale NULL: 1; FP64 device vectors, out one value per element).  With lambda the
+ *                  adjoint state of A(mu) u = f (A^T lambda = dJ/du) the gradient of J is
+ *                  dJ/dmu_e = -out[e].  One launch, deterministic.  No reference counterpart. */
+int dgop_sipdg_gradient(const dgop_operator* op, const double* u, const double* lambda, const double* scale,
+                        double* out, void* stream);
 int dgop_operator_destroy(dgop_operator* op);
 int64_t dgop_operator_num_dofs(const dgop_operator* op);
 

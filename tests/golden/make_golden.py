@@ -120,10 +120,42 @@ def sipdg_cases():
     return c
 
 
-def main():
+def main(only=None):
+    """Write cases.json and golden.npz.  With `only` (a case kind), regenerate that kind alone and
+    keep every other stored case and array as it is (the OpenMP reference solvers' last bits
+    depend on the thread schedule, so regenerating them all would churn the fixtures)."""
+    if only is not None:
+        with open(os.path.join(HERE, "cases.json")) as f:
+            old_cases = json.load(f)
+        with np.load(os.path.join(HERE, "golden.npz")) as z:
+            old_arrays = {k: z[k] for k in z.files}
+        new_cases, new_arrays = build(only)
+        ids = {c["id"] for c in new_cases[only]}
+        old_cases[only] = new_cases[only]
+        for k in list(old_arrays):
+            if k.split("_")[0] in ids:
+                del old_arrays[k]
+        old_arrays.update(new_arrays)
+        write(old_cases, old_arrays)
+        return
+    write(*build(None))
+
+
+def write(cases, arrays):
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(cases, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **arrays)
+    total = sum(a.nbytes for a in arrays.values())
+    print(f"wrote {len(arrays)} arrays ({total / 1e6:.2f} MB raw)")
+
+
+def build(only):
     ref = Reference()
     cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": []}
     arrays = {}
+    if only == "sipdg":
+        sipdg_fixtures(ref, cases, arrays)
+        return cases, arrays
     for seed in (0, 1, 2, 3, 12345):
         arrays[f"rng_seed{seed}"] = ref.fill_random(256, seed)
     for kind in (0, 1):
@@ -142,15 +174,7 @@ def main():
         for mode in (0, 1, 2):
             arrays[f"{cid}_mode{mode}_y"] = ref.advection_apply(case, x, mode)
         cases["advection"].append({"id": cid, **case})
-    for cid, case in sipdg_cases():
-        ne = int(np.prod(case["sizes"]))
-        mu = np.exp(np.random.default_rng(4).normal(0.0, 0.5, ne))
-        kappa = 10.0 * (case["P"] + 1) ** 2
-        case = dict(case, seed=5, kappa=kappa)
-        x = ref.fill_random(num_dofs(case), case["seed"])
-        arrays[f"{cid}_mu"] = mu
-        arrays[f"{cid}_y"] = ref.sipdg_apply(case, mu, case["sigma"], kappa, case["boundary"], x)
-        cases["sipdg"].append({"id": cid, **case})
+    sipdg_fixtures(ref, cases, arrays)
     # CG on the mass operator: b = M u (u from seed 0), x0 = 0 (conjugategradient.hpp:125)
     for cid, case, iters, tol in (("cg1", dict(cube(3, 4, 3, 4), sigma_kind=0, sigma_c=1.0), 20, 1e-6),
                                   ("cg2", dict(cube(3, 4, 3, 4), sigma_kind=1), 500, 1e-12),
@@ -172,12 +196,32 @@ def main():
         x, info = ref.system_gmres(case, b, np.zeros_like(b), 5000, 30, 1e-10)
         arrays[f"{cid}_x"] = x
         cases["gmres"].append({"id": cid, **case, "restart": 30, "tol": 1e-10, "max_iters": 5000, **info})
-    with open(os.path.join(HERE, "cases.json"), "w") as f:
-        json.dump(cases, f, indent=1)
-    np.savez_compressed(os.path.join(HERE, "golden.npz"), **arrays)
-    total = sum(a.nbytes for a in arrays.values())
-    print(f"wrote {len(arrays)} arrays ({total / 1e6:.2f} MB raw)")
+    return cases, arrays
+
+
+def sipdg_fixtures(ref, cases, arrays):
+    for cid, case in sipdg_cases():
+        ne = int(np.prod(case["sizes"]))
+        mu = np.exp(np.random.default_rng(4).normal(0.0, 0.5, ne))
+        kappa = 10.0 * (case["P"] + 1) ** 2
+        case = dict(case, seed=5, kappa=kappa)
+        x = ref.fill_random(num_dofs(case), case["seed"])
+        arrays[f"{cid}_mu"] = mu
+        arrays[f"{cid}_y"] = ref.sipdg_apply(case, mu, case["sigma"], kappa, case["boundary"], x)
+        # coefficient gradient lam^T (dA/dmu_e) x, lam from seed 6: A is linear in mu, so the
+        # derivative is the reference operator with the one-hot diffusivity of element e
+        lam = ref.fill_random(num_dofs(case), 6)
+        grad = np.empty(ne)
+        for e in range(ne):
+            onehot = np.zeros(ne)
+            onehot[e] = 1.0
+            grad[e] = lam @ ref.sipdg_apply(case, onehot, case["sigma"], kappa, case["boundary"], x)
+        arrays[f"{cid}_grad"] = grad
+        cases["sipdg"].append({"id": cid, **case, "grad_seed": 6})
 
 
 if __name__ == "__main__":
-    main()
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=["sipdg"], help="regenerate one case kind, keep the rest")
+    main(ap.parse_args().only)

@@ -63,3 +63,67 @@ def test_sipg_cg_solve():
     op(u, r)
     # the CG convention: |r| / |r0| below 1e-12 (r0 = f for u0 = 0)
     assert (torch.linalg.vector_norm(f - r) / torch.linalg.vector_norm(f)).item() <= 2e-12
+
+
+@pytest.mark.parametrize("case", CASES["sipdg"], ids=lambda c: c["id"])
+def test_coefficient_gradient_vs_reference_golden(case):
+    """lam^T (dA/dmu_e) u against the reference operator's one-hot derivative (A is linear in mu)."""
+    op = _op(case)
+    u = torch.tensor(inputs(case), device="cuda")
+    lam = torch.tensor(inputs(case, seed=case["grad_seed"]), device="cuda")
+    out = op.coefficient_gradient(u, lam)
+    ref = ARR[f"{case['id']}_grad"]
+    assert rel_max(out.cpu().numpy(), ref) <= 1e-12
+    scale = torch.linspace(0.5, 2.0, out.numel(), dtype=torch.float64, device="cuda")
+    out2 = op.coefficient_gradient(u, lam, scale=scale)
+    assert torch.equal(out2, scale * out)
+    again = op.coefficient_gradient(u, lam)
+    assert torch.equal(again, out)  # deterministic
+
+
+def test_coefficient_gradient_matches_directional_derivative():
+    """sum_e dmu_e out_e = lam^T A(dmu) u for a random direction (linearity in mu), 5^3 p = 3."""
+    case = {"D": 3, "P": 3, "Q": 5, "basis": 0, "sizes": [5, 4, 3], "h": [0.2, 0.25, 1 / 3], "origin": [0.0] * 3,
+            "periodic": [0, 1, 0]}
+    sp = make_space(case)
+    rng = np.random.default_rng(9)
+    mu = torch.tensor(np.exp(rng.normal(0, 0.5, sp.num_elements)), device="cuda")
+    dmu = torch.tensor(rng.normal(0, 1, sp.num_elements), device="cuda")
+    u = torch.tensor(rng.uniform(-1, 1, sp.num_dofs), device="cuda")
+    lam = torch.tensor(rng.uniform(-1, 1, sp.num_dofs), device="cuda")
+    op = g.SIPDGOperator(sp, 5, mu, sigma=1.0, kappa=160.0, boundary=True)
+    out = op.coefficient_gradient(u, lam)
+    opd = g.SIPDGOperator(sp, 5, dmu, sigma=1.0, kappa=160.0, boundary=True)
+    w = torch.empty_like(u)
+    opd(u, w)
+    lhs, rhs = float(dmu @ out), float(lam @ w)
+    assert abs(lhs - rhs) <= 1e-12 * float((dmu.abs() * out.abs()).sum())
+
+
+def test_loss_gradient_vs_central_differences():
+    """Configuration 4's gradient at 4^3, p = 4: J = 1/2 |u - u*|^2, A(exp z) u = f, dJ/dz by the
+    adjoint solve and the coefficient-gradient kernel against central differences (eps = 1e-6)
+    on 8 random elements."""
+    from gendil_b200 import adjoint
+    case = {"D": 3, "P": 4, "Q": 6, "basis": 0, "sizes": [4] * 3, "h": [0.25] * 3, "origin": [0.0] * 3,
+            "periodic": [0] * 3}
+    sp = make_space(case)
+    system = adjoint.DiffusionSystem(sp, 6, tol=1e-13)
+    z = torch.tensor(np.random.default_rng(4).normal(0.0, 0.5, sp.num_elements), device="cuda", requires_grad=True)
+    f = torch.tensor(oracle().fill_random(sp.num_dofs, 5), device="cuda")
+    ustar = torch.tensor(oracle().fill_random(sp.num_dofs, 6), device="cuda")
+
+    def loss(zv):
+        u = adjoint.solve_diffusion(system, torch.exp(zv), f)
+        return 0.5 * torch.sum((u - ustar) ** 2)
+
+    J = loss(z)
+    J.backward()
+    grad = z.grad.clone()
+    eps = 1e-6
+    for e in np.random.default_rng(8).choice(sp.num_elements, 8, replace=False):
+        zp, zm = z.detach().clone(), z.detach().clone()
+        zp[e] += eps
+        zm[e] -= eps
+        fd = (loss(zp).item() - loss(zm).item()) / (2 * eps)
+        assert abs(fd - grad[e].item()) <= 1e-5 * max(1.0, abs(grad).max().item()), (e, fd, grad[e].item())
