@@ -611,7 +611,10 @@ def run_sipdg(args):
     alg = 16.0 * nd + 8.0 * ne
     achieved = alg / (ms_step * 1e-3) / 1e9
     D, N = 3, p + 1
-    flop = 2 * N * D * (D + 2)  # D own-line passes, 2D neighbour-line passes, D(D-1) tangential mass passes
+    # per DoF: the D axis passes (Khat_a, N FMA, plus the rank-one face terms: own and neighbour
+    # value / derivative traces and the four-term update, 12 FMA) and D(D-1) tangential mass
+    # passes (N FMA each); 2 flop per FMA
+    flop = 2 * (D * (N + 12) + D * (D - 1) * N)
     peak64 = fp64_gemm_peak(torch, dev)
     a64 = flop * nd / (ms_step * 1e-3) / 1e12
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": 1, "steps": args.steps,

@@ -51,10 +51,12 @@ void fill(KronNDEntry<Real>& d) {
     d.func_batch = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, Real>);
     d.per_elem = KronNDShape<D, N>::PER_ELEM;
   }
-  if constexpr ((int64_t)KronDiffShape<D, N>::PER_ELEM * (int64_t)sizeof(Real) <= 200 * 1024) {
+  if constexpr ((int64_t)(KronDiffShape<D, N>::PER_ELEM + KronDiffShape<D, N>::HDR) * (int64_t)sizeof(Real) <=
+                200 * 1024) {
     d.launch_diff = &launch_kronnd_diff<D, N, Real>;
     d.func_diff = reinterpret_cast<const void*>(&kronnd_diff_kernel<D, N, Real>);
     d.per_elem_diff = KronDiffShape<D, N>::PER_ELEM;
+    d.header_diff = KronDiffShape<D, N>::HDR;
   }
   if constexpr (sizeof(Real) == 8 &&
                 (int64_t)(KronDiffGradShape<D, N>::PER_ELEM + KronDiffGradShape<D, N>::HDR) * (int64_t)sizeof(Real) <=

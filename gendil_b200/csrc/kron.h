@@ -117,6 +117,8 @@ enum DiffMat : int {
   kDiffMats = 14
 };
 
+constexpr int kDiffMaxEB = 64;  // elements per CTA of the diffusion kernels, at most
+
 template <typename Real>
 struct KronDiffParams {
   int64_t nelem, e_begin;

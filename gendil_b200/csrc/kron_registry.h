@@ -48,7 +48,7 @@ struct KronNDEntry {
   // interior-penalty diffusion (kronnd_diff_kernel.cuh)
   void (*launch_diff)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_diff = nullptr;
-  int per_elem_diff = 0;
+  int per_elem_diff = 0, header_diff = 0;
   // its coefficient gradient (kronnd_diff_grad_kernel.cuh)
   void (*launch_grad)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_grad = nullptr;

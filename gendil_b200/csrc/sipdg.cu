@@ -163,25 +163,37 @@ int setup_diff(dgop_operator* op, KronDiffCfg<Real>& K, const std::vector<double
     DGOP_CUDA_D(cudaGetLastError());
     p.mu = K.d_mu;
   }
-  // elements per CTA: the any-dimension kernel's rule (power of two, ~96 KB, enough lines)
+  // elements per CTA: as many as fit in ~72 KB (three CTAs per SM), then, among the counts down
+  // to half of that, the one whose lines fill the CTA's passes best (every pass runs over the
+  // lines of all the CTA's elements, kKronNDThreads at a time)
   const size_t per = (size_t)entry->per_elem_diff * sizeof(Real);
-  int eb = 1;
-  while (eb < 64 && per * (eb * 2) <= 96 * 1024) eb *= 2;
-  const int64_t lines = (int64_t)(s.ndofs / s.nelem) / s.n;
-  while (eb > 1 && (int64_t)(eb / 2) * lines >= kKronNDThreads) eb /= 2;
+  const size_t hdr = (size_t)entry->header_diff * sizeof(Real);
   int max_smem = 0;
   DGOP_CUDA_D(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
   cudaFuncAttributes fa{};
   DGOP_CUDA_D(cudaFuncGetAttributes(&fa, entry->func_diff));
   max_smem -= (int)fa.sharedSizeBytes;
-  while (eb > 1 && per * eb > (size_t)max_smem) eb /= 2;
-  if (per * eb > (size_t)max_smem) {
+  const size_t budget = std::min<size_t>((size_t)max_smem, 72 * 1024);
+  int ebmax = (int)std::min<int64_t>(kDiffMaxEB, budget > hdr ? (int64_t)((budget - hdr) / per) : 0);
+  if (ebmax < 1 && hdr + per <= (size_t)max_smem) ebmax = 1;
+  if (ebmax < 1) {
     set_error("element does not fit in shared memory");
     return DGOP_ERR_UNSUPPORTED;
   }
+  const int64_t lines = (int64_t)(s.ndofs / s.nelem) / s.n;
+  int eb = ebmax;
+  double best = -1.0;
+  for (int c = ebmax; c >= std::max(1, ebmax / 2); --c) {
+    const int64_t l = c * lines;
+    const double use = (double)l / (double)(((l + kKronNDThreads - 1) / kKronNDThreads) * kKronNDThreads);
+    if (use > best + 1e-9) {
+      best = use;
+      eb = c;
+    }
+  }
   p.eb = eb;
   K.block = dim3(kKronNDThreads);
-  K.smem = per * eb;
+  K.smem = hdr + per * eb;
   DGOP_CUDA_D(cudaFuncSetAttribute(entry->func_diff, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   int per_sm = 0;
   DGOP_CUDA_D(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, entry->func_diff, kKronNDThreads, K.smem));
