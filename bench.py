@@ -264,7 +264,7 @@ def run_ours(args):
     else:
         space = g.Space(3, [args.size] * 3, order=ORDER)
         op = g.AdvectionOperator(space, NQ, C.velocity_sincos(3), bc=g.BC_INFLOW, g=0.0)
-    if args.variant and op.kernel == "kron":
+    if args.variant and op.kernel in ("kron", "kronnd"):
         op.set_variant(args.variant)  # a fixed kernel for profiling; the autotuner's pick otherwise
     nd = space.num_dofs
     x_np = g.fill_random(nd, 1)

@@ -254,27 +254,31 @@ class _Operator:
     def select_kernel(self, name):
         check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1, "kronnd": 2}[name]))
 
-    VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl")
+    VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl")  # 3D register kernel ("kron")
+    ND_VARIANTS = ("nd-passes", "nd-grouped2", "nd-grouped3")  # any-dimension kernel ("kronnd")
+
+    def _variants(self):
+        return self.ND_VARIANTS if self.kernel == "kronnd" else self.VARIANTS
 
     @property
     def variant(self):
         """Kronecker-kernel variant picked by the autotuner (None without a Kronecker kernel)."""
         v = lib().dgop_operator_variant(self.handle)
-        return None if v < 0 else self.VARIANTS[v]
+        return None if v < 0 else self._variants()[v]
 
     def set_variant(self, name):
         """Force a Kronecker-kernel variant by name, or None to re-run the autotuner."""
-        check(lib().dgop_operator_set_variant(self.handle, -1 if name is None else self.VARIANTS.index(name)))
+        check(lib().dgop_operator_set_variant(self.handle, -1 if name is None else self._variants().index(name)))
 
     def variant_times(self):
-        """Autotuner time per launch (ms) of every variant (0.0: not available or not timed)."""
+        """Autotuner time per launch (ms) of every variant (0.0: not available or not timed; the
+        any-dimension kernel's variants are timed on the first 16,384 elements)."""
         out = {}
-        for k, name in enumerate(self.VARIANTS):
+        for k, name in enumerate(self._variants()):
             ms = ctypes.c_float()
             check(lib().dgop_operator_variant_time(self.handle, k, ctypes.byref(ms)))
             out[name] = ms.value
         return out
-        return self
 
     def close(self):
         if self.handle:

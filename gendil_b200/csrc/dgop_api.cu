@@ -568,7 +568,99 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
   }
   const int64_t ctas = std::min<int64_t>((s.nelem + eb - 1) / eb, (int64_t)device_sm_count(op->device) * per_sm);
   K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+  K.var[0] = {true, eb, K.grid, K.smem, 0.0f};
+  // grouped variants: elements per CTA so that the blocks of the largest group give every
+  // thread about one block, within ~110 KB of shared memory (two CTAs per SM)
+  for (int v = 1; v < kKronNDVariants; ++v) {
+    const int G = v + 1;
+    if (!entry->launch_g[v - 1]) continue;
+    int64_t gsz = 1;
+    for (int k = 0; k < std::min(G, D); ++k) gsz *= N;
+    const int64_t ipe = (s.ndofs / s.nelem) / gsz;  // blocks per element
+    int ebv = (int)std::max<int64_t>(1, std::min<int64_t>(64, (kKronNDThreads + ipe / 2) / ipe));
+    while (ebv > 1 && per * ebv > std::min<size_t>((size_t)max_smem, 110 * 1024)) --ebv;
+    if (per * ebv > (size_t)max_smem) continue;
+    cudaFuncAttributes fv{};
+    if (cudaFuncGetAttributes(&fv, entry->func_g[v - 1]) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    int max_v = 0;
+    DGOP_CUDA(cudaDeviceGetAttribute(&max_v, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
+    max_v -= (int)fv.sharedSizeBytes;
+    if (per * ebv > (size_t)max_v) continue;
+    DGOP_CUDA(cudaFuncSetAttribute(entry->func_g[v - 1], cudaFuncAttributeMaxDynamicSharedMemorySize, max_v));
+    int per_sm_v = 0;
+    DGOP_CUDA(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, entry->func_g[v - 1], kKronNDThreads, per * ebv));
+    if (per_sm_v < 1) continue;
+    const int64_t cv = std::min<int64_t>((s.nelem + ebv - 1) / ebv, (int64_t)device_sm_count(op->device) * per_sm_v);
+    K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), per * ebv, 0.0f};
+  }
+  K.variant = 0;
   K.ready = true;
+  return DGOP_OK;
+}
+
+// Launch of the any-dimension kernel's variant v with parameters p (p.eb set here).
+template <typename Real>
+void launch_kronnd_variant(const KronNDCfg<Real>& K, int v, KronNDParams<Real> p, cudaStream_t st) {
+  const auto& L = K.var[v];
+  p.eb = L.eb;
+  if (v == 0) K.entry->launch(p, L.grid, K.block, L.smem, st);
+  else K.entry->launch_g[v - 1](p, L.grid, K.block, L.smem, st);
+}
+
+// Time every usable variant on scratch vectors over the first elements (at most kTuneElems, so
+// that the cost stays bounded on large meshes) and keep the fastest.
+constexpr int64_t kTuneElems = 16384;
+template <typename Real>
+int autotune_kronnd(dgop_operator* op, KronNDCfg<Real>& K) {
+  int usable = 0;
+  for (const auto& L : K.var) usable += L.ok ? 1 : 0;
+  if (!K.ready || usable < 2) return DGOP_OK;
+  const int64_t n = op->sp.ndofs;
+  Real* x = nullptr;
+  Real* y = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int best = K.variant;
+  float best_ms = 0.0f;
+  bool ok = cudaMalloc(&x, sizeof(Real) * n) == cudaSuccess && cudaMalloc(&y, sizeof(Real) * n) == cudaSuccess &&
+            cudaMemset(x, 0, sizeof(Real) * n) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+            cudaEventCreate(&e1) == cudaSuccess;
+  for (int v = 0; ok && v < kKronNDVariants; ++v) {
+    auto& L = K.var[v];
+    if (!L.ok) continue;
+    KronNDParams<Real> p = K.params;
+    p.x = x;
+    p.y = y;
+    p.alpha = Real(1);
+    p.beta_y = Real(0);
+    p.skip = nullptr;
+    p.e_begin = 0;
+    p.nelem = std::min<int64_t>(op->sp.nelem, kTuneElems);
+    launch_kronnd_variant(K, v, p, 0);
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < 3; ++r) launch_kronnd_variant(K, v, p, 0);
+    cudaEventRecord(e1, 0);
+    ok = cudaEventSynchronize(e1) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    float ms = 0.0f;
+    if (ok) cudaEventElapsedTime(&ms, e0, e1);
+    L.ms = ms / 3.0f;
+    if (ok && (best_ms == 0.0f || L.ms < best_ms)) {
+      best_ms = L.ms;
+      best = v;
+    }
+  }
+  if (x) cudaFree(x);
+  if (y) cudaFree(y);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!ok) {
+    cudaGetLastError();
+    return DGOP_OK;  // keep the default variant
+  }
+  K.variant = best;
   return DGOP_OK;
 }
 
@@ -718,6 +810,10 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
       op->kron_why = plan.why;
     }
   }
+  if (op->kernel == DGOP_KERNEL_KRONND) {
+    autotune_kronnd(op, op->n64);
+    autotune_kronnd(op, op->n32);
+  }
   if (!op->f64.ready && !op->k64.ready && !op->n64.ready) {
     free_launch(op->f32);
     free_kron(op->k32);
@@ -792,7 +888,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.e_begin = e_begin;
     p.nelem = e_end;
     if (linear) p.g = Real(0);
-    KN.entry->launch(p, KN.grid, KN.block, KN.smem, s);
+    launch_kronnd_variant(KN, KN.variant, p, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
     return DGOP_OK;
@@ -1019,17 +1115,42 @@ int dgop_operator_select_kernel(dgop_operator* op, int kernel) {
   return DGOP_OK;
 }
 
+static bool uses_kronnd(const dgop_operator* op) { return op->kernel == DGOP_KERNEL_KRONND && op->n64.ready; }
+
 int dgop_operator_variant(const dgop_operator* op) {
-  if (!op || !op->k64.ready) return -1;
+  if (!op) return -1;
+  if (uses_kronnd(op)) return op->n64.variant;
+  if (!op->k64.ready) return -1;
   return op->k64.variant;
 }
 
 const char* dgop_operator_variant_name(const dgop_operator* op) {
   const int v = dgop_operator_variant(op);
-  return v < 0 ? "" : kKronVariantNames[v];
+  if (v < 0) return "";
+  return uses_kronnd(op) ? kKronNDVariantNames[v] : kKronVariantNames[v];
 }
 
 int dgop_operator_set_variant(dgop_operator* op, int variant) {
+  if (op && uses_kronnd(op)) {
+    if (variant < -1 || variant >= kKronNDVariants) {
+      set_error("dgop_operator_set_variant: bad arguments");
+      return DGOP_ERR_ARG;
+    }
+    if (variant == -1) {
+      autotune_kronnd(op, op->n64);
+      autotune_kronnd(op, op->n32);
+    } else {
+      if (!op->n64.var[variant].ok) {
+        set_error(std::string("kernel variant ") + kKronNDVariantNames[variant] +
+                  " is not available for this operator");
+        return DGOP_ERR_UNSUPPORTED;
+      }
+      op->n64.variant = variant;
+      if (op->n32.ready && op->n32.var[variant].ok) op->n32.variant = variant;
+    }
+    ++op->version;
+    return DGOP_OK;
+  }
   if (!op || variant < -1 || variant >= kKronVariants) {
     set_error("dgop_operator_set_variant: bad arguments");
     return DGOP_ERR_ARG;
@@ -1054,6 +1175,10 @@ int dgop_operator_set_variant(dgop_operator* op, int variant) {
 }
 
 int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms) {
+  if (op && ms && uses_kronnd(op) && variant >= 0 && variant < kKronNDVariants) {
+    *ms = op->n64.var[variant].ms;
+    return DGOP_OK;
+  }
   if (!op || !ms || variant < 0 || variant >= kKronVariants || !op->k64.ready) {
     set_error("dgop_operator_variant_time: bad arguments");
     return DGOP_ERR_ARG;

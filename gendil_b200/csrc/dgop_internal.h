@@ -66,6 +66,15 @@ struct KronNDCfg {
   Real* d_phi = nullptr;
   signed char* d_sgn = nullptr;
   Real* d_elem[kMaxDim + 1] = {};  // converted per-element factors (FP32 only)
+  // launch shapes of the variants (kKronNDVariants; 0 = grid / smem / params.eb above)
+  struct Variant {
+    bool ok = false;
+    int eb = 0;
+    dim3 grid;
+    size_t smem = 0;
+    float ms = 0.0f;  // autotuner's time per launch (0: not timed)
+  } var[kKronNDVariants];
+  int variant = 0;
 };
 
 template <typename Real>

@@ -45,6 +45,9 @@ struct KronNDEntry {
                        dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_batch = nullptr;
   int per_elem = 0;  // Real values of shared memory per element
+  // grouped variants (kronnd_grouped_kernel), groups of 2 and 3 axes: same parameters and layout
+  void (*launch_g[2])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
+  const void* func_g[2] = {};
   // interior-penalty diffusion (kronnd_diff_kernel.cuh)
   void (*launch_diff)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_diff = nullptr;
@@ -54,6 +57,10 @@ struct KronNDEntry {
   const void* func_grad = nullptr;
   int per_elem_grad = 0, header_grad = 0;
 };
+// Variants of the any-dimension kernel (the autotuner picks one per operator):
+//   0: one shared-memory pass per axis; 1, 2: groups of 2 or 3 axes per pass in registers
+constexpr int kKronNDVariants = 3;
+extern const char* const kKronNDVariantNames[kKronNDVariants];
 KronNDEntry<double>& kronnd_slot_f64(int D, int N);
 KronNDEntry<float>& kronnd_slot_f32(int D, int N);
 void register_kronnd_d1();

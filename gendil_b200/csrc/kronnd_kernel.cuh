@@ -188,12 +188,11 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
   }
 }
 
-// One batch of ne elements starting at e0 (the CTA's shared memory holds them); x / y are the
-// instance's vectors.
+// Shared-memory setup of one batch of ne elements starting at e0: U (the input), Y = 0, the
+// element coordinates, every element's slot matrices and face records.
 template <int D, int N, typename Real>
-__device__ __forceinline__ void kronnd_block(const KronNDParams<Real>& P, const Real* __restrict__ xin,
-                                             Real* __restrict__ yout, int64_t e0, int ne, int EB, Real* base,
-                                             Real* escale, int (*ecoord)[kMaxDim]) {
+__device__ __forceinline__ void nd_setup(const KronNDParams<Real>& P, const Real* __restrict__ xin, int64_t e0, int ne,
+                                         Real* base, int (*ecoord)[kMaxDim]) {
   using S = KronNDShape<D, N>;
   const bool adv = P.has_adv != 0;
   __syncthreads();
@@ -234,6 +233,30 @@ __device__ __forceinline__ void kronnd_block(const KronNDParams<Real>& P, const 
     reinterpret_cast<uint32_t*>(rec + 4 * D)[1] = fl[1];
   }
   __syncthreads();
+}
+
+// y = alpha Y + beta_y y for the batch.
+template <int D, int N, typename Real>
+__device__ __forceinline__ void nd_output(const KronNDParams<Real>& P, Real* __restrict__ yout, int64_t e0, int ne,
+                                          const Real* base) {
+  using S = KronNDShape<D, N>;
+  for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+    const int b = l / S::ND, i = l - b * S::ND;
+    const Real v = base[(size_t)b * S::PER_ELEM + 2 * S::ND + i];
+    Real* dst = yout + e0 * S::ND + l;
+    *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
+  }
+}
+
+// One batch of ne elements starting at e0 (the CTA's shared memory holds them); x / y are the
+// instance's vectors.
+template <int D, int N, typename Real>
+__device__ __forceinline__ void kronnd_block(const KronNDParams<Real>& P, const Real* __restrict__ xin,
+                                             Real* __restrict__ yout, int64_t e0, int ne, int EB, Real* base,
+                                             Real* escale, int (*ecoord)[kMaxDim]) {
+  using S = KronNDShape<D, N>;
+  const bool adv = P.has_adv != 0;
+  nd_setup<D, N>(P, xin, e0, ne, base, ecoord);
   if (adv) {
     static_for<0, D>([&](auto ac) {
       constexpr int a = decltype(ac)::value;
@@ -287,13 +310,7 @@ __device__ __forceinline__ void kronnd_block(const KronNDParams<Real>& P, const 
       __syncthreads();
     }
   }
-  // y = alpha Y + beta_y y
-  for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-    const int b = l / S::ND, i = l - b * S::ND;
-    const Real v = base[(size_t)b * S::PER_ELEM + 2 * S::ND + i];
-    Real* dst = yout + e0 * S::ND + l;
-    *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
-  }
+  nd_output<D, N>(P, yout, e0, ne, base);
 }
 
 template <int D, int N, typename Real>
@@ -307,6 +324,152 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_kernel(const __grid_con
   for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
     kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Grouped variant: the axes are cut into groups of G consecutive axes, and one thread takes a
+// block of the element that spans one group (N^G values with the other axes fixed), runs the
+// group's passes in registers and writes the block back once.  A term costs one shared-memory
+// round trip per group instead of one per axis: for D = 6, N = 3 and G = 3, two round trips of
+// 27-value blocks instead of six of 3-value lines.  The term's own axis (D_a scaled by the element
+// factor, then the face terms of that axis) is in the first group a term runs; the other groups
+// follow in increasing order and the last one accumulates into Y.  Same shared-memory layout and
+// setup as the per-axis kernel above; the tangential passes run in another order, so the results
+// agree with it to rounding (the passes along different axes commute exactly in real arithmetic).
+// ------------------------------------------------------------------------------------------
+template <int D, int N, int G>
+struct KronGroups {
+  static constexpr int NG = (D + G - 1) / G;
+  static constexpr int lo(int g) { return g * G; }
+  static constexpr int hi(int g) { return (g + 1) * G < D ? (g + 1) * G : D; }
+  static constexpr int size(int g) { return kpow(N, hi(g) - lo(g)); }
+  static constexpr int inner(int g) { return kpow(N, lo(g)); }
+  // step st of a term whose first pass is along AX: AX's group first, then the others in order
+  static constexpr int group(int AX, int st) { return st == 0 ? AX / G : (st <= AX / G ? st - 1 : st); }
+  // the kk-th axis a step of group g runs: AX first in the term's first step (its face terms need
+  // the input values), the group's other axes in increasing order
+  static constexpr int axis(int g, int kk, bool first, int AX) {
+    return !first ? lo(g) + kk : (kk == 0 ? AX : (lo(g) + kk - 1 < AX ? lo(g) + kk - 1 : lo(g) + kk));
+  }
+};
+
+// Step ST of term TERM (TERM == D: the separate mass term, first pass along D - 1) over the blocks
+// of its group, for the ne elements of the batch.
+template <int D, int N, int G, int TERM, int ST, typename Real>
+__device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const Real* __restrict__ xin, Real* base,
+                                              int ne, int64_t e0, const int (*ecoord)[kMaxDim]) {
+  using S = KronNDShape<D, N>;
+  using GR = KronGroups<D, N, G>;
+  constexpr bool MASS = TERM == D;
+  constexpr int AX = MASS ? D - 1 : TERM;
+  constexpr int g = GR::group(AX, ST);
+  constexpr int LO = GR::lo(g), HI = GR::hi(g), GSZ = GR::size(g), INNER = GR::inner(g);
+  constexpr int IPE = S::ND / GSZ;  // blocks per element
+  constexpr bool FIRST = ST == 0, LAST = ST == GR::NG - 1;
+  const int total = ne * IPE;
+  for (int it = threadIdx.x; it < total; it += blockDim.x) {
+    const int b = it / IPE;
+    const int loc = it - b * IPE;
+    const int o = loc / INNER, t = loc - o * INNER;
+    const int off = o * GSZ * INNER + t;  // block value j sits at off + j * INNER
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    const Real* src = FIRST ? el : el + S::ND;
+    Real v[GSZ];
+#pragma unroll
+    for (int j = 0; j < GSZ; ++j) v[j] = src[off + j * INNER];
+    static_for<0, HI - LO>([&](auto kc) {
+      constexpr int k = GR::axis(g, decltype(kc)::value, FIRST, AX);
+      constexpr int SK = kpow(N, k - LO);  // stride of axis k inside the block
+      constexpr bool OWN = FIRST && k == AX;
+      const PassMat<N, Real> m(el + 3 * S::ND + (MASS ? D * D + k : TERM * D + k) * S::MAT);
+      Real scale = Real(1);
+      if constexpr (OWN) {
+        const Real* ef = MASS ? P.elem_mass : P.elem[AX];
+        if (ef) scale = ef[e0 + b];
+      }
+#pragma unroll
+      for (int ln = 0; ln < GSZ / N; ++ln) {
+        const int p0 = (ln / SK) * SK * N + (ln % SK);
+        Real w[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          Real s = m(j, 0) * v[p0];
+#pragma unroll
+          for (int i = 1; i < N; ++i) s += m(j, i) * v[p0 + i * SK];
+          w[j] = s;
+        }
+        if constexpr (OWN) {
+          if (MASS ? P.elem_mass != nullptr : P.elem[AX] != nullptr) {
+#pragma unroll
+            for (int j = 0; j < N; ++j) w[j] *= scale;
+          }
+          if constexpr (!MASS) {
+            // face terms of axis AX on the line's two ends (GLL: the trace is the end value)
+            const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+            const uint32_t* fw = reinterpret_cast<const uint32_t*>(rec + 4 * D);
+#pragma unroll
+            for (int sd = 0; sd < 2; ++sd) {
+              const int fi = AX * 2 + sd;
+              const uint32_t f = (fw[fi / 6] >> (5 * (fi % 6))) & 31u;
+              if (!f) continue;
+              const int sl = sd ? N - 1 : 0;
+              Real add = Real(0);
+              if (f & 1u) add += rec[2 * fi] * v[p0 + sl * SK];
+              if (f & 2u) {
+                const int64_t n = P.sizes[AX];
+                const int64_t ca = ecoord[b][AX];
+                const int64_t cn = sd ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
+                const int64_t en = e0 + b + (cn - ca) * P.estride[AX];
+                add += rec[2 * fi + 1] * xin[en * S::ND + off + (p0 + (N - 1 - sl) * SK) * INNER];
+              } else if (f & 4u) {
+                add += rec[2 * fi + 1] * P.g;
+              }
+              w[sl] += add;
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < N; ++j) v[p0 + j * SK] = w[j];
+      }
+    });
+    Real* dst = el + (LAST ? 2 : 1) * S::ND;
+#pragma unroll
+    for (int j = 0; j < GSZ; ++j) {
+      if constexpr (LAST) dst[off + j * INNER] += v[j];
+      else dst[off + j * INNER] = v[j];
+    }
+  }
+}
+
+template <int D, int N, int G, typename Real>
+__global__ void __launch_bounds__(kKronNDThreads)
+    kronnd_grouped_kernel(const __grid_constant__ KronNDParams<Real> P) {
+  using GR = KronGroups<D, N, G>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* base = reinterpret_cast<Real*>(smem_raw);
+  __shared__ int ecoord[64][kMaxDim];
+  if (P.skip && *P.skip) return;
+  const int EB = P.eb;
+  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    nd_setup<D, N>(P, P.x, e0, ne, base, ecoord);
+    if (P.has_adv) {
+      static_for<0, D>([&](auto ac) {
+        constexpr int a = decltype(ac)::value;
+        static_for<0, GR::NG>([&](auto sc) {
+          nd_group_step<D, N, G, a, decltype(sc)::value>(P, P.x, base, ne, e0, ecoord);
+          __syncthreads();
+        });
+      });
+    }
+    if (P.has_mass && !(P.has_adv && P.mass_merged)) {
+      static_for<0, GR::NG>([&](auto sc) {
+        nd_group_step<D, N, G, D, decltype(sc)::value>(P, P.x, base, ne, e0, ecoord);
+        __syncthreads();
+      });
+    }
+    nd_output<D, N>(P, P.y, e0, ne, base);
   }
 }
 
