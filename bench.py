@@ -492,7 +492,7 @@ def run_batch(args):
             "unit": "GDoF/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic (seed 7)",
             "config": {"workload": f"batch of {len(ops)} instances (d in 2..4, p in 1..5, E log-uniform 1e3..1e5, "
                                    "constant velocity, dt 1e-3)", "total_dofs": int(total), "kernels": kinds,
-                       "groups": len({(o.space.dim, o.space.order) for o in ops if o.kernel == "kronnd"}),
+                       "groups": len({(o.space.dim, o.space.order, o.variant) for o in ops if o.kernel == "kronnd"}),
                        "setup_s": setup_s},
             "apply": {"batched_ms": ms_batch, "one_launch_each_ms": ms_each,
                       "batched_gdofs_per_s": total / ms_batch / 1e6, "one_launch_each_gdofs_per_s": total / ms_each / 1e6},

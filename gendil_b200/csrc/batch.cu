@@ -1,6 +1,7 @@
 // Batches of independent operators: one persistent launch per (dimension, order) class.
 //
-// Operators on the any-dimension Kronecker kernel are grouped by (D, N); each group's parameter
+// Operators on the any-dimension Kronecker kernel are grouped by (D, N, kernel variant); each
+// group's parameter
 // table (the operators' forward parameters, x and y patched per apply) and the prefix sums of
 // their element batches live on the device, and one launch of kronnd_batch_kernel walks every
 // element batch of every operator of the group.  Operators on another kernel are applied one
@@ -9,6 +10,7 @@
 
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <new>
 #include <vector>
 
@@ -19,6 +21,7 @@ using namespace dgop;
 namespace {
 struct BatchGroup {
   const KronNDEntry<double>* entry = nullptr;
+  int variant = 0;
   std::vector<int> members;                 // indices into the batch
   std::vector<KronNDParams<double>> table;  // host copy (x, y patched per apply)
   std::vector<int64_t> first;
@@ -56,21 +59,23 @@ void release(dgop_batch* b) {
 }
 
 int setup(dgop_batch* b) {
-  std::map<std::pair<int, int>, int> index;
+  std::map<std::tuple<int, int, int>, int> index;
   for (int i = 0; i < (int)b->ops.size(); ++i) {
     dgop_operator* op = b->ops[i];
-    if (op->kernel != DGOP_KERNEL_KRONND || !op->n64.ready) {
+    const int v = op->n64.variant;
+    if (op->kernel != DGOP_KERNEL_KRONND || !op->n64.ready || !op->n64.entry->launch_batch[v]) {
       b->singles.push_back(i);
       continue;
     }
-    const auto key = std::make_pair(op->sp.D, op->sp.n);
+    const auto key = std::make_tuple(op->sp.D, op->sp.n, v);
     auto it = index.find(key);
     if (it == index.end()) {
       it = index.emplace(key, (int)b->groups.size()).first;
       b->groups.emplace_back();
       b->groups.back().entry = op->n64.entry;
-      b->groups.back().eb = op->n64.params.eb;
-      b->groups.back().smem = op->n64.smem;
+      b->groups.back().variant = v;
+      b->groups.back().eb = op->n64.var[v].eb;
+      b->groups.back().smem = op->n64.var[v].smem;
       b->groups.back().block = op->n64.block;
     }
     b->groups[it->second].members.push_back(i);
@@ -101,11 +106,12 @@ int setup(dgop_batch* b) {
     DGOP_CUDA_B(cudaMalloc(&g.d_first, sizeof(int64_t) * g.first.size()));
     DGOP_CUDA_B(cudaMemcpy(g.d_first, g.first.data(), sizeof(int64_t) * g.first.size(), cudaMemcpyHostToDevice));
     cudaFuncAttributes fa{};
-    DGOP_CUDA_B(cudaFuncGetAttributes(&fa, g.entry->func_batch));
-    DGOP_CUDA_B(cudaFuncSetAttribute(g.entry->func_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const void* fn = g.entry->func_batch[g.variant];
+    DGOP_CUDA_B(cudaFuncGetAttributes(&fa, fn));
+    DGOP_CUDA_B(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      max_smem - (int)fa.sharedSizeBytes));
     int per_sm = 0;
-    DGOP_CUDA_B(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g.entry->func_batch, (int)g.block.x, g.smem));
+    DGOP_CUDA_B(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)g.block.x, g.smem));
     if (per_sm < 1) per_sm = 1;
     g.grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(g.first.back(), (int64_t)sms * per_sm)));
   }
@@ -169,7 +175,8 @@ int dgop_batch_apply(dgop_batch* b, const double* const* x, double* const* y, vo
     }
     DGOP_CUDA_B(cudaMemcpyAsync(g.d_table, g.h_pinned, sizeof(KronNDParams<double>) * g.members.size(),
                                 cudaMemcpyHostToDevice, st));
-    g.entry->launch_batch(g.d_table, g.d_first, (int)g.members.size(), g.eb, g.grid, g.block, g.smem, st);
+    g.entry->launch_batch[g.variant](g.d_table, g.d_first, (int)g.members.size(), g.eb, g.grid, g.block, g.smem,
+                                     st);
     DGOP_CUDA_B(cudaGetLastError());
   }
   DGOP_CUDA_B(cudaEventRecord(b->uploaded, st));

@@ -25,10 +25,10 @@ void launch_kronnd_grouped(const KronNDParams<Real>& p, dim3 grid, dim3 block, s
   kronnd_grouped_kernel<D, N, G, Real><<<grid, block, smem, s>>>(p);
 }
 
-template <int D, int N, typename Real>
+template <int D, int N, int V, typename Real>
 void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, int count, int eb, dim3 grid,
                          dim3 block, size_t smem, cudaStream_t s) {
-  kronnd_batch_kernel<D, N, Real><<<grid, block, smem, s>>>(table, first, count, eb);
+  kronnd_batch_kernel<D, N, V, Real><<<grid, block, smem, s>>>(table, first, count, eb);
 }
 
 template <int D, int N, typename Real>
@@ -52,17 +52,25 @@ void fill(KronNDEntry<Real>& d) {
   if constexpr (fits<D, N, Real>()) {
     d.launch = &launch_kronnd<D, N, Real>;
     d.func = reinterpret_cast<const void*>(&kronnd_kernel<D, N, Real>);
-    d.launch_batch = &launch_kronnd_batch<D, N, Real>;
-    d.func_batch = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, Real>);
+    d.launch_batch[0] = &launch_kronnd_batch<D, N, 0, Real>;
+    d.func_batch[0] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 0, Real>);
     d.per_elem = KronNDShape<D, N>::PER_ELEM;
     // grouped variants while a block (N^G values) stays a register array
     if constexpr (D >= 2 && N >= 2 && N * N <= 27) {
       d.launch_g[0] = &launch_kronnd_grouped<D, N, 2, Real>;
       d.func_g[0] = reinterpret_cast<const void*>(&kronnd_grouped_kernel<D, N, 2, Real>);
+      if constexpr (sizeof(Real) == 8) {
+        d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
+        d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);
+      }
     }
     if constexpr (D >= 3 && N >= 2 && N * N * N <= 27) {
       d.launch_g[1] = &launch_kronnd_grouped<D, N, 3, Real>;
       d.func_g[1] = reinterpret_cast<const void*>(&kronnd_grouped_kernel<D, N, 3, Real>);
+      if constexpr (sizeof(Real) == 8) {
+        d.launch_batch[2] = &launch_kronnd_batch<D, N, 2, Real>;
+        d.func_batch[2] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 2, Real>);
+      }
     }
   }
   if constexpr ((int64_t)(KronDiffShape<D, N>::PER_ELEM + KronDiffShape<D, N>::HDR) * (int64_t)sizeof(Real) <=

@@ -35,15 +35,20 @@ KronEntry<double>& kron3d_slot_f64(int N);
 KronEntry<float>& kron3d_slot_f32(int N);
 void register_kron3d();
 
-// Kronecker form, any dimension, shared-memory kernel (kronnd_kernel.cuh).
+// Kronecker form, any dimension, shared-memory kernel (kronnd_kernel.cuh).  Variants (the
+// autotuner picks one per operator): 0 one shared-memory pass per axis; 1, 2 groups of 2 or 3
+// axes per pass in registers.
+constexpr int kKronNDVariants = 3;
+extern const char* const kKronNDVariantNames[kKronNDVariants];
+
 template <typename Real>
 struct KronNDEntry {
   void (*launch)(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func = nullptr;
-  // many operators of this (D, N) in one launch (dgop_batch_apply)
-  void (*launch_batch)(const KronNDParams<Real>* table, const int64_t* first, int count, int eb, dim3 grid,
-                       dim3 block, size_t smem, cudaStream_t s) = nullptr;
-  const void* func_batch = nullptr;
+  // many operators of this (D, N) in one launch (dgop_batch_apply), per variant
+  void (*launch_batch[kKronNDVariants])(const KronNDParams<Real>* table, const int64_t* first, int count, int eb,
+                                        dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
+  const void* func_batch[kKronNDVariants] = {};
   int per_elem = 0;  // Real values of shared memory per element
   // grouped variants (kronnd_grouped_kernel), groups of 2 and 3 axes: same parameters and layout
   void (*launch_g[2])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
@@ -57,10 +62,6 @@ struct KronNDEntry {
   const void* func_grad = nullptr;
   int per_elem_grad = 0, header_grad = 0;
 };
-// Variants of the any-dimension kernel (the autotuner picks one per operator):
-//   0: one shared-memory pass per axis; 1, 2: groups of 2 or 3 axes per pass in registers
-constexpr int kKronNDVariants = 3;
-extern const char* const kKronNDVariantNames[kKronNDVariants];
 KronNDEntry<double>& kronnd_slot_f64(int D, int N);
 KronNDEntry<float>& kronnd_slot_f32(int D, int N);
 void register_kronnd_d1();

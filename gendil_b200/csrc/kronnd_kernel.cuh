@@ -34,8 +34,8 @@ struct KronNDShape {
   static constexpr int NS = D * D + D;   // matrix slots: D terms x D axes, plus the mass term
   static constexpr int MAT = N * N;
   // per element: U, W, Y, the slot matrices, and 2D face records (corner, neighbour / inflow
-  // coefficient) + flags
-  static constexpr int REC = 4 * D + 2;
+  // coefficient) + one flag byte per face (16 bytes, whatever the Real)
+  static constexpr int REC = 4 * D + 16 / (int)sizeof(float);
   static constexpr int PER_ELEM = 3 * ND + NS * MAT + REC;
 };
 
@@ -93,58 +93,49 @@ __device__ __forceinline__ void nd_pass(Real* base, int ne, int eb, int slot, co
   }
 }
 
-// Face records of element e (one thread per element): for face f = a * 2 + s, rec[2 f] is the
-// own-trace (corner) coefficient, rec[2 f + 1] the neighbour / inflow coefficient, and bits of
-// the flag word (5 per face): 1 corner, 2 neighbour trace, 4 inflow value.  Follows the upwind
-// rule of advectionoperator.hpp:379-386 / 422-428 per element, as the 3D kernel does.
+// Face record of face fi = a * 2 + s of element e (one thread per face): rec[2 fi] is the
+// own-trace (corner) coefficient, rec[2 fi + 1] the neighbour / inflow coefficient, and the
+// face's flag byte: 1 corner, 2 neighbour trace, 4 inflow value.  Follows the upwind rule of
+// advectionoperator.hpp:379-386 / 422-428 per element, as the 3D kernel does.
 template <int D, typename Real>
-__device__ __forceinline__ void nd_face_records(const KronNDParams<Real>& P, int64_t e, const int64_t (&c)[kMaxDim],
-                                                Real* rec, uint32_t* flags_out) {
-  // 5 bits per face, six faces per 32-bit word: faces 0..5 in word 0, 6..11 in word 1
-  uint32_t flags[2] = {0u, 0u};
+__device__ __forceinline__ void nd_face_record(const KronNDParams<Real>& P, int64_t e, const int* c, int fi, Real* rec,
+                                               uint8_t* flag) {
   const bool transpose = (P.flags & kTranspose) != 0;
+  const int a = fi >> 1, s = fi & 1;
+  Real tsign = Real(1);
 #pragma unroll
-  for (int a = 0; a < D; ++a) {
-    Real tsign = Real(1);
-#pragma unroll
-    for (int k = 0; k < D; ++k)
-      if (k != a) tsign *= (Real)P.sgn[a][k][c[k]];
-    const Real el = P.elem[a] ? P.elem[a][e] : Real(1);
-    const int64_t n = P.sizes[a];
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const bool interior = s == 0 ? (c[a] > 0 || P.periodic[a]) : (c[a] + 1 < n || P.periodic[a]);
-      const bool active = interior ? (P.flags & kFaceInt) : (P.flags & kFaceBnd);
-      const Real phi = P.phi[a][c[a] * 2 + s];
-      Real coef = Real(0);
-      uint32_t bits = 0;
-      if (active) {
-        if (phi * tsign * el > Real(0)) bits |= 1u;
-        if (!transpose) {
-          if (!(phi * tsign * el > Real(0))) {
-            coef = phi * el;
-            bits |= interior ? 2u : 4u;
-          }
-        } else if (interior) {
-          // transposed coupling: the neighbour's row, taken when its face 1 - s is inflow for it
-          const int64_t cn = s ? (c[a] + 1 == n ? 0 : c[a] + 1) : (c[a] == 0 ? n - 1 : c[a] - 1);
-          const int64_t en = e + (cn - c[a]) * P.estride[a];
-          const Real phin = P.phi[a][cn * 2 + (1 - s)];
-          const Real eln = P.elem[a] ? P.elem[a][en] : Real(1);
-          if (!(phin * tsign * eln > Real(0))) {
-            coef = phin * eln;
-            bits |= 2u;
-          }
-        }
+  for (int k = 0; k < D; ++k)
+    if (k != a) tsign *= (Real)P.sgn[a][k][c[k]];
+  const Real el = P.elem[a] ? P.elem[a][e] : Real(1);
+  const int64_t n = P.sizes[a];
+  const int64_t ca = c[a];
+  const bool interior = s == 0 ? (ca > 0 || P.periodic[a]) : (ca + 1 < n || P.periodic[a]);
+  const bool active = interior ? (P.flags & kFaceInt) : (P.flags & kFaceBnd);
+  const Real phi = P.phi[a][ca * 2 + s];
+  Real coef = Real(0);
+  uint32_t bits = 0;
+  if (active) {
+    if (phi * tsign * el > Real(0)) bits |= 1u;
+    if (!transpose) {
+      if (!(phi * tsign * el > Real(0))) {
+        coef = phi * el;
+        bits |= interior ? 2u : 4u;
       }
-      rec[2 * (a * 2 + s)] = phi * el;
-      rec[2 * (a * 2 + s) + 1] = coef;
-      const int fi = a * 2 + s;
-      flags[fi / 6] |= bits << (5 * (fi % 6));
+    } else if (interior) {
+      // transposed coupling: the neighbour's row, taken when its face 1 - s is inflow for it
+      const int64_t cn = s ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
+      const int64_t en = e + (cn - ca) * P.estride[a];
+      const Real phin = P.phi[a][cn * 2 + (1 - s)];
+      const Real eln = P.elem[a] ? P.elem[a][en] : Real(1);
+      if (!(phin * tsign * eln > Real(0))) {
+        coef = phin * eln;
+        bits |= 2u;
+      }
     }
   }
-  flags_out[0] = flags[0];
-  flags_out[1] = flags[1];
+  rec[2 * fi] = phi * el;
+  rec[2 * fi + 1] = coef;
+  *flag = (uint8_t)bits;
 }
 
 // Face terms of axis A added to W (= D_A U) on the two slices of that axis.  One thread takes a
@@ -161,11 +152,11 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
     const int o = p / INNER, t = p - o * INNER;
     Real* el = base + (size_t)b * S::PER_ELEM;
     const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
-    const uint32_t* fw = reinterpret_cast<const uint32_t*>(rec + 4 * D);
+    const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int fi = A * 2 + s;
-      const uint32_t f = (fw[fi / 6] >> (5 * (fi % 6))) & 31u;
+      const uint32_t f = fb[fi];
       if (!f) continue;
       const int sl = s ? N - 1 : 0;
       const int idx = o * N * INNER + sl * INNER + t;
@@ -220,17 +211,12 @@ __device__ __forceinline__ void nd_setup(const KronNDParams<Real>& P, const Real
     if (m.off >= 0) v = P.mats[m.off + (int64_t)ecoord[b][k] * m.stride + q];
     base[(size_t)b * S::PER_ELEM + 3 * S::ND + r] = v;
   }
-  if (adv && threadIdx.x < ne) {
-    const int b = threadIdx.x;
-    const int64_t e = e0 + b;
-    int64_t c[kMaxDim];
-#pragma unroll
-    for (int k = 0; k < D; ++k) c[k] = ecoord[b][k];
-    Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
-    uint32_t fl[2];
-    nd_face_records<D>(P, e, c, rec, fl);
-    reinterpret_cast<uint32_t*>(rec + 4 * D)[0] = fl[0];
-    reinterpret_cast<uint32_t*>(rec + 4 * D)[1] = fl[1];
+  if (adv) {
+    for (int l = threadIdx.x; l < ne * 2 * D; l += blockDim.x) {
+      const int b = l / (2 * D), fi = l - b * (2 * D);
+      Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
+      nd_face_record<D>(P, e0 + b, ecoord[b], fi, rec, reinterpret_cast<uint8_t*>(rec + 4 * D) + fi);
+    }
   }
   __syncthreads();
 }
@@ -407,11 +393,11 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
           if constexpr (!MASS) {
             // face terms of axis AX on the line's two ends (GLL: the trace is the end value)
             const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
-            const uint32_t* fw = reinterpret_cast<const uint32_t*>(rec + 4 * D);
+            const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
 #pragma unroll
             for (int sd = 0; sd < 2; ++sd) {
               const int fi = AX * 2 + sd;
-              const uint32_t f = (fw[fi / 6] >> (5 * (fi % 6))) & 31u;
+              const uint32_t f = fb[fi];
               if (!f) continue;
               const int sl = sd ? N - 1 : 0;
               Real add = Real(0);
@@ -442,10 +428,34 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
   }
 }
 
+// One batch of ne elements starting at e0 with the grouped passes.
+template <int D, int N, int G, typename Real>
+__device__ __forceinline__ void kronnd_grouped_block(const KronNDParams<Real>& P, const Real* __restrict__ xin,
+                                                     Real* __restrict__ yout, int64_t e0, int ne, Real* base,
+                                                     int (*ecoord)[kMaxDim]) {
+  using GR = KronGroups<D, N, G>;
+  nd_setup<D, N>(P, xin, e0, ne, base, ecoord);
+  if (P.has_adv) {
+    static_for<0, D>([&](auto ac) {
+      constexpr int a = decltype(ac)::value;
+      static_for<0, GR::NG>([&](auto sc) {
+        nd_group_step<D, N, G, a, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+        __syncthreads();
+      });
+    });
+  }
+  if (P.has_mass && !(P.has_adv && P.mass_merged)) {
+    static_for<0, GR::NG>([&](auto sc) {
+      nd_group_step<D, N, G, D, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+      __syncthreads();
+    });
+  }
+  nd_output<D, N>(P, yout, e0, ne, base);
+}
+
 template <int D, int N, int G, typename Real>
 __global__ void __launch_bounds__(kKronNDThreads)
     kronnd_grouped_kernel(const __grid_constant__ KronNDParams<Real> P) {
-  using GR = KronGroups<D, N, G>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* base = reinterpret_cast<Real*>(smem_raw);
   __shared__ int ecoord[64][kMaxDim];
@@ -453,30 +463,15 @@ __global__ void __launch_bounds__(kKronNDThreads)
   const int EB = P.eb;
   for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
-    nd_setup<D, N>(P, P.x, e0, ne, base, ecoord);
-    if (P.has_adv) {
-      static_for<0, D>([&](auto ac) {
-        constexpr int a = decltype(ac)::value;
-        static_for<0, GR::NG>([&](auto sc) {
-          nd_group_step<D, N, G, a, decltype(sc)::value>(P, P.x, base, ne, e0, ecoord);
-          __syncthreads();
-        });
-      });
-    }
-    if (P.has_mass && !(P.has_adv && P.mass_merged)) {
-      static_for<0, GR::NG>([&](auto sc) {
-        nd_group_step<D, N, G, D, decltype(sc)::value>(P, P.x, base, ne, e0, ecoord);
-        __syncthreads();
-      });
-    }
-    nd_output<D, N>(P, P.y, e0, ne, base);
+    kronnd_grouped_block<D, N, G>(P, P.x, P.y, e0, ne, base, ecoord);
   }
 }
 
-// Many operators of one (D, N) in one persistent launch: table[i] holds instance i's parameters
-// (forward operator, x / y set per apply), its element batches are the global batch indices
-// [first[i], first[i + 1]); every CTA walks the global batches.
-template <int D, int N, typename Real>
+// Many operators of one (D, N) and kernel variant V (0: one pass per axis, 1 / 2: groups of 2 / 3
+// axes) in one persistent launch: table[i] holds instance i's parameters (forward operator, x / y
+// set per apply), its element batches are the global batch indices [first[i], first[i + 1]);
+// every CTA walks the global batches.
+template <int D, int N, int V, typename Real>
 __global__ void __launch_bounds__(kKronNDThreads)
     kronnd_batch_kernel(const KronNDParams<Real>* __restrict__ table, const int64_t* __restrict__ first, int count,
                         int EB) {
@@ -495,7 +490,8 @@ __global__ void __launch_bounds__(kKronNDThreads)
     const KronNDParams<Real>& P = table[lo];
     const int64_t e0 = (gb - first[lo]) * EB;
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
-    kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
+    if constexpr (V == 0) kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
+    else kronnd_grouped_block<D, N, V + 1>(P, P.x, P.y, e0, ne, base, ecoord);
   }
 }
 

@@ -1,5 +1,5 @@
 """GPU: batches of independent operators (dgop_batch_apply): one persistent launch per
-(dimension, order) group on the any-dimension Kronecker kernel, the rest one launch each; results
+(dimension, order, kernel variant) group on the any-dimension Kronecker kernel, the rest one launch each; results
 bit-identical to each operator's own apply."""
 import numpy as np
 import pytest
@@ -34,7 +34,7 @@ def test_batch_apply_equals_individual_applies():
         o(x, y)
         want.append(y)
     batch = g.Batch(ops)
-    assert batch.groups == len({(o.space.dim, o.space.order) for o in ops if o.kernel == "kronnd"})
+    assert batch.groups == len({(o.space.dim, o.space.order, o.variant) for o in ops if o.kernel == "kronnd"})
     for _ in range(2):  # twice: the parameter upload of the previous apply is reused safely
         ys = [torch.full_like(x, float("nan")) for x in xs]
         batch.apply(xs, ys)
