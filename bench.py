@@ -258,7 +258,7 @@ def run_ours(args):
     six = args.workload == "6d"
     if six:
         # configuration 3: 8^6 elements on [0,1]^3 x [-1,1]^3, p = 2, q = 3, beta = (v, -x + 0.5)
-        n6 = 8
+        n6 = args.size_6d
         space = g.Space(6, [n6] * 6, [1.0 / n6] * 3 + [2.0 / n6] * 3, [0.0] * 3 + [-1.0] * 3, None, 2)
         op = g.AdvectionOperator(space, 3, C.velocity_phase_space(6), bc=g.BC_INFLOW, g=0.0)
     else:
@@ -317,7 +317,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)",
-                "config": {"workload": WORKLOAD_6D if six else WORKLOAD, "dofs": nd,
+                "config": {"workload": (WORKLOAD_6D.replace("8^6", f"{n6}^6") if six else WORKLOAD), "dofs": nd,
                            "elements": space.num_elements,
                            "parallelism": f"replicas{world}" if world > 1 else "single",
                            "l2": f"inputs larger than L2 (x, y {8 * nd / 1e6:.0f} MB each)"},
@@ -519,7 +519,7 @@ def run_sipdg(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    n, p, q = 32, 4, 6
+    n, p, q = args.size_sipdg, 4, 6
     space = g.Space(3, [n] * 3, order=p)
     ne, nd = space.num_elements, space.num_dofs
     z = torch.tensor(np.random.default_rng(4).normal(0.0, 0.5, ne), device=dev)
@@ -559,6 +559,14 @@ def run_sipdg(args):
         s.close()
         return u, info, a.elapsed_time(b) * 1e-3
 
+    if args.no_solve:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": 1, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                          "dtype": "f64", "data": "synthetic", "gpu_launches": args.steps,
+                          "config": {"workload": WORKLOAD_SIPDG.replace("32^3", f"{n}^3"), "dofs": nd,
+                                     "kernel": op.kernel, "note": "apply only (--no-solve)"}}))
+        op.close()
+        return 0
     cg(f, tol=1e-2)  # warm-up
     u, info_f, t_fwd = cg(f)
     r = torch.empty_like(u)
@@ -620,7 +628,7 @@ def run_sipdg(args):
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seeds 1, 5, 6; numpy normal seed 4)",
-            "config": {"workload": WORKLOAD_SIPDG, "dofs": nd, "elements": ne, "kernel": op.kernel,
+            "config": {"workload": WORKLOAD_SIPDG.replace("32^3", f"{n}^3"), "dofs": nd, "elements": ne, "kernel": op.kernel,
                        "l2": f"inputs smaller than L2 ({8 * nd / 1e6:.0f} MB each); applies back to back"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
@@ -647,7 +655,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--size", type=int, default=N_AXIS, help="elements per axis (profiling runs only)")
+    ap.add_argument("--size", type=int, default=None,
+                    help="elements per axis (profiling runs only; defaults 64 for 3d, 8 for 6d, 32 for sipdg)")
     ap.add_argument("--variant", default=None, help="force a Kronecker-kernel variant (profiling runs only)")
     ap.add_argument("--workload", choices=["3d", "6d", "batch", "sipdg"], default="3d",
                     help="3d: the 64^3 p=3 advection apply (default); 6d: the 8^6 p=2 phase-space configuration; "
@@ -656,6 +665,9 @@ def main():
     ap.add_argument("--instances", type=int, default=512, help="batch workload: number of instances")
     ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent solve streams")
     args = ap.parse_args()
+    args.size_6d = args.size or 8
+    args.size_sipdg = args.size or 32
+    args.size = args.size or N_AXIS
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
