@@ -25,8 +25,9 @@ import numpy as np
 from .coefficients import Coefficient, as_coefficient
 
 __all__ = ["Space", "MassOperator", "AdvectionOperator", "MassAdvectionOperator", "SystemOperator",
-           "CGSolver", "GMRESSolver", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL", "BC_NONE",
-           "BC_INFLOW"]
+           "SIPDGOperator", "DiffusionOperator", "MassInverseOperator", "CGSolver", "GMRESSolver", "GMRESIRSolver",
+           "Batch", "HostIO", "element_dot", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL",
+           "BC_NONE", "BC_INFLOW"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libdgop.so")
@@ -328,6 +329,21 @@ class SIPDGOperator(_Operator):
         check(lib().dgop_sipdg_gradient(self.handle, _ptr(u), _ptr(lam), None if scale is None else _ptr(scale),
                                         _ptr(out), _stream(stream)))
         return out
+
+
+class DiffusionOperator(SIPDGOperator):
+    """MakeDiffusionOperator<KP>(fes, ir, velocity, sigma, kappa), the reference's legacy SIPDG
+    operator (FiniteElementMethod/MatrixFreeOperators/diffusionoperator.hpp:554): cell term,
+    interior and boundary faces, penalty kappa / h.  `diffusivity` is a constant (the reference
+    evaluates a function of X; constants are what its tests use) or one value per element."""
+
+    def __init__(self, space, q, diffusivity, sigma, kappa):
+        import torch
+        if isinstance(diffusivity, (int, float)):
+            mu = torch.full((space.num_elements,), float(diffusivity), dtype=torch.float64, device="cuda")
+        else:
+            mu = diffusivity
+        super().__init__(space, q, mu, sigma=sigma, kappa=kappa, boundary=True)
 
 
 class MassInverseOperator(_Operator):

@@ -898,7 +898,12 @@ struct OperatorPlan {
   std::shared_ptr<const detail::ScalarField> outflow;  // boundary indicator (null: 1)
   std::shared_ptr<const detail::ScalarField> inflow;   // legacy bc(X) (null: 0 or no boundary)
   const Real* beta_factor = nullptr;  // per-element velocity factor (device, num_elements; null: 1)
+  // interior-penalty diffusion (MakeDiffusionOperator): diffusivity constant on each element
+  bool diffusion = false;
+  std::shared_ptr<const detail::ScalarField> diffusivity;
+  Real ip_sigma = -1.0, ip_kappa = 0.0;
   std::string describe() const {
+    if (diffusion) return "interior-penalty diffusion, diffusivity=" + (diffusivity ? diffusivity->name : "?");
     std::ostringstream s;
     s << (mass ? "mass" : "") << (mass && cell ? "+" : "") << (cell ? "cell" : "") << (interior ? "+interior" : "")
       << (boundary ? "+boundary" : "");
@@ -1099,7 +1104,11 @@ class Operator {
   Integer Size() const { return fes_.GetNumberOfFiniteElementDofs(); }
   dgop_operator* handle() const { return op_.get(); }
   const OperatorPlan& plan() const { return plan_; }
-  std::string KernelName() const { return dgop_operator_kernel(op_.get()) == DGOP_KERNEL_KRON ? "kron" : "generic"; }
+  std::string KernelName() const {
+    static const char* const names[] = {"generic", "kron", "kronnd", "diffusion"};
+    const int k = dgop_operator_kernel(op_.get());
+    return (k >= 0 && k < 4) ? names[k] : "unknown";
+  }
 
   // device-resident solvers, created once per (kind, restart, inner precision); kind 0 CG,
   // 1 GMRES, 2 refinement GMRES, 3 a second GMRES handle (the adjoint solve's)
@@ -1127,6 +1136,53 @@ class Operator {
     if (x.Size() != Size() || y.Size() != Size()) throw Error("operator: vector size does not match the space");
   }
 
+  std::shared_ptr<Real> mu_;  // per-element diffusivity on the device (diffusion operators)
+
+  // The Kronecker-form diffusion kernel takes one diffusivity per element: evaluate the
+  // reference's function of X at every Gauss point of every element and require it constant
+  // on each element.
+  void create_diffusion(const detail::Grid& g) {
+    const CartesianMesh<D>& mesh = fes_.GetMesh();
+    int64_t ne = 1;
+    for (Integer k = 0; k < D; ++k) ne *= (int64_t)mesh.sizes[k];
+    std::vector<Real> mu((size_t)ne);
+    const int q = q_;
+    int64_t qd = 1;
+    for (Integer k = 0; k < D; ++k) qd *= q;
+    for (int64_t e = 0; e < ne; ++e) {
+      int64_t c[D];
+      int64_t r = e;
+      for (Integer k = 0; k < D; ++k) {
+        c[k] = r % (int64_t)mesh.sizes[k];
+        r /= (int64_t)mesh.sizes[k];
+      }
+      Real first = 0.0;
+      for (int64_t p = 0; p < qd; ++p) {
+        Real X[6];
+        int64_t t = p;
+        for (Integer k = 0; k < D; ++k) {
+          X[k] = g.x[k][c[k] * (q + 2) + t % q];
+          t /= q;
+        }
+        const Real v = plan_.diffusivity->eval((int)D, X);
+        if (p == 0) first = v;
+        else if (std::abs(v - first) > 1e-14 * std::max(std::abs(first), Real(1)))
+          throw Error("MakeDiffusionOperator: the diffusivity '" + plan_.diffusivity->name +
+                      "' must be constant on each element");
+      }
+      mu[(size_t)e] = first;
+    }
+    Real* d = nullptr;
+    if (cudaMalloc(&d, sizeof(Real) * (size_t)ne) != cudaSuccess) throw Error("MakeDiffusionOperator: cudaMalloc");
+    mu_ = std::shared_ptr<Real>(d, [](Real* ptr) { cudaFree(ptr); });
+    if (cudaMemcpy(d, mu.data(), sizeof(Real) * (size_t)ne, cudaMemcpyHostToDevice) != cudaSuccess)
+      throw Error("MakeDiffusionOperator: cudaMemcpy");
+    dgop_operator* op = nullptr;
+    detail::check(dgop_sipdg_create(fes_.handle(), q_, d, plan_.ip_sigma, plan_.ip_kappa, 1, &op),
+                  "operator creation (" + plan_.describe() + ")");
+    op_ = std::shared_ptr<dgop_operator>(op, [](dgop_operator* o) { dgop_operator_destroy(o); });
+  }
+
   void create() {
     const CartesianMesh<D>& mesh = fes_.GetMesh();
     int64_t n[D];
@@ -1136,6 +1192,10 @@ class Operator {
       per[k] = mesh.is_periodic_boundary[k];
     }
     detail::Grid g = detail::make_grid(fes_.handle(), (int)D, n, per, q_);
+    if (plan_.diffusion) {
+      create_diffusion(g);
+      return;
+    }
     detail::Separated sig;
     dgop_coef sigma{};
     if (plan_.mass) {
@@ -1243,6 +1303,20 @@ Operator<D> MakeMassAdvectionOperator(const FiniteElementSpace<D>& fes, const In
   p.mass = p.cell = p.interior = true;
   p.sigma = detail::make_scalar(sigma, "sigma");
   p.beta = detail::make_vector(adv, "adv");
+  return Operator<D>(fes, ir, p);
+}
+
+// MakeDiffusionOperator<KP>(fes, ir, velocity, sigma, kappa) (diffusionoperator.hpp:554): the
+// legacy SIPDG operator with diffusivity velocity(X), penalty kappa / h, boundary faces included;
+// here the diffusivity must be constant on each element.
+template <typename KernelPolicy, Integer D, typename Velocity>
+Operator<D> MakeDiffusionOperator(const FiniteElementSpace<D>& fes, const IntegrationRule<D>& ir,
+                                  const Velocity& velocity, const Real sigma, const Real kappa) {
+  OperatorPlan p;
+  p.diffusion = true;
+  p.diffusivity = detail::make_scalar(velocity, "velocity");
+  p.ip_sigma = sigma;
+  p.ip_kappa = kappa;
   return Operator<D>(fes, ir, p);
 }
 

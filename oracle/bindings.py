@@ -154,6 +154,18 @@ class Reference(_Lib):
             raise NotImplementedError("sipdg_apply: case not instantiated")
         return y
 
+    def diffusion_legacy_apply(self, case, d, sigma, kappa, x):
+        """The reference's legacy MakeDiffusionOperator (part_sipdg.cpp): constant diffusivity d,
+        interior and boundary faces, tau = kappa / h."""
+        sizes, h, origin, periodic = self._mesh(case)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        rc = self.lib.gref_diffusion_legacy_apply(case["D"], case["P"], case["Q"], _p(sizes), _p(h), _p(origin),
+                                                  _p(periodic), _cd(d), _cd(sigma), _cd(kappa), _p(x), _p(y))
+        if rc != 0:
+            raise NotImplementedError("diffusion_legacy_apply: case not instantiated")
+        return y
+
     def time_advection(self, case, x, pairs):
         """Seconds per apply of the reference advection operator (inflow value case['g'])."""
         sizes, h, origin, _ = self._mesh(case)

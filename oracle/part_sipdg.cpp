@@ -57,9 +57,28 @@ void SipdgApply( const MeshArgs & m, const double * mu_elem, double sigma, doubl
    } );
 }
 
+// The reference's legacy SIPDG operator, MakeDiffusionOperator<KP>(fes, ir, velocity, sigma, kappa)
+// (FiniteElementMethod/MatrixFreeOperators/diffusionoperator.hpp:554): cell term, interior faces
+// and boundary faces, with a constant diffusivity `d` as the `velocity` function of X.
+template < int D, int P, int Q >
+void DiffusionLegacyApply( const MeshArgs & m, double d, double sigma, double kappa, const double * x, double * y )
+{
+   WithSpace< D, P, Q, 0 >( m, [&]( auto & fes, auto & ir )
+   {
+      const size_t n = fes.GetNumberOfFiniteElementDofs();
+      Vector vx( n ), vy( n );
+      CopyIn( vx, x );
+      auto diffusivity = [=] GENDIL_HOST_DEVICE ( std::array< Real, D > const & ) -> Real { return d; };
+      auto op = MakeDiffusionOperator< SerialKernelConfiguration >( fes, ir, diffusivity, sigma, kappa );
+      vy = 0.0;
+      op( vx, vy );
+      CopyOut( vy, y );
+   } );
+}
+
 }  // namespace gref
 
-#define GREF_SIPDG_LIST( X ) X( 2, 1, 3 ) X( 2, 2, 4 ) X( 3, 1, 3 ) X( 3, 2, 4 ) X( 3, 3, 5 ) X( 3, 4, 6 )
+#define GREF_SIPDG_LIST( X ) X( 1, 1, 4 ) X( 2, 1, 3 ) X( 2, 2, 4 ) X( 3, 1, 3 ) X( 3, 2, 4 ) X( 3, 3, 5 ) X( 3, 4, 6 )
 
 extern "C" int gref_sipdg_apply( int D, int P, int Q, const long * sizes, const double * h, const double * origin,
                                  const int * periodic, const double * mu_elem, double sigma, double kappa,
@@ -68,6 +87,18 @@ extern "C" int gref_sipdg_apply( int D, int P, int Q, const long * sizes, const 
    gref::MeshArgs m{ sizes, h, origin, periodic };
 #define X( d, p, q ) \
    if ( D == d && P == p && Q == q ) { gref::SipdgApply< d, p, q >( m, mu_elem, sigma, kappa, boundary, x, y ); return 0; }
+   GREF_SIPDG_LIST( X )
+#undef X
+   return gref::GREF_UNSUPPORTED;
+}
+
+extern "C" int gref_diffusion_legacy_apply( int D, int P, int Q, const long * sizes, const double * h,
+                                            const double * origin, const int * periodic, double d, double sigma,
+                                            double kappa, const double * x, double * y )
+{
+   gref::MeshArgs m{ sizes, h, origin, periodic };
+#define X( dd, p, q ) \
+   if ( D == dd && P == p && Q == q ) { gref::DiffusionLegacyApply< dd, p, q >( m, d, sigma, kappa, x, y ); return 0; }
    GREF_SIPDG_LIST( X )
 #undef X
    return gref::GREF_UNSUPPORTED;

@@ -278,6 +278,26 @@ int run_mode(const char* path) {
     std::printf("check H_fd %.6g\n", worst / gmax);
     record("H_grad_theta", grad_theta);
   }
+  {  // I: legacy interior-penalty diffusion, MakeDiffusionOperator(fes, ir, velocity, sigma, kappa):
+     // periodic 3^3, p = 2, q = 4, diffusivity 2.5, sigma = -1, kappa = 90 (golden case d4)
+    CartesianMesh<3> mesh({3, 3, 3}, {1.0 / 3, 1.0 / 3, 1.0 / 3}, {0.0, 0.0, 0.0}, true);
+    auto fes = MakeFiniteElementSpace(mesh, MakeLobattoFiniteElement(FiniteElementOrders<2, 2, 2>{}));
+    auto ir = MakeIntegrationRule(IntegrationRuleNumPoints<4, 4, 4>{});
+    auto velocity = [](const std::array<Real, 3>&) { return 2.5; };
+    Vector x(fes), y(fes);
+    FillRandom(x, 5);
+    auto A = MakeDiffusionOperator<KernelPolicy>(fes, ir, velocity, -1.0, 90.0);
+    A(x, y);
+    record("I_diffusion", y);
+    std::printf("check I_kernel_is_diffusion %d\n", A.KernelName() == "diffusion" ? 1 : 0);
+    auto varying = [](const std::array<Real, 3>& X) { return 1.0 + X[0]; };
+    try {
+      MakeDiffusionOperator<KernelPolicy>(fes, ir, varying, -1.0, 90.0);
+      std::printf("check I_rejects_varying 0\n");
+    } catch (const Error&) {
+      std::printf("check I_rejects_varying 1\n");
+    }
+  }
   std::fclose(g_out);
   return 0;
 }

@@ -120,6 +120,22 @@ def sipdg_cases():
     return c
 
 
+def diffusion_cases():
+    """The reference's legacy MakeDiffusionOperator (oracle/part_sipdg.cpp): constant diffusivity,
+    interior and boundary faces; the 1D case is the two-element periodic mesh of the reference's
+    tests/integration/gendil/test-diffusion-symmetry-1d-minimal.cpp (sigma = 1, kappa = 0)."""
+    c = []
+    c.append(("d1", dict(cube(1, 0, 1, 4, sizes=[2], periodic=[1]), diffusivity=1.0, sigma=1.0, kappa=0.0)))
+    c.append(("d2", dict(cube(1, 0, 1, 4, sizes=[7]), diffusivity=0.8, sigma=-1.0, kappa=40.0)))
+    c.append(("d3", dict(cube(2, 0, 1, 3, sizes=[5, 4]), diffusivity=1.0, sigma=1.0, kappa=0.0)))
+    c.append(("d4", dict(cube(3, 0, 2, 4, sizes=[3, 3, 3], periodic=[1, 1, 1]), diffusivity=2.5, sigma=-1.0,
+                         kappa=90.0)))
+    c.append(("d5", dict(cube(3, 0, 3, 5, sizes=[3, 2, 2]), diffusivity=0.7, sigma=0.0, kappa=160.0)))
+    c.append(("d6", dict(cube(3, 0, 4, 6, sizes=[2, 3, 2], h=[0.5, 0.25, 1 / 3]), diffusivity=1.3, sigma=-1.0,
+                         kappa=250.0)))
+    return c
+
+
 def main(only=None):
     """Write cases.json and golden.npz.  With `only` (a case kind), regenerate that kind alone and
     keep every other stored case and array as it is (the OpenMP reference solvers' last bits
@@ -130,8 +146,10 @@ def main(only=None):
         with np.load(os.path.join(HERE, "golden.npz")) as z:
             old_arrays = {k: z[k] for k in z.files}
         new_cases, new_arrays = build(only)
-        ids = {c["id"] for c in new_cases[only]}
-        old_cases[only] = new_cases[only]
+        kinds = [only] + (["diffusion"] if only == "sipdg" else [])
+        ids = {c["id"] for k in kinds for c in new_cases[k]}
+        for k in kinds:
+            old_cases[k] = new_cases[k]
         for k in list(old_arrays):
             if k.split("_")[0] in ids:
                 del old_arrays[k]
@@ -151,7 +169,7 @@ def write(cases, arrays):
 
 def build(only):
     ref = Reference()
-    cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": []}
+    cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": [], "diffusion": []}
     arrays = {}
     if only == "sipdg":
         sipdg_fixtures(ref, cases, arrays)
@@ -218,6 +236,11 @@ def sipdg_fixtures(ref, cases, arrays):
             grad[e] = lam @ ref.sipdg_apply(case, onehot, case["sigma"], kappa, case["boundary"], x)
         arrays[f"{cid}_grad"] = grad
         cases["sipdg"].append({"id": cid, **case, "grad_seed": 6})
+    for cid, case in diffusion_cases():
+        case = dict(case, seed=5)
+        x = ref.fill_random(num_dofs(case), case["seed"])
+        arrays[f"{cid}_y"] = ref.diffusion_legacy_apply(case, case["diffusivity"], case["sigma"], case["kappa"], x)
+        cases["diffusion"].append({"id": cid, **case})
 
 
 if __name__ == "__main__":

@@ -138,3 +138,7 @@ def test_facade_operators_and_solvers_match_the_oracle(facade_bin, tmp_path):
     # adjoint gradient (AdvectionSolveFunction) against central differences
     assert solves["H_forward"]["success"] and solves["H_adjoint"]["success"]
     assert checks["H_fd"] <= 1e-6
+
+    # legacy diffusion operator (MakeDiffusionOperator) against the reference's own output
+    assert rel_max(vec["I_diffusion"], arr["d4_y"]) <= APPLY_TOL
+    assert checks["I_kernel_is_diffusion"] == 1 and checks["I_rejects_varying"] == 1

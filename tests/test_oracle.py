@@ -75,3 +75,29 @@ def test_oracle_vs_live_reference_advection_16():
             "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "seed": 1}
     x = inputs(case)
     assert rel_max(oracle().advection_apply(case, x, 1), Reference().advection_apply(case, x, 1)) <= APPLY_TOL
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference library not built here")
+@pytest.mark.parametrize("case", CASES["sipdg"], ids=lambda c: c["id"])
+def test_sipdg_fixtures_reproduce_live_reference(case):
+    """The stored SIPDG fixtures are what the reference's generic weak form computes here."""
+    from helpers import Reference
+    ref = Reference()
+    y = ref.sipdg_apply(case, ARR[f"{case['id']}_mu"], case["sigma"], case["kappa"], case["boundary"], inputs(case))
+    assert rel_max(y, ARR[f"{case['id']}_y"]) <= 1e-14
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference library not built here")
+@pytest.mark.parametrize("case", CASES["diffusion"], ids=lambda c: c["id"])
+def test_legacy_diffusion_equals_generic_sipdg(case):
+    """The reference's legacy MakeDiffusionOperator and its generic SIPDG weak form (constant
+    diffusivity, boundary terms on) agree, as the reference's own diffusion tests check, and the
+    stored fixture is the legacy operator's output."""
+    from helpers import Reference
+    ref = Reference()
+    x = inputs(case)
+    ne = int(np.prod(case["sizes"]))
+    legacy = ref.diffusion_legacy_apply(case, case["diffusivity"], case["sigma"], case["kappa"], x)
+    generic = ref.sipdg_apply(case, np.full(ne, case["diffusivity"]), case["sigma"], case["kappa"], 1, x)
+    assert rel_max(legacy, ARR[f"{case['id']}_y"]) <= 1e-14
+    assert rel_max(generic, legacy) <= 1e-13

@@ -127,3 +127,20 @@ def test_loss_gradient_vs_central_differences():
         zm[e] -= eps
         fd = (loss(zp).item() - loss(zm).item()) / (2 * eps)
         assert abs(fd - grad[e].item()) <= 1e-5 * max(1.0, abs(grad).max().item()), (e, fd, grad[e].item())
+
+
+@pytest.mark.parametrize("case", CASES["diffusion"], ids=lambda c: c["id"])
+def test_legacy_diffusion_operator_vs_reference_golden(case):
+    """DiffusionOperator against the reference's legacy MakeDiffusionOperator (constant diffusivity,
+    interior and boundary faces), including the two-element periodic 1D mesh of the reference's
+    symmetry test and sigma = 1, 0, -1."""
+    sp = make_space(case)
+    op = g.DiffusionOperator(sp, case["Q"], case["diffusivity"], case["sigma"], case["kappa"])
+    x = torch.tensor(inputs(case), device="cuda")
+    y = torch.empty_like(x)
+    op(x, y)
+    assert rel_max(y.cpu().numpy(), ARR[f"{case['id']}_y"]) <= APPLY_TOL
+    if case["sigma"] == -1.0:
+        yt = torch.empty_like(x)
+        op.apply_transpose(x, yt)
+        assert torch.equal(yt, y)
