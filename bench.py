@@ -288,6 +288,21 @@ def run_ours(args):
     ms_step = ms / args.steps
     value = reps.throughput(nd * args.steps, ms) / 1e9
 
+    # the speed-of-light operator (y = x element by element, MakeSpeedOfLightOperator) on the same
+    # vectors: the in-framework bandwidth reference of an apply
+    sol = g.SpeedOfLightOperator(space)
+    for _ in range(args.warmup):
+        sol(x, y)
+    barrier()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        sol(x, y)
+    s1.record(stream)
+    barrier()
+    sol.close()
+    ms_sol = reps.max(s0.elapsed_time(s1)) / args.steps
+
     # end to end through the C ABI on host vectors (dgop_host_io_apply): pinned host input ->
     # device -> apply -> host result, upload / apply / download pipelined over slabs of z planes
     xh = torch.from_numpy(x_np).pin_memory()
@@ -328,7 +343,12 @@ def run_ours(args):
                         "d2h_bytes_per_step": 8 * nd, "steps": e_steps,
                         "path": f"dgop_host_io_apply (pinned host vectors, {HOST_SLABS} slabs)"},
                 "gpu_launches": args.steps,
-                "clocks": clocks.summary()}
+                "clocks": clocks.summary(),
+                "speed_of_light": {"ms_per_apply": ms_sol, "gdofs_per_s": nd / (ms_sol * 1e-3) / 1e9,
+                                   "gbs": 16.0 * nd / (ms_sol * 1e-3) / 1e9,
+                                   "frac_of_measured_hbm": 16.0 * nd / (ms_sol * 1e-3) / 1e9 / hbm,
+                                   "apply_time_over_copy_time": ms_step / ms_sol,
+                                   "note": "SpeedOfLightOperator (y = x, 16 B/DoF) on the same vectors, same steps"}}
         if op.kernel in ("kron", "kronnd"):
             # FP64 work: D^2 n x n passes (D terms x D axes), n FMA per DoF each, 2 flop per FMA
             D, n = space.dim, space.order + 1

@@ -25,7 +25,7 @@ import numpy as np
 from .coefficients import Coefficient, as_coefficient
 
 __all__ = ["Space", "MassOperator", "AdvectionOperator", "MassAdvectionOperator", "SystemOperator",
-           "SIPDGOperator", "DiffusionOperator", "MassInverseOperator", "CGSolver", "GMRESSolver", "GMRESIRSolver",
+           "SIPDGOperator", "DiffusionOperator", "MassInverseOperator", "SpeedOfLightOperator", "CGSolver", "GMRESSolver", "GMRESIRSolver",
            "Batch", "HostIO", "element_dot", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL",
            "BC_NONE", "BC_INFLOW"]
 
@@ -101,6 +101,7 @@ def lib():
         L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
         L.dgop_element_dot.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_sipdg_gradient.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.dgop_speed_of_light_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_batch_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
         L.dgop_batch_groups.argtypes = [vp]
@@ -246,7 +247,7 @@ class _Operator:
     def kernel(self):
         """'generic' (sum-factorized), 'kron' (register-resident 3D Kronecker form) or 'kronnd'
         (shared-memory Kronecker form, any dimension)."""
-        return ("generic", "kron", "kronnd", "diffusion")[lib().dgop_operator_kernel(self.handle)]
+        return ("generic", "kron", "kronnd", "diffusion", "copy")[lib().dgop_operator_kernel(self.handle)]
 
     @property
     def kernel_note(self):
@@ -344,6 +345,17 @@ class DiffusionOperator(SIPDGOperator):
         else:
             mu = diffusivity
         super().__init__(space, q, mu, sigma=sigma, kappa=kappa, boundary=True)
+
+
+class SpeedOfLightOperator(_Operator):
+    """y = x element by element (MakeSpeedOfLightOperator, speedoflightoperator.hpp:198): the
+    bandwidth reference of an apply (16 B/DoF in FP64)."""
+
+    def __init__(self, space, q=1):
+        super().__init__(space, q)
+        h = ctypes.c_void_p()
+        check(lib().dgop_speed_of_light_create(space.handle, q, ctypes.byref(h)))
+        self.handle = h
 
 
 class MassInverseOperator(_Operator):

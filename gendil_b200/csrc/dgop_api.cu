@@ -8,6 +8,7 @@
 #include <new>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "basis.h"
@@ -828,6 +829,47 @@ int create_operator(const dgop_space* space, int q, const dgop_coef* sigma, cons
 
 }  // namespace
 
+// y[i] = alpha x[i] (+ beta_y y[i]) for i in [i0, i1): the speed-of-light operator.  The body
+// moves 16-byte vectors (x and y equally aligned: the copy starts with the scalar head that
+// reaches a 16-byte boundary of y); the scalar path covers the rest.
+template <typename Real>
+__global__ void __launch_bounds__(256) copy_kernel(const Real* __restrict__ x, Real* __restrict__ y, int64_t i0,
+                                                   int64_t i1, Real alpha, Real beta_y, const int* skip) {
+  if (skip && *skip) return;
+  constexpr int V = 16 / sizeof(Real);
+  using Vec = typename std::conditional<sizeof(Real) == 8, double2, float4>::type;
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  const bool same = ((reinterpret_cast<uintptr_t>(x) ^ reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+  int64_t head = i0;
+  if (same) {
+    while (head < i1 && (reinterpret_cast<uintptr_t>(y + head) & 15)) ++head;
+  } else {
+    head = i1;  // all scalar
+  }
+  for (int64_t i = i0 + tid; i < head; i += nth) y[i] = beta_y == Real(0) ? alpha * x[i] : alpha * x[i] + beta_y * y[i];
+  const int64_t nvec = (i1 - head) / V;
+  const Vec* xv = reinterpret_cast<const Vec*>(x + head);
+  Vec* yv = reinterpret_cast<Vec*>(y + head);
+  for (int64_t k = tid; k < nvec; k += nth) {
+    Vec a = xv[k];
+    Real* pa = reinterpret_cast<Real*>(&a);
+    if (beta_y == Real(0)) {
+      if (alpha != Real(1))
+#pragma unroll
+        for (int j = 0; j < V; ++j) pa[j] *= alpha;
+    } else {
+      Vec b = yv[k];
+      const Real* pb = reinterpret_cast<const Real*>(&b);
+#pragma unroll
+      for (int j = 0; j < V; ++j) pa[j] = alpha * pa[j] + beta_y * pb[j];
+    }
+    yv[k] = a;
+  }
+  for (int64_t i = head + nvec * V + tid; i < i1; i += nth)
+    y[i] = beta_y == Real(0) ? alpha * x[i] : alpha * x[i] + beta_y * y[i];
+}
+
 template <typename Real>
 static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, KronNDCfg<Real>& KN,
                        KronDiffCfg<Real>& SD, Real alpha, const Real* x, Real beta_y, Real* y, int extra_flags,
@@ -855,6 +897,18 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
   }
   const bool linear = (extra_flags & kLinear) != 0;
   extra_flags &= ~kLinear;
+  if (op->kernel == DGOP_KERNEL_COPY) {
+    const int64_t nd = op->sp.ndofs / op->sp.nelem;
+    const int64_t i0 = e_begin * nd, i1 = e_end * nd;
+    if (i1 > i0) {
+      const int64_t blocks =
+          std::max<int64_t>(1, std::min<int64_t>((int64_t)device_sms(op->device) * 8, (i1 - i0 + 2047) / 2048));
+      copy_kernel<Real><<<(unsigned)blocks, 256, 0, s>>>(x, y, i0, i1, alpha, beta_y, skip);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "speed-of-light kernel launch");
+    }
+    return DGOP_OK;
+  }
   if (op->kernel == DGOP_KERNEL_DIFF) {
     if (!SD.ready) {
       set_error("the diffusion operator has no kernel for this precision");
@@ -1042,6 +1096,27 @@ int dgop_space_coordinates(const dgop_space* space, int q, int axis, double* coo
 
 int dgop_mass_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out) {
   return create_operator(space, q, sigma, nullptr, kMass, 0.0, out);
+}
+
+int dgop_speed_of_light_create(const dgop_space* space, int q, dgop_operator** out) {
+  if (!space || !out) {
+    set_error("dgop_speed_of_light_create: null argument");
+    return DGOP_ERR_ARG;
+  }
+  *out = nullptr;
+  auto* op = new (std::nothrow) dgop_operator();
+  if (!op) {
+    set_error("host allocation failed");
+    return DGOP_ERR_ALLOC;
+  }
+  op->sp = *space;
+  op->q = q;
+  op->flags = 0;
+  op->kernel = DGOP_KERNEL_COPY;
+  op->kron_why = "speed-of-light copy";
+  cudaGetDevice(&op->device);
+  *out = op;
+  return DGOP_OK;
 }
 
 int dgop_mass_inverse_create(const dgop_space* space, int q, const dgop_coef* sigma, dgop_operator** out) {

@@ -97,6 +97,12 @@ int dgop_sipdg_create(const dgop_space* space, int q, const double* mu, double s
  *                  dJ/dmu_e = -out[e].  One launch, deterministic.  No reference counterpart. */
 int dgop_sipdg_gradient(const dgop_operator* op, const double* u, const double* lambda, const double* scale,
                         double* out, void* stream);
+/* speed_of_light:  y = x read and written element by element (SpeedOfLightOperator,
+ *                  MakeSpeedOfLightOperator, FiniteElementMethod/MatrixFreeOperators/
+ *                  speedoflightoperator.hpp:198): the bandwidth reference of an apply, 16 B/DoF in
+ *                  FP64; 128-bit loads and stores, a grid of a multiple of the SM count (kernel
+ *                  DGOP_KERNEL_COPY; transpose and FP32 the same copy; q is not used). */
+int dgop_speed_of_light_create(const dgop_space* space, int q, dgop_operator** out);
 int dgop_operator_destroy(dgop_operator* op);
 int64_t dgop_operator_num_dofs(const dgop_operator* op);
 
@@ -108,7 +114,13 @@ int64_t dgop_operator_num_dofs(const dgop_operator* op);
  * (GLL, separable coefficients, element within shared memory), chosen when the register kernel
  * does not apply.
  * dgop_operator_kernel_note() says why the Kronecker form was not chosen. */
-enum dgop_kernel { DGOP_KERNEL_GENERIC = 0, DGOP_KERNEL_KRON = 1, DGOP_KERNEL_KRONND = 2, DGOP_KERNEL_DIFF = 3 };
+enum dgop_kernel {
+  DGOP_KERNEL_GENERIC = 0,
+  DGOP_KERNEL_KRON = 1,
+  DGOP_KERNEL_KRONND = 2,
+  DGOP_KERNEL_DIFF = 3,
+  DGOP_KERNEL_COPY = 4
+};
 int dgop_operator_kernel(const dgop_operator* op);
 const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);

@@ -900,10 +900,12 @@ struct OperatorPlan {
   const Real* beta_factor = nullptr;  // per-element velocity factor (device, num_elements; null: 1)
   // interior-penalty diffusion (MakeDiffusionOperator): diffusivity constant on each element
   bool diffusion = false;
+  bool speed_of_light = false;  // y = x (MakeSpeedOfLightOperator)
   std::shared_ptr<const detail::ScalarField> diffusivity;
   Real ip_sigma = -1.0, ip_kappa = 0.0;
   std::string describe() const {
     if (diffusion) return "interior-penalty diffusion, diffusivity=" + (diffusivity ? diffusivity->name : "?");
+    if (speed_of_light) return "speed of light (copy)";
     std::ostringstream s;
     s << (mass ? "mass" : "") << (mass && cell ? "+" : "") << (cell ? "cell" : "") << (interior ? "+interior" : "")
       << (boundary ? "+boundary" : "");
@@ -1105,9 +1107,9 @@ class Operator {
   dgop_operator* handle() const { return op_.get(); }
   const OperatorPlan& plan() const { return plan_; }
   std::string KernelName() const {
-    static const char* const names[] = {"generic", "kron", "kronnd", "diffusion"};
+    static const char* const names[] = {"generic", "kron", "kronnd", "diffusion", "copy"};
     const int k = dgop_operator_kernel(op_.get());
-    return (k >= 0 && k < 4) ? names[k] : "unknown";
+    return (k >= 0 && k < 5) ? names[k] : "unknown";
   }
 
   // device-resident solvers, created once per (kind, restart, inner precision); kind 0 CG,
@@ -1190,6 +1192,12 @@ class Operator {
     for (Integer k = 0; k < D; ++k) {
       n[k] = (int64_t)mesh.sizes[k];
       per[k] = mesh.is_periodic_boundary[k];
+    }
+    if (plan_.speed_of_light) {
+      dgop_operator* op = nullptr;
+      detail::check(dgop_speed_of_light_create(fes_.handle(), q_, &op), "operator creation (speed of light)");
+      op_ = std::shared_ptr<dgop_operator>(op, [](dgop_operator* o) { dgop_operator_destroy(o); });
+      return;
     }
     detail::Grid g = detail::make_grid(fes_.handle(), (int)D, n, per, q_);
     if (plan_.diffusion) {
@@ -1317,6 +1325,15 @@ Operator<D> MakeDiffusionOperator(const FiniteElementSpace<D>& fes, const Integr
   p.diffusivity = detail::make_scalar(velocity, "velocity");
   p.ip_sigma = sigma;
   p.ip_kappa = kappa;
+  return Operator<D>(fes, ir, p);
+}
+
+// MakeSpeedOfLightOperator<KP>(fes, ir) (speedoflightoperator.hpp:198): y = x element by
+// element, the bandwidth reference of an apply.
+template <typename KernelPolicy, Integer D>
+Operator<D> MakeSpeedOfLightOperator(const FiniteElementSpace<D>& fes, const IntegrationRule<D>& ir) {
+  OperatorPlan p;
+  p.speed_of_light = true;
   return Operator<D>(fes, ir, p);
 }
 

@@ -298,6 +298,18 @@ int run_mode(const char* path) {
       std::printf("check I_rejects_varying 1\n");
     }
   }
+  {  // J: speed-of-light operator (y = x), 2D 5 x 4, p = 3
+    CartesianMesh<2> mesh({5, 4}, {0.2, 0.25}, {0.0, 0.0});
+    auto fes = MakeFiniteElementSpace(mesh, MakeLobattoFiniteElement(FiniteElementOrders<3, 3>{}));
+    auto ir = MakeIntegrationRule(IntegrationRuleNumPoints<4, 4>{});
+    Vector x(fes), y(fes);
+    FillRandom(x, 3);
+    auto sol = MakeSpeedOfLightOperator<KernelPolicy>(fes, ir);
+    sol(x, y);
+    bool same = true;
+    for (Integer i = 0; i < x.Size(); ++i) same = same && (x[i] == y[i]);
+    std::printf("check J_copy_exact %d\n", same ? 1 : 0);
+  }
   std::fclose(g_out);
   return 0;
 }

@@ -142,3 +142,4 @@ def test_facade_operators_and_solvers_match_the_oracle(facade_bin, tmp_path):
     # legacy diffusion operator (MakeDiffusionOperator) against the reference's own output
     assert rel_max(vec["I_diffusion"], arr["d4_y"]) <= APPLY_TOL
     assert checks["I_kernel_is_diffusion"] == 1 and checks["I_rejects_varying"] == 1
+    assert checks["J_copy_exact"] == 1

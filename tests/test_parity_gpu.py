@@ -268,3 +268,34 @@ def test_kronnd_variants(cid, case, kind, mode):
     assert tried >= 1
     op.set_variant(None)
     assert op.variant in op.ND_VARIANTS
+
+
+def test_speed_of_light_operator_copies_exactly():
+    """SpeedOfLightOperator: y = x bit for bit (16-byte vectors and the unaligned scalar path),
+    alpha / beta, FP32 and the host-vector path."""
+    import torch
+    import gendil_b200 as g
+    sp = g.Space(3, [5, 4, 3], order=2)
+    op = g.SpeedOfLightOperator(sp, 3)
+    assert op.kernel == "copy"
+    n = sp.num_dofs
+    base = torch.rand(n + 3, dtype=torch.float64, device="cuda")
+    for off in (0, 1):
+        x = base[off:off + n]
+        y = torch.full((n + 3,), float("nan"), dtype=torch.float64, device="cuda")[off:off + n]
+        op(x, y)
+        assert torch.equal(x, y), off
+    x = base[:n].contiguous()
+    y0 = torch.rand(n, dtype=torch.float64, device="cuda")
+    y = y0.clone()
+    op.apply(x, y, alpha=2.0, beta=-0.5)
+    assert torch.equal(y, 2.0 * x - 0.5 * y0)
+    x32, y32 = x.float(), torch.empty(n, dtype=torch.float32, device="cuda")
+    op.apply_f32(x32, y32)
+    assert torch.equal(x32, y32)
+    io = g.HostIO(op, slabs=3)
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    io.apply(xh, yh)
+    assert torch.equal(xh, yh)
+    io.close()
