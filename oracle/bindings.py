@@ -148,7 +148,8 @@ class Reference(_Lib):
         x = np.ascontiguousarray(x, dtype=np.float64)
         mu = np.ascontiguousarray(mu_elem, dtype=np.float64)
         y = np.zeros_like(x)
-        rc = self.lib.gref_sipdg_apply(case["D"], case["P"], case["Q"], _p(sizes), _p(h), _p(origin), _p(periodic),
+        rc = self.lib.gref_sipdg_apply(case["D"], case["P"], case["Q"], case.get("basis", 0), _p(sizes), _p(h),
+                                       _p(origin), _p(periodic),
                                        _p(mu), _cd(sigma), _cd(kappa), int(boundary), _p(x), _p(y))
         if rc != 0:
             raise NotImplementedError("sipdg_apply: case not instantiated")
@@ -160,8 +161,8 @@ class Reference(_Lib):
         sizes, h, origin, periodic = self._mesh(case)
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.zeros_like(x)
-        rc = self.lib.gref_diffusion_legacy_apply(case["D"], case["P"], case["Q"], _p(sizes), _p(h), _p(origin),
-                                                  _p(periodic), _cd(d), _cd(sigma), _cd(kappa), _p(x), _p(y))
+        rc = self.lib.gref_diffusion_legacy_apply(case["D"], case["P"], case["Q"], case.get("basis", 0), _p(sizes),
+                                                  _p(h), _p(origin), _p(periodic), _cd(d), _cd(sigma), _cd(kappa), _p(x), _p(y))
         if rc != 0:
             raise NotImplementedError("diffusion_legacy_apply: case not instantiated")
         return y

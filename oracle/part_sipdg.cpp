@@ -7,11 +7,11 @@
 
 namespace gref {
 
-template < int D, int P, int Q >
+template < int D, int P, int Q, int Basis >
 void SipdgApply( const MeshArgs & m, const double * mu_elem, double sigma, double kappa, int boundary,
                  const double * x, double * y )
 {
-   WithSpace< D, P, Q, 0 >( m, [&]( auto & fes, auto & ir )
+   WithSpace< D, P, Q, Basis >( m, [&]( auto & fes, auto & ir )
    {
       const size_t n = fes.GetNumberOfFiniteElementDofs();
       const size_t ne = fes.GetNumberOfFiniteElements();
@@ -60,10 +60,10 @@ void SipdgApply( const MeshArgs & m, const double * mu_elem, double sigma, doubl
 // The reference's legacy SIPDG operator, MakeDiffusionOperator<KP>(fes, ir, velocity, sigma, kappa)
 // (FiniteElementMethod/MatrixFreeOperators/diffusionoperator.hpp:554): cell term, interior faces
 // and boundary faces, with a constant diffusivity `d` as the `velocity` function of X.
-template < int D, int P, int Q >
+template < int D, int P, int Q, int Basis >
 void DiffusionLegacyApply( const MeshArgs & m, double d, double sigma, double kappa, const double * x, double * y )
 {
-   WithSpace< D, P, Q, 0 >( m, [&]( auto & fes, auto & ir )
+   WithSpace< D, P, Q, Basis >( m, [&]( auto & fes, auto & ir )
    {
       const size_t n = fes.GetNumberOfFiniteElementDofs();
       Vector vx( n ), vy( n );
@@ -78,27 +78,38 @@ void DiffusionLegacyApply( const MeshArgs & m, double d, double sigma, double ka
 
 }  // namespace gref
 
-#define GREF_SIPDG_LIST( X ) X( 1, 1, 4 ) X( 2, 1, 3 ) X( 2, 2, 4 ) X( 3, 1, 3 ) X( 3, 2, 4 ) X( 3, 3, 5 ) X( 3, 4, 6 )
+// (dimension, order, points, basis: 0 GLL, 1 GL)
+#define GREF_SIPDG_LIST( X )                                                                          \
+   X( 1, 1, 4, 0 ) X( 2, 1, 3, 0 ) X( 2, 2, 4, 0 ) X( 3, 1, 3, 0 ) X( 3, 2, 4, 0 ) X( 3, 3, 5, 0 ) \
+   X( 3, 4, 6, 0 ) X( 2, 2, 4, 1 ) X( 3, 2, 4, 1 ) X( 4, 1, 3, 0 )
 
-extern "C" int gref_sipdg_apply( int D, int P, int Q, const long * sizes, const double * h, const double * origin,
-                                 const int * periodic, const double * mu_elem, double sigma, double kappa,
-                                 int boundary, const double * x, double * y )
+extern "C" int gref_sipdg_apply( int D, int P, int Q, int basis, const long * sizes, const double * h,
+                                 const double * origin, const int * periodic, const double * mu_elem, double sigma,
+                                 double kappa, int boundary, const double * x, double * y )
 {
    gref::MeshArgs m{ sizes, h, origin, periodic };
-#define X( d, p, q ) \
-   if ( D == d && P == p && Q == q ) { gref::SipdgApply< d, p, q >( m, mu_elem, sigma, kappa, boundary, x, y ); return 0; }
+#define X( d, p, q, b )                                                                         \
+   if ( D == d && P == p && Q == q && basis == b )                                              \
+   {                                                                                           \
+      gref::SipdgApply< d, p, q, b >( m, mu_elem, sigma, kappa, boundary, x, y );              \
+      return 0;                                                                                \
+   }
    GREF_SIPDG_LIST( X )
 #undef X
    return gref::GREF_UNSUPPORTED;
 }
 
-extern "C" int gref_diffusion_legacy_apply( int D, int P, int Q, const long * sizes, const double * h,
+extern "C" int gref_diffusion_legacy_apply( int D, int P, int Q, int basis, const long * sizes, const double * h,
                                             const double * origin, const int * periodic, double d, double sigma,
                                             double kappa, const double * x, double * y )
 {
    gref::MeshArgs m{ sizes, h, origin, periodic };
-#define X( dd, p, q ) \
-   if ( D == dd && P == p && Q == q ) { gref::DiffusionLegacyApply< dd, p, q >( m, d, sigma, kappa, x, y ); return 0; }
+#define X( dd, p, q, b )                                                                        \
+   if ( D == dd && P == p && Q == q && basis == b )                                             \
+   {                                                                                           \
+      gref::DiffusionLegacyApply< dd, p, q, b >( m, d, sigma, kappa, x, y );                   \
+      return 0;                                                                                \
+   }
    GREF_SIPDG_LIST( X )
 #undef X
    return gref::GREF_UNSUPPORTED;

@@ -117,6 +117,10 @@ def sipdg_cases():
     c.append(("s5", dict(cube(3, 0, 3, 5, sizes=[3, 2, 2]), sigma=1.0, boundary=1)))
     c.append(("s6", dict(cube(3, 0, 4, 6, sizes=[2, 3, 2]), sigma=-1.0, boundary=1)))
     c.append(("s7", dict(cube(3, 0, 4, 6, sizes=[3, 2, 2], h=[0.2, 0.5, 0.25]), sigma=0.0, boundary=1)))
+    # Gauss-Legendre nodes (the traces are full contractions, not end values) and a 4D mesh
+    c.append(("s8", dict(cube(2, 0, 2, 4, basis=1, sizes=[4, 3]), sigma=-1.0, boundary=1)))
+    c.append(("s9", dict(cube(3, 0, 2, 4, basis=1, sizes=[3, 2, 3], periodic=[0, 1, 0]), sigma=1.0, boundary=1)))
+    c.append(("s10", dict(cube(4, 0, 1, 3, sizes=[3, 2, 3, 2], periodic=[0, 0, 1, 0]), sigma=-1.0, boundary=1)))
     return c
 
 
@@ -133,6 +137,7 @@ def diffusion_cases():
     c.append(("d5", dict(cube(3, 0, 3, 5, sizes=[3, 2, 2]), diffusivity=0.7, sigma=0.0, kappa=160.0)))
     c.append(("d6", dict(cube(3, 0, 4, 6, sizes=[2, 3, 2], h=[0.5, 0.25, 1 / 3]), diffusivity=1.3, sigma=-1.0,
                          kappa=250.0)))
+    c.append(("d7", dict(cube(3, 0, 2, 4, basis=1, sizes=[3, 3, 2]), diffusivity=0.9, sigma=-1.0, kappa=90.0)))
     return c
 
 
