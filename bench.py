@@ -36,7 +36,7 @@ WORKLOAD = "fp64 upwind DG advection apply, 3D 64^3 hex, p=3 GLL, q=4 GL, sin/co
 WORKLOAD_6D = ("fp64 upwind DG advection apply, 6D phase space 8^6 hypercubes on [0,1]^3 x [-1,1]^3, p=2 GLL, "
                "q=3 GL, beta = (v, -x + 0.5), inflow 0")
 FALLBACK_HBM_GBS = 6650.0
-HOST_SLABS = 16  # pipeline depth of the host-vector apply (slabs of z planes)
+HOST_SLABS = 4  # slabs of z planes per host-vector apply (consecutive steps overlap, so few slabs suffice)
 # DRAM bytes (read + write) of one launch measured by ncu on the 64^3 workload, by kernel family
 TRAFFIC_BYTES = {("kron", 64): 221.3e6}
 
@@ -303,8 +303,10 @@ def run_ours(args):
     sol.close()
     ms_sol = reps.max(s0.elapsed_time(s1)) / args.steps
 
-    # end to end through the C ABI on host vectors (dgop_host_io_apply): pinned host input ->
-    # device -> apply -> host result, upload / apply / download pipelined over slabs of z planes
+    # end to end through the C ABI on host vectors: every step uploads its input from pinned host
+    # memory, applies and downloads its result (dgop_host_io_apply_async: upload / apply /
+    # download pipelined over slabs of z planes, and one step's uploads overlapping the previous
+    # step's downloads); the timed region ends when the last result is in host memory
     xh = torch.from_numpy(x_np).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
     io = g.HostIO(op, slabs=HOST_SLABS)
@@ -315,7 +317,8 @@ def run_ours(args):
     e_steps = max(3, min(args.steps, 20))
     e0.record(stream)
     for _ in range(e_steps):
-        io.apply(xh, yh, stream)
+        io.apply_async(xh, yh, stream)
+    io.wait(stream)
     e1.record(stream)
     barrier()
     io.close()
@@ -341,7 +344,8 @@ def run_ours(args):
                              "algorithmic_bytes_per_launch": alg_bytes},
                 "e2e": {"value": e2e_value, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * nd,
                         "d2h_bytes_per_step": 8 * nd, "steps": e_steps,
-                        "path": f"dgop_host_io_apply (pinned host vectors, {HOST_SLABS} slabs)"},
+                        "path": f"dgop_host_io_apply_async + dgop_host_io_wait (pinned host vectors, {HOST_SLABS} slabs, "
+                                "consecutive steps overlapped)"},
                 "gpu_launches": args.steps,
                 "clocks": clocks.summary(),
                 "speed_of_light": {"ms_per_apply": ms_sol, "gdofs_per_s": nd / (ms_sol * 1e-3) / 1e9,

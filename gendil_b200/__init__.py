@@ -103,6 +103,8 @@ def lib():
         L.dgop_sipdg_gradient.argtypes = [vp, vp, vp, vp, vp, vp]
         L.dgop_speed_of_light_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_host_io_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.dgop_host_io_apply_async.argtypes = [vp, vp, vp, vp]
+        L.dgop_host_io_wait.argtypes = [vp, vp]
         L.dgop_batch_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
         L.dgop_batch_groups.argtypes = [vp]
         L.dgop_batch_apply.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
@@ -535,6 +537,16 @@ class HostIO:
 
     def apply(self, x, y, stream=None):
         check(lib().dgop_host_io_apply(self.handle, self._host_ptr(x), self._host_ptr(y), _stream(stream)))
+
+    def apply_async(self, x, y, stream=None):
+        """Queue y = A x and return (dgop_host_io_apply_async): consecutive calls overlap one
+        apply's uploads with the previous one's downloads.  x and y must stay alive and untouched
+        until wait() has been called and the stream synchronized."""
+        check(lib().dgop_host_io_apply_async(self.handle, self._host_ptr(x), self._host_ptr(y), _stream(stream)))
+
+    def wait(self, stream=None):
+        """Make `stream` wait for every queued asynchronous apply (dgop_host_io_wait)."""
+        check(lib().dgop_host_io_wait(self.handle, _stream(stream)))
 
     def close(self):
         if self.handle:

@@ -8,6 +8,12 @@
 // result of slab k goes back on a third stream as soon as its apply is done.  Upload and download
 // use the two copy directions at once, so a host apply costs about one transfer of the vector
 // instead of two.
+//
+// The device copies are double-buffered: consecutive asynchronous applies alternate between two
+// (x, y) pairs, so the uploads of one apply run while the downloads of the previous one finish.
+// An apply waits only for what reuses its buffers: its uploads for the applies that read the
+// pair two calls earlier, its applies for the downloads of that call; and its uploads for the
+// downloads of an earlier call whose result vector overlaps its input (chained applies).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,8 +26,12 @@ using namespace dgop;
 
 struct dgop_host_io {
   dgop_operator* op = nullptr;
-  double* x = nullptr;  // device copies of the input and the result
-  double* y = nullptr;
+  double* x[2] = {nullptr, nullptr};  // device copies of the input and the result, two pairs
+  double* y[2] = {nullptr, nullptr};
+  cudaEvent_t read_done[2] = {nullptr, nullptr};  // the last applies that read x[b]
+  cudaEvent_t sent[2] = {nullptr, nullptr};       // the last downloads of y[b]
+  unsigned calls = 0;
+  const double* y_host[2] = {nullptr, nullptr};  // result vector of the last call on pair b
   cudaStream_t up = nullptr, run = nullptr, down = nullptr;
   cudaEvent_t start = nullptr, finished = nullptr;
   std::vector<cudaEvent_t> uploaded, applied;
@@ -43,8 +53,12 @@ namespace {
   } while (0)
 
 void release(dgop_host_io* io) {
-  if (io->x) cudaFree(io->x);
-  if (io->y) cudaFree(io->y);
+  for (int b = 0; b < 2; ++b) {
+    if (io->x[b]) cudaFree(io->x[b]);
+    if (io->y[b]) cudaFree(io->y[b]);
+    if (io->read_done[b]) cudaEventDestroy(io->read_done[b]);
+    if (io->sent[b]) cudaEventDestroy(io->sent[b]);
+  }
   for (cudaStream_t s : {io->up, io->run, io->down})
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t e : {io->start, io->finished})
@@ -62,8 +76,12 @@ int setup(dgop_host_io* io, int slabs) {
   const int64_t per_plane = sp.nelem / planes;
   const int k = (int)std::max<int64_t>(1, std::min<int64_t>(slabs, planes));
   for (int i = 0; i <= k; ++i) io->first.push_back(per_plane * ((planes * i) / k));
-  DGOP_CUDA_H(cudaMalloc(&io->x, sizeof(double) * sp.ndofs));
-  DGOP_CUDA_H(cudaMalloc(&io->y, sizeof(double) * sp.ndofs));
+  for (int b = 0; b < 2; ++b) {
+    DGOP_CUDA_H(cudaMalloc(&io->x[b], sizeof(double) * sp.ndofs));
+    DGOP_CUDA_H(cudaMalloc(&io->y[b], sizeof(double) * sp.ndofs));
+    DGOP_CUDA_H(cudaEventCreateWithFlags(&io->read_done[b], cudaEventDisableTiming));
+    DGOP_CUDA_H(cudaEventCreateWithFlags(&io->sent[b], cudaEventDisableTiming));
+  }
   DGOP_CUDA_H(cudaStreamCreateWithFlags(&io->up, cudaStreamNonBlocking));
   DGOP_CUDA_H(cudaStreamCreateWithFlags(&io->run, cudaStreamNonBlocking));
   DGOP_CUDA_H(cudaStreamCreateWithFlags(&io->down, cudaStreamNonBlocking));
@@ -104,7 +122,7 @@ int dgop_host_io_create(dgop_operator* op, int slabs, dgop_host_io** out) {
   return DGOP_OK;
 }
 
-int dgop_host_io_apply(dgop_host_io* io, const double* x_host, double* y_host, void* stream) {
+int dgop_host_io_apply_async(dgop_host_io* io, const double* x_host, double* y_host, void* stream) {
   if (!io || !x_host || !y_host) {
     set_error("dgop_host_io_apply: null argument");
     return DGOP_ERR_ARG;
@@ -115,26 +133,56 @@ int dgop_host_io_apply(dgop_host_io* io, const double* x_host, double* y_host, v
   const bool faces = (io->op->flags & (kFaceInt | kFaceBnd)) != 0;
   const bool wrap = faces && sp.periodic[sp.D - 1] && k > 1;
   cudaStream_t user = (cudaStream_t)stream;
-  // the copies start after the work already queued on the caller's stream
+  const int b = (int)(io->calls & 1u);
+  double* x = io->x[b];
+  double* y = io->y[b];
+  // the copies start after the work already queued on the caller's stream, and once the applies
+  // of the call two back (same device pair) no longer read x
   DGOP_CUDA_H(cudaEventRecord(io->start, user));
   DGOP_CUDA_H(cudaStreamWaitEvent(io->up, io->start, 0));
+  if (io->calls >= 2) DGOP_CUDA_H(cudaStreamWaitEvent(io->up, io->read_done[b], 0));
+  for (int c = 0; c < 2; ++c) {
+    const double* yp = io->y_host[c];
+    if (yp && x_host < yp + sp.ndofs && yp < x_host + sp.ndofs)
+      DGOP_CUDA_H(cudaStreamWaitEvent(io->up, io->sent[c], 0));
+  }
   for (int i = 0; i < k; ++i) {
     const int64_t d0 = io->first[i] * nd, dn = (io->first[i + 1] - io->first[i]) * nd;
-    DGOP_CUDA_H(cudaMemcpyAsync(io->x + d0, x_host + d0, sizeof(double) * dn, cudaMemcpyHostToDevice, io->up));
+    DGOP_CUDA_H(cudaMemcpyAsync(x + d0, x_host + d0, sizeof(double) * dn, cudaMemcpyHostToDevice, io->up));
     DGOP_CUDA_H(cudaEventRecord(io->uploaded[i], io->up));
   }
+  // y is rewritten once the downloads of the call two back are done
+  if (io->calls >= 2) DGOP_CUDA_H(cudaStreamWaitEvent(io->run, io->sent[b], 0));
   for (int i = 0; i < k; ++i) {
     // slabs i - 1 .. i + 1 are read; uploads complete in order, so waiting for the highest is enough
     const int need = (wrap && i == 0) ? k - 1 : (faces ? std::min(i + 1, k - 1) : i);
     DGOP_CUDA_H(cudaStreamWaitEvent(io->run, io->uploaded[need], 0));
-    DGOP_TRY_H(launch_range_f64(io->op, io->x, io->y, io->first[i], io->first[i + 1], io->run));
+    DGOP_TRY_H(launch_range_f64(io->op, x, y, io->first[i], io->first[i + 1], io->run));
     DGOP_CUDA_H(cudaEventRecord(io->applied[i], io->run));
     DGOP_CUDA_H(cudaStreamWaitEvent(io->down, io->applied[i], 0));
     const int64_t d0 = io->first[i] * nd, dn = (io->first[i + 1] - io->first[i]) * nd;
-    DGOP_CUDA_H(cudaMemcpyAsync(y_host + d0, io->y + d0, sizeof(double) * dn, cudaMemcpyDeviceToHost, io->down));
+    DGOP_CUDA_H(cudaMemcpyAsync(y_host + d0, y + d0, sizeof(double) * dn, cudaMemcpyDeviceToHost, io->down));
   }
+  DGOP_CUDA_H(cudaEventRecord(io->read_done[b], io->run));
+  DGOP_CUDA_H(cudaEventRecord(io->sent[b], io->down));
   DGOP_CUDA_H(cudaEventRecord(io->finished, io->down));
-  DGOP_CUDA_H(cudaStreamWaitEvent(user, io->finished, 0));
+  io->y_host[b] = y_host;
+  ++io->calls;
+  return DGOP_OK;
+}
+
+int dgop_host_io_wait(dgop_host_io* io, void* stream) {
+  if (!io) {
+    set_error("dgop_host_io_wait: null argument");
+    return DGOP_ERR_ARG;
+  }
+  DGOP_CUDA_H(cudaStreamWaitEvent((cudaStream_t)stream, io->finished, 0));
+  return DGOP_OK;
+}
+
+int dgop_host_io_apply(dgop_host_io* io, const double* x_host, double* y_host, void* stream) {
+  DGOP_TRY_H(dgop_host_io_apply_async(io, x_host, y_host, stream));
+  DGOP_TRY_H(dgop_host_io_wait(io, stream));
   DGOP_CUDA_H(cudaEventSynchronize(io->finished));
   return DGOP_OK;
 }

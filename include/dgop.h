@@ -164,13 +164,20 @@ int dgop_batch_destroy(dgop_batch* batch);
  * massoperator.hpp:209, advectionoperator.hpp:1070, where the data lives in host memory):
  * y_host = A x_host.  The host-to-device copy, the apply and the device-to-host copy are pipelined
  * over `slabs` ranges of element planes of the last axis (slabs <= 0: 8), so upload and download
- * overlap.  The handle owns two device vectors and three streams (allocated at creation).  The
- * call starts after the work queued on `stream`, makes `stream` wait for its end and returns when
- * y_host is written.  Pinned host memory (cudaMallocHost / cudaHostRegister) copies at full link
- * speed; pageable memory works, more slowly. */
+ * overlap.  The handle owns two pairs of device vectors and three streams (allocated at
+ * creation).  dgop_host_io_apply starts after the work queued on `stream`, makes `stream` wait for
+ * its end and returns when y_host is written.  dgop_host_io_apply_async queues the same work and
+ * returns at once: consecutive asynchronous applies alternate between the two device pairs, so
+ * one apply's uploads run while the previous one's downloads finish (an input that overlaps an
+ * earlier call's result waits for that result).  Its results are complete once
+ * dgop_host_io_wait(io, stream) has made `stream` wait for them (then synchronize the stream) or
+ * after a later dgop_host_io_apply returns.  Pinned host memory (cudaMallocHost /
+ * cudaHostRegister) copies at full link speed; pageable memory works, more slowly. */
 typedef struct dgop_host_io dgop_host_io;
 int dgop_host_io_create(dgop_operator* op, int slabs, dgop_host_io** out);
 int dgop_host_io_apply(dgop_host_io* io, const double* x_host, double* y_host, void* stream);
+int dgop_host_io_apply_async(dgop_host_io* io, const double* x_host, double* y_host, void* stream);
+int dgop_host_io_wait(dgop_host_io* io, void* stream);
 int dgop_host_io_destroy(dgop_host_io* io);
 
 /* ---- Krylov solvers, device resident (workspaces allocated at create time).

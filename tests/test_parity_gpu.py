@@ -299,3 +299,32 @@ def test_speed_of_light_operator_copies_exactly():
     io.apply(xh, yh)
     assert torch.equal(xh, yh)
     io.close()
+
+
+@pytest.mark.parametrize("cid,case,kind,mode,slabs", HOSTIO_CASES[:2], ids=[c[0] for c in HOSTIO_CASES[:2]])
+def test_host_io_async_applies_overlap_and_chain(cid, case, kind, mode, slabs):
+    """dgop_host_io_apply_async: several queued applies on distinct host vectors (alternating
+    device pairs) and a chain y1 = A x, y2 = A y1, y3 = A y2 through host memory give the bits of
+    the device applies once dgop_host_io_wait has run."""
+    import torch
+    import gendil_b200 as g
+    op = make_operator(case, kind, mode)
+    io = g.HostIO(op, slabs=slabs)
+    stream = torch.cuda.current_stream()
+    xs = [torch.from_numpy(inputs(dict(case, seed=s))).pin_memory() for s in (1, 2, 3, 4, 5)]
+    ys = [torch.full_like(x, float("nan")).pin_memory() for x in xs]
+    for x, y in zip(xs, ys):
+        io.apply_async(x, y, stream)
+    chain = [torch.full_like(xs[0], float("nan")).pin_memory() for _ in range(3)]
+    io.apply_async(xs[0], chain[0], stream)
+    io.apply_async(chain[0], chain[1], stream)
+    io.apply_async(chain[1], chain[2], stream)
+    io.wait(stream)
+    stream.synchronize()
+    for x, y in zip(xs, ys):
+        assert np.array_equal(y.numpy(), cuda_apply(op, x.numpy()))
+    want = xs[0].numpy()
+    for c in chain:
+        want = cuda_apply(op, want)
+        assert np.array_equal(c.numpy(), want)
+    io.close()
