@@ -81,6 +81,7 @@ def lib():
         L.dgop_apply_ex.argtypes = [vp, d, vp, d, vp, vp]
         L.dgop_apply_transpose.argtypes = [vp, vp, vp, vp]
         L.dgop_apply_f32.argtypes = [vp, vp, vp, vp]
+        L.dgop_apply_bf16.argtypes = [vp, vp, vp, i, vp]
         L.dgop_fill_random.argtypes = [vp, i64, ctypes.c_uint, d, d]
         L.dgop_operator_kernel.argtypes = [vp]
         L.dgop_operator_kernel_note.argtypes = [vp]
@@ -239,6 +240,12 @@ class _Operator:
 
     def apply_f32(self, x, y, stream=None):
         check(lib().dgop_apply_f32(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        return y
+
+    def apply_bf16(self, x, y, transpose=False, stream=None):
+        """y = A x (A^T x) for FP32 tensors with BF16 tensor-core contractions, FP32 accumulation and
+        per-element max-abs scaling (dgop_apply_bf16; even dimensions, (p+1)^(D/2) <= 32)."""
+        check(lib().dgop_apply_bf16(self.handle, _ptr(x), _ptr(y), 1 if transpose else 0, _stream(stream)))
         return y
 
     @property
@@ -473,13 +480,14 @@ class GMRESSolver(_Solver):
 
 class GMRESIRSolver(_Solver):
     """GMRES(restart) with iterative refinement: restart cycles solve the correction equation
-    with operator applies and a Krylov basis in `inner` precision ("fp32" or "fp64"), the residual
-    and the solution are updated in FP64.  Same solve() contract and stopping test as
-    GMRESSolver; no reference counterpart."""
+    with operator applies and a Krylov basis in `inner` precision ("fp32", "fp64", or "bf16": an
+    FP32 basis with the operator's BF16 tensor-core applies), the residual and the solution are
+    updated in FP64.  Same solve() contract and stopping test as GMRESSolver; no reference
+    counterpart."""
 
     def __init__(self, op, restart=30, inner="fp32"):
         super().__init__(op)
-        prec = {"fp32": 1, "fp64": 0}[inner]
+        prec = {"fp32": 1, "fp64": 0, "bf16": 2}[inner]
         h = ctypes.c_void_p()
         check(lib().dgop_gmres_ir_create(op.handle, int(restart), prec, ctypes.byref(h)))
         self.handle = h

@@ -458,6 +458,99 @@ int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
   return DGOP_OK;
 }
 
+// BF16 bits of a finite float, rounded to nearest even.
+uint16_t to_bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, sizeof(u));
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
+// Kronecker tiles of the tensor-core variant (kronnd_tc_kernel.cuh): for every term and half of
+// the axes, the product of the term's tangential matrices over the half's axes (the identity on
+// the term's own axis), one tile per combination of coordinates along the half's axes whose
+// matrices vary, scaled by its largest magnitude, as BF16 in a P x (P + 8) padded tile.  Returns
+// false (no tensor-core launch) when the tables would exceed 256 MB.
+bool build_tc_tiles(const dgop_space& s, const KronPlanHost& plan, KronNDCfg<float>& K) {
+  const int D = s.D, N = s.n, H = D / 2;
+  int F = 1;
+  for (int k = 0; k < H; ++k) F *= N;
+  const int P = F <= 16 ? 16 : 32, LD = P + 8;
+  auto& p = K.params;
+  std::vector<int> terms;
+  if (plan.has_adv)
+    for (int t = 0; t < D; ++t) terms.push_back(t);
+  if (plan.has_mass && !(plan.has_adv && plan.mass_merged)) terms.push_back(D);
+  int64_t count = 0;
+  for (int t : terms)
+    for (int h = 0; h < 2; ++h) {
+      const int ax = t < D ? t : D - 1;
+      p.tc_base[t][h] = (int)count;
+      int64_t mult = 1;
+      for (int k = h * H; k < h * H + H; ++k) {
+        const KronMat m = t < D ? (k == t ? plan.D[t] : plan.T[t][k]) : (k == D - 1 ? plan.MD : plan.MT[k]);
+        p.tc_mult[t][k] = 0;
+        if (k != ax && m.off >= 0 && m.stride != 0) {
+          p.tc_mult[t][k] = (int)mult;
+          mult *= s.sizes[k];
+        }
+      }
+      count += mult;
+    }
+  const size_t tile = (size_t)P * LD;
+  if (count * tile * 2 > (size_t)256 << 20) return false;
+  std::vector<uint16_t> tiles((size_t)count * tile, 0);
+  std::vector<float> scales((size_t)count, 0.0f);
+  std::vector<double> val((size_t)F * F);
+  for (int t : terms)
+    for (int h = 0; h < 2; ++h) {
+      const int ax = t < D ? t : D - 1;
+      const int lo = h * H;
+      int64_t combos = 1;
+      for (int k = lo; k < lo + H; ++k)
+        if (p.tc_mult[t][k]) combos *= s.sizes[k];
+      for (int64_t cb = 0; cb < combos; ++cb) {
+        int64_t c[kMaxDim] = {};
+        int64_t rem = cb;
+        for (int k = lo; k < lo + H; ++k)
+          if (p.tc_mult[t][k]) {
+            c[k] = rem % s.sizes[k];
+            rem /= s.sizes[k];
+          }
+        double mx = 0.0;
+        for (int r = 0; r < F; ++r)
+          for (int q = 0; q < F; ++q) {
+            double v = 1.0;
+            int rr = r, qq = q;
+            for (int k = lo; k < lo + H; ++k) {
+              const int i = rr % N, j = qq % N;
+              rr /= N;
+              qq /= N;
+              const KronMat m = t < D ? (k == t ? plan.D[t] : plan.T[t][k]) : (k == D - 1 ? plan.MD : plan.MT[k]);
+              if (k == ax) v *= (i == j) ? 1.0 : 0.0;
+              else v *= m.off >= 0 ? plan.mats[(size_t)(m.off + c[k] * m.stride + i * N + j)] : 0.0;
+            }
+            val[(size_t)r * F + q] = v;
+            mx = std::max(mx, std::fabs(v));
+          }
+        const int64_t id = p.tc_base[t][h] + cb;
+        scales[(size_t)id] = (float)mx;
+        uint16_t* dst = tiles.data() + (size_t)id * tile;
+        for (int r = 0; r < F; ++r)
+          for (int q = 0; q < F; ++q) dst[(size_t)r * LD + q] = to_bf16_bits(mx > 0 ? (float)(val[(size_t)r * F + q] / mx) : 0.0f);
+      }
+    }
+  if (cudaMalloc(&K.d_tc_tiles, tiles.size() * sizeof(uint16_t)) != cudaSuccess ||
+      cudaMalloc(&K.d_tc_scale, scales.size() * sizeof(float)) != cudaSuccess ||
+      cudaMemcpy(K.d_tc_tiles, tiles.data(), tiles.size() * sizeof(uint16_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(K.d_tc_scale, scales.data(), scales.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  p.tc_tiles = K.d_tc_tiles;
+  p.tc_scale = K.d_tc_scale;
+  return true;
+}
+
 // Any-dimension Kronecker kernel: matrix tables, face tables and launch shape.
 template <typename Real>
 int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan, const double* elem_sigma,
@@ -599,6 +692,35 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), per * ebv, 0.0f};
   }
   K.variant = 0;
+  if constexpr (sizeof(Real) == 4) {
+    if (entry->launch_tc && build_tc_tiles(s, plan, K)) {
+      // the transposed parameters share the tangential matrices, hence the tiles
+      K.params_t.tc_tiles = K.params.tc_tiles;
+      K.params_t.tc_scale = K.params.tc_scale;
+      std::memcpy(K.params_t.tc_base, K.params.tc_base, sizeof(K.params.tc_base));
+      std::memcpy(K.params_t.tc_mult, K.params.tc_mult, sizeof(K.params.tc_mult));
+      const size_t tsm = (size_t)entry->tc_warp_bytes * (kKronTCThreads / 32);
+      cudaFuncAttributes ft{};
+      int max_t = 0;
+      if (cudaFuncGetAttributes(&ft, entry->func_tc) == cudaSuccess &&
+          cudaDeviceGetAttribute(&max_t, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device) == cudaSuccess &&
+          tsm + ft.sharedSizeBytes <= (size_t)max_t &&
+          cudaFuncSetAttribute(entry->func_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               max_t - (int)ft.sharedSizeBytes) == cudaSuccess) {
+        int per_sm_t = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, entry->func_tc, kKronTCThreads, tsm) ==
+                cudaSuccess &&
+            per_sm_t >= 1) {
+          const int64_t ct = std::min<int64_t>((s.nelem + kKronTCThreads / 32 - 1) / (kKronTCThreads / 32),
+                                               (int64_t)device_sm_count(op->device) * per_sm_t);
+          K.tc_grid = dim3((unsigned)std::max<int64_t>(ct, 1));
+          K.tc_smem = tsm;
+          K.tc_ok = true;
+        }
+      }
+      cudaGetLastError();
+    }
+  }
   K.ready = true;
   return DGOP_OK;
 }
@@ -667,6 +789,8 @@ int autotune_kronnd(dgop_operator* op, KronNDCfg<Real>& K) {
 
 template <typename Real>
 void free_kronnd(KronNDCfg<Real>& K) {
+  if (K.d_tc_tiles) cudaFree(K.d_tc_tiles);
+  if (K.d_tc_scale) cudaFree(K.d_tc_scale);
   if (K.d_mats) cudaFree(K.d_mats);
   if (K.d_phi) cudaFree(K.d_phi);
   if (K.d_sgn) cudaFree(K.d_sgn);
@@ -994,6 +1118,40 @@ int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, flo
   return launch_impl<float>(op, op->f32, op->k32, op->n32, op->s32, alpha, x, beta_y, y, extra_flags, s, skip);
 }
 
+int launch_bf16(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
+                cudaStream_t s, const int* skip) {
+  KronNDCfg<float>& K = op->n32;
+  if (!K.ready || !K.tc_ok) {
+    set_error("no BF16 tensor-core kernel for this operator (it needs the any-dimension Kronecker form, an even "
+              "dimension and (p+1)^(D/2) <= 32)");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (!x || !y || x == y) {
+    set_error("null or aliasing vectors");
+    return DGOP_ERR_ARG;
+  }
+  if (reinterpret_cast<uintptr_t>(x) % 4 || reinterpret_cast<uintptr_t>(y) % 4) {
+    set_error("vectors must be aligned to their element size");
+    return DGOP_ERR_ARG;
+  }
+  const bool linear = (extra_flags & kLinear) != 0;
+  extra_flags &= ~kLinear;
+  KronNDParams<float> p = (extra_flags & kTranspose) ? K.params_t : K.params;
+  p.x = x;
+  p.y = y;
+  p.alpha = alpha;
+  p.beta_y = beta_y;
+  p.flags = op->flags | extra_flags;
+  p.skip = skip;
+  p.e_begin = 0;
+  p.nelem = op->sp.nelem;
+  if (linear) p.g = 0.0f;
+  K.entry->launch_tc(p, K.tc_grid, dim3(kKronTCThreads), K.tc_smem, s);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "tensor-core kernel launch");
+  return DGOP_OK;
+}
+
 int launch_range_f64(dgop_operator* op, const double* x, double* y, int64_t e_begin, int64_t e_end, cudaStream_t s) {
   return launch_impl<double>(op, op->f64, op->k64, op->n64, op->s64, 1.0, x, 0.0, y, 0, s, nullptr, e_begin, e_end);
 }
@@ -1276,6 +1434,14 @@ int dgop_apply_ex(dgop_operator* op, double alpha, const double* x, double beta,
     return DGOP_ERR_ARG;
   }
   return launch_f64(op, alpha, x, beta, y, 0, (cudaStream_t)stream);
+}
+
+int dgop_apply_bf16(dgop_operator* op, const float* x, float* y, int transpose, void* stream) {
+  if (!op) {
+    set_error("null operator");
+    return DGOP_ERR_ARG;
+  }
+  return launch_bf16(op, 1.0f, x, 0.0f, y, transpose ? kTranspose : 0, (cudaStream_t)stream, nullptr);
 }
 
 int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* stream) {

@@ -75,6 +75,12 @@ struct KronNDCfg {
     float ms = 0.0f;  // autotuner's time per launch (0: not timed)
   } var[kKronNDVariants];
   int variant = 0;
+  // BF16 tensor-core launch (FP32 configuration only) and its Kronecker tile tables
+  bool tc_ok = false;
+  dim3 tc_grid;
+  size_t tc_smem = 0;
+  void* d_tc_tiles = nullptr;
+  float* d_tc_scale = nullptr;
 };
 
 template <typename Real>
@@ -123,6 +129,8 @@ namespace dgop {
 // When `skip` (a device word) is non-zero at run time the launch does nothing.
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
                cudaStream_t s, const int* skip = nullptr);
+int launch_bf16(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
+                cudaStream_t s, const int* skip);
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                cudaStream_t s, const int* skip = nullptr);
 // y = Op(x) on the elements [e_begin, e_end) only (y elsewhere untouched; x read around them)

@@ -4,6 +4,7 @@
 #include "kronnd_diff_grad_kernel.cuh"
 #include "kronnd_diff_kernel.cuh"
 #include "kronnd_kernel.cuh"
+#include "kronnd_tc_kernel.cuh"
 
 #ifndef DGOP_GEN_D
 #error "DGOP_GEN_D must be defined"
@@ -23,6 +24,11 @@ void launch_kronnd(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t sm
 template <int D, int N, int G, typename Real>
 void launch_kronnd_grouped(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   kronnd_grouped_kernel<D, N, G, Real><<<grid, block, smem, s>>>(p);
+}
+
+template <int D, int N>
+void launch_kronnd_tc(const KronNDParams<float>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_tc_kernel<D, N><<<grid, block, smem, s>>>(p);
 }
 
 template <int D, int N, int V, typename Real>
@@ -63,6 +69,11 @@ void fill(KronNDEntry<Real>& d) {
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);
       }
+    }
+    if constexpr (sizeof(Real) == 4 && KronTCShape<D, N>::OK && KronTCShape<D, N>::WARP_BYTES * 4 <= 200 * 1024) {
+      d.launch_tc = &launch_kronnd_tc<D, N>;
+      d.func_tc = reinterpret_cast<const void*>(&kronnd_tc_kernel<D, N>);
+      d.tc_warp_bytes = KronTCShape<D, N>::WARP_BYTES;
     }
     if constexpr (D >= 3 && N >= 2 && N * N * N <= 27) {
       d.launch_g[1] = &launch_kronnd_grouped<D, N, 3, Real>;

@@ -101,6 +101,14 @@ struct KronNDParams {
   const Real* elem[kMaxDim];
   const Real* elem_mass;
   const int* skip;
+  // tensor-core variant (kronnd_tc_kernel.cuh, FP32 operators): BF16 Kronecker products of every
+  // term's tangential matrices over the fast half (h = 0) and the slow half (h = 1) of the axes,
+  // padded tiles; the tile of term t, half h for an element with coordinates c is number
+  // tc_base[t][h] + sum_k c_k tc_mult[t][k] (over the half's axes), its scale tc_scale[that]
+  const void* tc_tiles;
+  const float* tc_scale;
+  int tc_base[kMaxDim + 1][2];
+  int tc_mult[kMaxDim + 1][kMaxDim];
 };
 
 // Interior-penalty diffusion (kronnd_diff_kernel.cuh, sipdg.cu).

@@ -9,6 +9,7 @@ namespace dgop {
 
 constexpr int kKronThreads = 128;
 constexpr int kKronNDThreads = 256;  // threads per CTA of the any-dimension kernel
+constexpr int kKronTCThreads = 128;  // tensor-core variant: four warps (elements) per CTA
 
 // Kernel variants of one (N, precision); the autotuner picks one per operator.
 //   0: two staging stages, exchanges through the shared tile
@@ -53,6 +54,10 @@ struct KronNDEntry {
   // grouped variants (kronnd_grouped_kernel), groups of 2 and 3 axes: same parameters and layout
   void (*launch_g[2])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
   const void* func_g[2] = {};
+  // BF16 tensor-core variant (kronnd_tc_kernel.cuh; FP32 parameters, even D, N^(D/2) <= 32)
+  void (*launch_tc)(const KronNDParams<float>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func_tc = nullptr;
+  int tc_warp_bytes = 0;
   // interior-penalty diffusion (kronnd_diff_kernel.cuh)
   void (*launch_diff)(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_diff = nullptr;

@@ -541,7 +541,7 @@ struct SolverImpl {
   void* state = nullptr;       // CGState / GMState (device)
   double* small = nullptr;     // GMRES: H, cs, sn, e1, y
   int* h_flag = nullptr;       // host copies of `done`, one per segment parity (pinned)
-  int inner = 0;               // refinement solver: DGOP_FP32 or DGOP_FP64 inner cycles
+  int inner = 0;               // refinement solver: DGOP_FP64, DGOP_FP32 or DGOP_BF16 inner cycles
   double* wide = nullptr;      // refinement solver: (restart + 1) x kRB projection partials
   // Segments (a CG chunk, a GMRES cycle) are replayed from one CUDA graph, captured for the
   // current (b, x, operator version) and re-captured when any of them changes (tolerance and
@@ -844,6 +844,14 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
   };
+  // the inner operator: the BF16 tensor-core kernel for DGOP_BF16 (FP32 vectors), else the
+  // kernel of the inner type
+  auto apply_op = [&](const T* in, T* out, cudaStream_t q) -> int {
+    if constexpr (sizeof(T) == 4) {
+      if (s.inner == DGOP_BF16) return launch_bf16(s.op, 1.0f, in, 0.0f, out, kLinear | s.op_flags, q, inactive);
+    }
+    return apply_inner(s.op, in, out, s.op_flags, q, inactive);
+  };
   auto cycle = [&](cudaStream_t q) -> int {
     k_gm_cycle_start<<<1, 1, 0, q>>>(gs, csv, snv, e1, y, m);
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(r64), V, n, -1);  // V0 = r / |r|
@@ -853,9 +861,9 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
       if (s.prec) {
         T* z = static_cast<T*>(s.pz);
         DGOP_TRY(apply_inner(s.prec, vj, z, 0, q, inactive));
-        DGOP_TRY(apply_inner(s.op, z, w, s.op_flags, q, inactive));
+        DGOP_TRY(apply_op(z, w, q));
       } else {
-        DGOP_TRY(apply_inner(s.op, vj, w, s.op_flags, q, inactive));
+        DGOP_TRY(apply_op(vj, w, q));
       }
       const dim3 dgrid(kRB, (j + 1 + kGsChunk - 1) / kGsChunk);
       k_gs_dots<T><<<dgrid, kRT, 0, q>>>(gs, V, ld, j, w, s.wide);
@@ -902,12 +910,17 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dg
     return DGOP_ERR_ARG;
   }
   *out = nullptr;
-  if (inner_precision != DGOP_FP32 && inner_precision != DGOP_FP64) {
-    set_error("dgop_gmres_ir_create: inner_precision must be DGOP_FP32 or DGOP_FP64");
+  if (inner_precision != DGOP_FP32 && inner_precision != DGOP_FP64 && inner_precision != DGOP_BF16) {
+    set_error("dgop_gmres_ir_create: inner_precision must be DGOP_FP32, DGOP_FP64 or DGOP_BF16");
     return DGOP_ERR_ARG;
   }
-  if (inner_precision == DGOP_FP32 && !op->f32.ready && !op->k32.ready) {
+  if (inner_precision == DGOP_FP32 && !op->f32.ready && !op->k32.ready && !op->n32.ready) {
     set_error("dgop_gmres_ir_create: the operator has no FP32 kernel");
+    return DGOP_ERR_UNSUPPORTED;
+  }
+  if (inner_precision == DGOP_BF16 && !(op->n32.ready && op->n32.tc_ok)) {
+    set_error("dgop_gmres_ir_create: the operator has no BF16 tensor-core kernel (any-dimension Kronecker form, "
+              "even dimension, (p+1)^(D/2) <= 32)");
     return DGOP_ERR_UNSUPPORTED;
   }
   auto* sv = new (std::nothrow) dgop_solver();
@@ -924,7 +937,7 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dg
   const size_t small = (size_t)(restart + 1) * restart + 2 * restart + (restart + 1) + restart;
   // two FP64 vectors (A x, residual), then restart + 2 inner vectors (w and the basis) at stride
   // ir_stride(n); the padding entries must read as zero, so the workspace starts zeroed
-  const size_t inner_words = (size_t)ir_stride(s.n) * (inner_precision == DGOP_FP32 ? 4 : 8) / 8;
+  const size_t inner_words = (size_t)ir_stride(s.n) * (inner_precision != DGOP_FP64 ? 4 : 8) / 8;
   const size_t words = 2 * (size_t)vec_stride(s.n) + (size_t)(restart + 2) * inner_words;
   int rc = solver_alloc(sv, words, sizeof(GMState), small);
   if (rc == DGOP_OK) {
@@ -1004,7 +1017,7 @@ int dgop_solver_solve(dgop_solver* sv, const double* b, double* x, int max_iters
   cudaStream_t st = (cudaStream_t)stream;
   if (sv->s.kind == 0) return cg_solve(sv->s, b, x, max_iters, tol, result, st);
   if (sv->s.kind == 2)
-    return sv->s.inner == DGOP_FP32 ? gmres_ir_solve<float>(sv->s, b, x, max_iters, tol, result, st)
+    return sv->s.inner != DGOP_FP64 ? gmres_ir_solve<float>(sv->s, b, x, max_iters, tol, result, st)
                                     : gmres_ir_solve<double>(sv->s, b, x, max_iters, tol, result, st);
   return gmres_solve(sv->s, b, x, max_iters, tol, result, st);
 }
@@ -1032,12 +1045,12 @@ int dgop_solver_set_preconditioner(dgop_solver* sv, dgop_operator* prec) {
     set_error("dgop_solver_set_preconditioner: the preconditioner acts on another space");
     return DGOP_ERR_ARG;
   }
-  if (prec && s.kind == 2 && s.inner == DGOP_FP32 && !prec->f32.ready && !prec->k32.ready && !prec->n32.ready) {
+  if (prec && s.kind == 2 && s.inner != DGOP_FP64 && !prec->f32.ready && !prec->k32.ready && !prec->n32.ready) {
     set_error("dgop_solver_set_preconditioner: the preconditioner has no FP32 kernel");
     return DGOP_ERR_UNSUPPORTED;
   }
   if (prec && !s.pz) {
-    const size_t zbytes = s.kind == 2 ? (size_t)ir_stride(s.n) * (s.inner == DGOP_FP32 ? 4 : 8) : sizeof(double) * s.n;
+    const size_t zbytes = s.kind == 2 ? (size_t)ir_stride(s.n) * (s.inner != DGOP_FP64 ? 4 : 8) : sizeof(double) * s.n;
     cudaError_t e = cudaMalloc(&s.pz, zbytes);
     if (e == cudaSuccess) e = cudaMemset(s.pz, 0, zbytes);
     if (e == cudaSuccess) e = cudaMalloc(&s.pt, sizeof(double) * s.n);

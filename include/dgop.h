@@ -28,7 +28,7 @@ enum dgop_status {
 
 enum dgop_basis { DGOP_BASIS_GLL = 0, DGOP_BASIS_GL = 1 };
 enum dgop_bc { DGOP_BC_NONE = 0, DGOP_BC_INFLOW = 1 };
-enum dgop_precision { DGOP_FP64 = 0, DGOP_FP32 = 1 };
+enum dgop_precision { DGOP_FP64 = 0, DGOP_FP32 = 1, DGOP_BF16 = 2 };
 
 typedef struct dgop_space dgop_space;
 typedef struct dgop_operator dgop_operator;
@@ -145,6 +145,13 @@ int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms);
 int dgop_apply(dgop_operator* op, const double* x, double* y, void* stream);
 int dgop_apply_ex(dgop_operator* op, double alpha, const double* x, double beta, double* y, void* stream);
 /* y = A^T x: the adjoint of the linear part (inflow value treated as 0); no reference counterpart. */
+/* apply_bf16:      y = A x (transpose: A^T x) for FP32 vectors with BF16 tensor-core contractions,
+ *                  FP32 accumulation and per-element max-abs scaling (the low-precision inner
+ *                  operator of the refinement solver, DGOP_BF16): operators on the any-dimension
+ *                  Kronecker form with an even dimension and (p+1)^(D/2) <= 32 (6D p <= 2, 4D
+ *                  p <= 4, 2D any order).  Relative error about 1e-2 of |A| |x|.  No reference
+ *                  counterpart. */
+int dgop_apply_bf16(dgop_operator* op, const float* x, float* y, int transpose, void* stream);
 int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* stream);
 /* FP32 apply of the same operator (tables rounded to FP32); no reference counterpart. */
 int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
