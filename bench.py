@@ -188,7 +188,7 @@ def run_reference(args):
 
 
 def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=None, seed=2, max_iters=20000,
-              plain=True):
+              plain=True, bf16=False):
     """Implicit-Euler system (M/dt + A) x = b, b = FillRandom(seed), GMRES(restart) to tol
     relative FP64 residual from x0 = 0, timed on the device (CUDA events around the whole solve):
     FP64 GMRES with the reference's modified Gram-Schmidt, then the refinement solver with FP64
@@ -210,6 +210,10 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
         legs = []
     legs += [("fp64_gmres_massprec", lambda: g.GMRESSolver(A, restart).precondition(P)),
              ("mixed_gmres_ir_massprec", lambda: g.GMRESIRSolver(A, restart, inner="fp32").precondition(P))]
+    if bf16:
+        # inner applies with BF16 tensor-core contractions (FP32 accumulation, per-element max-abs
+        # scaling), FP32 basis, FP64 refinement
+        legs.append(("bf16_gmres_ir_massprec", lambda: g.GMRESIRSolver(A, restart, inner="bf16").precondition(P)))
     for name, make in legs:
         solver = make()
         x = torch.zeros_like(b)
@@ -238,6 +242,9 @@ def solve_leg(g, C, space, dev, dt=1e-3, restart=30, tol=1e-10, q=None, beta=Non
         out["fp64_over_mixed_time"] = out["fp64_gmres"]["seconds"] / out["mixed_gmres_ir"]["seconds"]
     out["fp64_over_mixed_time_massprec"] = (out["fp64_gmres_massprec"]["seconds"] /
                                             out["mixed_gmres_ir_massprec"]["seconds"])
+    if "bf16_gmres_ir_massprec" in out:
+        out["fp64_over_bf16_time_massprec"] = (out["fp64_gmres_massprec"]["seconds"] /
+                                               out["bf16_gmres_ir_massprec"]["seconds"])
     A.close()
     P.close()
     return out
@@ -375,7 +382,8 @@ def run_ours(args):
                 # a relative residual of 0.12 after 200 iterations), so the legs solve it with the
                 # element mass inverse as right preconditioner (same 1e-10 on |b - A x| / |b|).
                 line["solve"] = solve_leg(g, C, space, dev, dt=5e-3, restart=20, q=3,
-                                          beta=C.velocity_phase_space(6), seed=3, max_iters=2000, plain=False)
+                                          beta=C.velocity_phase_space(6), seed=3, max_iters=2000, plain=False,
+                                          bf16=True)
             else:
                 line["solve"] = solve_leg(g, C, space, dev)
         if six:

@@ -187,10 +187,18 @@ __device__ __forceinline__ void tc_term(const KronNDParams<float>& P, int64_t e,
   const __nv_bfloat16* KF = tiles + t0 * S::TILE;
   const __nv_bfloat16* KS = tiles + t1 * S::TILE;
   const float sf = P.tc_scale[t0], ss = P.tc_scale[t1];
-  // W / wmax into the tile ([s][f]; the padding stays zero)
+  // W / wmax into the tile ([s][f]; the padding stays zero): lane s converts row s, two columns
+  // per 32-bit store (row stride F floats in Wf: distinct banks for odd F)
   __syncwarp();
   const float winv = 1.0f / wmax;
-  for (int i = lane; i < S::ND; i += 32) T0[(i / S::F) * S::LD + i % S::F] = __float2bfloat16_rn(Wf[i] * winv);
+  for (int r = lane; r < S::F; r += 32) {
+    const float* src = Wf + r * S::F;
+    __nv_bfloat16* dst = T0 + r * S::LD;
+#pragma unroll
+    for (int c = 0; c + 1 < S::F; c += 2)
+      *reinterpret_cast<__nv_bfloat162*>(dst + c) = __floats2bfloat162_rn(src[c] * winv, src[c + 1] * winv);
+    if constexpr (S::F % 2) dst[S::F - 1] = __float2bfloat16_rn(src[S::F - 1] * winv);
+  }
   __syncwarp();
   float C[S::MT][S::NT][4];
   tc_gemm<D, N>(KF, T0, C, lane);  // T^T = K_F W^T  (rows f', columns s)
