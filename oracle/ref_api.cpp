@@ -81,6 +81,8 @@ double gref_time_advection( int D, int P, int Q, int basis, const long * sizes, 
    };
    if ( basis != 0 ) return -1.0;
    if ( D == 3 && P == 3 && Q == 4 ) run( std::integral_constant< int, 3 >{}, std::integral_constant< int, 3 >{}, std::integral_constant< int, 4 >{} );
+   // the 6D phase-space configuration (p = 2, q = 3)
+   if ( D == 6 && P == 2 && Q == 3 ) run( std::integral_constant< int, 6 >{}, std::integral_constant< int, 2 >{}, std::integral_constant< int, 3 >{} );
    return seconds;
 }
 
