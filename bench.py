@@ -37,8 +37,9 @@ WORKLOAD_6D = ("fp64 upwind DG advection apply, 6D phase space 8^6 hypercubes on
                "q=3 GL, beta = (v, -x + 0.5), inflow 0")
 FALLBACK_HBM_GBS = 6650.0
 HOST_SLABS = 4  # slabs of z planes per host-vector apply (consecutive steps overlap, so few slabs suffice)
-# DRAM bytes (read + write) of one launch measured by ncu on the 64^3 workload, by kernel family
-TRAFFIC_BYTES = {("kron", 64): 221.3e6}
+# DRAM bytes (read + write) of one launch measured by ncu (one-pass capture of the full workload),
+# by (workload, kernel variant, elements per axis)
+TRAFFIC_BYTES = {("3d", "stage1-tile", 64): 221.3e6, ("6d", "nd-grouped2", 8): 4.25e9}
 
 
 def case_dict(n=N_AXIS):
@@ -357,7 +358,7 @@ def run_ours(args):
     alg_bytes = 16.0 * nd
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
     # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu, summarized under profiles/)
-    traffic = None if six else TRAFFIC_BYTES.get((op.kernel, args.size))
+    traffic = TRAFFIC_BYTES.get(("6d", op.variant, args.size_6d) if six else ("3d", op.variant, args.size))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
