@@ -92,6 +92,7 @@ def lib():
         L.dgop_operator_variant_name.restype = ctypes.c_char_p
         L.dgop_operator_set_variant.argtypes = [vp, i]
         L.dgop_operator_variant_time.argtypes = [vp, i, ctypes.POINTER(ctypes.c_float)]
+        L.dgop_operator_variant_f32.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_float)]
         L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
@@ -280,6 +281,14 @@ class _Operator:
     def set_variant(self, name):
         """Force a Kronecker-kernel variant by name, or None to re-run the autotuner."""
         check(lib().dgop_operator_set_variant(self.handle, -1 if name is None else self._variants().index(name)))
+
+    def variant_f32(self):
+        """(variant name, {name: autotuner ms or -1 when unusable}) of the FP32 kernel configuration."""
+        v = ctypes.c_int()
+        ms = (ctypes.c_float * 3)()
+        check(lib().dgop_operator_variant_f32(self.handle, ctypes.byref(v), ms))
+        names = self._variants()
+        return (None if v.value < 0 else names[v.value]), {n: ms[i] for i, n in enumerate(names)}
 
     def variant_times(self):
         """Autotuner time per launch (ms) of every variant (0.0: not available or not timed; the

@@ -1407,6 +1407,23 @@ int dgop_operator_set_variant(dgop_operator* op, int variant) {
   return DGOP_OK;
 }
 
+int dgop_operator_variant_f32(const dgop_operator* op, int* variant, float* ms) {
+  if (!op || !variant || !ms) {
+    set_error("dgop_operator_variant_f32: null argument");
+    return DGOP_ERR_ARG;
+  }
+  if (op->kernel == DGOP_KERNEL_KRONND && op->n32.ready) {
+    *variant = op->n32.variant;
+    for (int v = 0; v < kKronNDVariants; ++v) ms[v] = op->n32.var[v].ok ? op->n32.var[v].ms : -1.0f;
+  } else if (op->kernel == DGOP_KERNEL_KRON && op->k32.ready) {
+    *variant = op->k32.variant;
+    for (int v = 0; v < kKronVariants; ++v) ms[v] = op->k32.launch[v].ok ? op->k32.launch[v].ms : -1.0f;
+  } else {
+    *variant = -1;
+  }
+  return DGOP_OK;
+}
+
 int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms) {
   if (op && ms && uses_kronnd(op) && variant >= 0 && variant < kKronNDVariants) {
     *ms = op->n64.var[variant].ms;

@@ -136,6 +136,9 @@ int dgop_operator_variant(const dgop_operator* op);
 const char* dgop_operator_variant_name(const dgop_operator* op);
 int dgop_operator_set_variant(dgop_operator* op, int variant);
 int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms);
+/* The FP32 kernel configuration's variant and its autotuner times (ms[v]; -1: variant not usable;
+ * ms holds 3 entries); variant -1 without a Kronecker kernel. */
+int dgop_operator_variant_f32(const dgop_operator* op, int* variant, float* ms);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers, aligned to their
  * element size; the Kronecker-form kernel runs on 16-byte aligned vectors (any cudaMalloc'd or
