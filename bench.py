@@ -688,7 +688,10 @@ def run_sipdg(args):
             "config": {"workload": WORKLOAD_SIPDG.replace("32^3", f"{n}^3"), "dofs": nd, "elements": ne, "kernel": op.kernel,
                        "l2": f"inputs smaller than L2 ({8 * nd / 1e6:.0f} MB each); applies back to back"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+                         # dram__bytes_read.sum + dram__bytes_write.sum of one 32^3 launch (ncu, one
+                         # pass): x and mu read once, y still in L2 when the launch ends
+                         "traffic": 34.3e6 if n == 32 else None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg},
             "roofline_fp64": {"bound": "fp64", "achieved": a64, "peak": peak64, "unit": "TFLOP/s", "frac": a64 / peak64,
                               "flop_per_dof": flop, "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch), best of 3"},
             "gpu_launches": args.steps, "clocks": clocks.summary(),
