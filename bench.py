@@ -42,6 +42,14 @@ HOST_SLABS = 4  # slabs of z planes per host-vector apply (consecutive steps ove
 TRAFFIC_BYTES = {("3d", "stage1-tile", 64): 221.3e6, ("6d", "nd-grouped2", 8): 4.25e9}
 
 
+def workload_config(world, n=N_AXIS):
+    """The `config` of the default (3D advection) line, identical in both arms."""
+    nd = n ** 3 * (ORDER + 1) ** 3
+    return {"workload": WORKLOAD.replace("64^3", f"{n}^3"), "dofs": nd, "elements": n ** 3,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": f"inputs larger than L2 (x, y {8 * nd / 1e6:.0f} MB each)"}
+
+
 def case_dict(n=N_AXIS):
     return {"D": 3, "P": ORDER, "Q": NQ, "basis": 0, "sizes": [n] * 3, "h": [1.0 / n] * 3, "origin": [0.0] * 3,
             "periodic": [0] * 3, "beta_kind": 2, "g": 0.0}
@@ -185,25 +193,25 @@ def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    import numpy as np  # noqa: F401
-    from oracle.bindings import have_reference
+    from oracle.bindings import Reference, have_reference
     if not have_reference():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgendil_ref.so was not built"}))
         return 0
-    import gendil_b200 as g
-    x = g.fill_random((N_AXIS ** 3) * (ORDER + 1) ** 3, 1)
-    from oracle.bindings import Reference
+    # everything on this arm comes from the reference compiled from its own headers: the input is
+    # its FillRandom(seed 1) (Algebra/vector.hpp:632), the operator its AdvectionOperator WithBC
     ref = Reference()
     case = case_dict()
+    x = ref.fill_random((N_AXIS ** 3) * (ORDER + 1) ** 3, 1)
     ref.time_advection(case, x, max(1, args.warmup // 2))
     t = ref.time_advection(case, x, max(1, args.steps // 2))
     v = len(x) / t / 1e9
     line = {"metric": METRIC, "value": v, "unit": "GDoF/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "dofs": len(x), "l2": "inputs larger than L2"},
+            "config": workload_config(world),
             "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": ref.num_threads(), "kind": "reference",
-                             "sample": f"full 64^3 mesh, {2 * max(1, args.steps // 2)} applies, OpenMP"},
+                             "sample": f"full 64^3 mesh, {2 * max(1, args.steps // 2)} applies "
+                                       "(op(x,y); op(y,x) pairs), GenDiL AdvectionOperator WithBC, OpenMP"},
             "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -364,10 +372,11 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (FillRandom seed 1)",
-                "config": {"workload": (WORKLOAD_6D.replace("8^6", f"{n6}^6") if six else WORKLOAD), "dofs": nd,
-                           "elements": space.num_elements,
-                           "parallelism": f"replicas{world}" if world > 1 else "single",
-                           "l2": f"inputs larger than L2 (x, y {8 * nd / 1e6:.0f} MB each)"},
+                "config": (workload_config(world, args.size) if not six else
+                           {"workload": WORKLOAD_6D.replace("8^6", f"{n6}^6"), "dofs": nd,
+                            "elements": space.num_elements,
+                            "parallelism": f"replicas{world}" if world > 1 else "single",
+                            "l2": f"inputs larger than L2 (x, y {8 * nd / 1e6:.0f} MB each)"}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                              "algorithmic_bytes_per_launch": alg_bytes},
@@ -391,12 +400,10 @@ def run_ours(args):
             line["roofline_fp64"] = {"bound": "fp64", "achieved": a64, "peak": peak64, "unit": "TFLOP/s",
                                      "frac": a64 / peak64, "flop_per_dof": flop,
                                      "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch), best of 3"}
-        line["config"]["kernel"] = op.kernel
+        line["kernel"] = {"family": op.kernel}
         if op.variant:
-            line["config"]["kernel_variant"] = op.variant
-            line["config"]["autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in op.variant_times().items() if v}
-        if args.size != N_AXIS and not six:
-            line["config"]["workload"] = WORKLOAD.replace("64^3", f"{args.size}^3")
+            line["kernel"]["variant"] = op.variant
+            line["kernel"]["autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in op.variant_times().items() if v}
         if world == 1 and not args.no_solve:
             if six:
                 # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3.  The unpreconditioned

@@ -133,6 +133,24 @@ def _ptr(t):
     return t.data_ptr()
 
 
+def _dvec(t, n, dtype="float64", name="vector"):
+    """Device address of a contiguous CUDA tensor of exactly `n` values of `dtype`.  The kernels
+    read and write `n` values through this address, so a CPU tensor, another dtype, a strided view
+    or a short tensor is rejected here instead of becoming an out-of-bounds access on the device.
+    A plain integer is taken as a raw device address whose size the caller vouches for."""
+    if isinstance(t, int):
+        return t
+    if not getattr(t, "is_cuda", False):
+        raise ValueError(f"{name}: a CUDA tensor is required")
+    if str(t.dtype) != f"torch.{dtype}":
+        raise ValueError(f"{name}: dtype {dtype} required, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: a contiguous tensor is required")
+    if t.numel() != n:
+        raise ValueError(f"{name}: {n} values required, got {t.numel()}")
+    return t.data_ptr()
+
+
 def _stream(stream):
     if stream is None:
         try:
@@ -227,26 +245,34 @@ class _Operator:
 
     def __call__(self, x, y, stream=None):
         """y = A x (overwrites y), FP64 device tensors."""
-        check(lib().dgop_apply(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        n = self.space.num_dofs
+        check(lib().dgop_apply(self.handle, _dvec(x, n, name="x"), _dvec(y, n, name="y"), _stream(stream)))
         return y
 
     def apply(self, x, y, alpha=1.0, beta=0.0, stream=None):
         """y = alpha A x + beta y."""
-        check(lib().dgop_apply_ex(self.handle, float(alpha), _ptr(x), float(beta), _ptr(y), _stream(stream)))
+        n = self.space.num_dofs
+        check(lib().dgop_apply_ex(self.handle, float(alpha), _dvec(x, n, name="x"), float(beta), _dvec(y, n, name="y"),
+                                  _stream(stream)))
         return y
 
     def apply_transpose(self, x, y, stream=None):
-        check(lib().dgop_apply_transpose(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        n = self.space.num_dofs
+        check(lib().dgop_apply_transpose(self.handle, _dvec(x, n, name="x"), _dvec(y, n, name="y"), _stream(stream)))
         return y
 
     def apply_f32(self, x, y, stream=None):
-        check(lib().dgop_apply_f32(self.handle, _ptr(x), _ptr(y), _stream(stream)))
+        n = self.space.num_dofs
+        check(lib().dgop_apply_f32(self.handle, _dvec(x, n, "float32", "x"), _dvec(y, n, "float32", "y"),
+                                   _stream(stream)))
         return y
 
     def apply_bf16(self, x, y, transpose=False, stream=None):
         """y = A x (A^T x) for FP32 tensors with BF16 tensor-core contractions, FP32 accumulation and
         per-element max-abs scaling (dgop_apply_bf16; even dimensions, (p+1)^(D/2) <= 32)."""
-        check(lib().dgop_apply_bf16(self.handle, _ptr(x), _ptr(y), 1 if transpose else 0, _stream(stream)))
+        n = self.space.num_dofs
+        check(lib().dgop_apply_bf16(self.handle, _dvec(x, n, "float32", "x"), _dvec(y, n, "float32", "y"),
+                                    1 if transpose else 0, _stream(stream)))
         return y
 
     @property
@@ -345,8 +371,10 @@ class SIPDGOperator(_Operator):
         import torch
         if out is None:
             out = torch.empty(self.space.num_elements, dtype=torch.float64, device=u.device)
-        check(lib().dgop_sipdg_gradient(self.handle, _ptr(u), _ptr(lam), None if scale is None else _ptr(scale),
-                                        _ptr(out), _stream(stream)))
+        n, ne = self.space.num_dofs, self.space.num_elements
+        check(lib().dgop_sipdg_gradient(self.handle, _dvec(u, n, name="u"), _dvec(lam, n, name="lam"),
+                                        None if scale is None else _dvec(scale, ne, name="scale"),
+                                        _dvec(out, ne, name="out"), _stream(stream)))
         return out
 
 
@@ -435,7 +463,9 @@ class _Solver:
         Returns {"success", "iterations", "relative_error"} with the reference's conventions
         (IterativeSolverResult, Solvers/iterativesolverresult.hpp:41)."""
         res = _SolveResult()
-        check(lib().dgop_solver_solve(self.handle, _ptr(b), _ptr(x), int(max_iters), float(tol), ctypes.byref(res),
+        n = self.op.space.num_dofs
+        check(lib().dgop_solver_solve(self.handle, _dvec(b, n, name="b"), _dvec(x, n, name="x"), int(max_iters),
+                                      float(tol), ctypes.byref(res),
                                       _stream(stream)))
         return {"success": bool(res.success), "iterations": res.iterations, "relative_error": res.relative_error}
 
@@ -518,8 +548,14 @@ class Batch:
         return int(lib().dgop_batch_groups(self.handle))
 
     def apply(self, xs, ys, stream=None):
-        xa = (ctypes.c_void_p * len(xs))(*[_ptr(x) for x in xs])
-        ya = (ctypes.c_void_p * len(ys))(*[_ptr(y) for y in ys])
+        xs, ys = list(xs), list(ys)
+        if not (len(xs) == len(ys) == len(self.ops)):
+            raise ValueError(f"Batch.apply: {len(self.ops)} operators need as many inputs and outputs "
+                             f"(got {len(xs)} and {len(ys)})")
+        xa = (ctypes.c_void_p * len(xs))(*[_dvec(x, o.space.num_dofs, name=f"xs[{i}]")
+                                           for i, (x, o) in enumerate(zip(xs, self.ops))])
+        ya = (ctypes.c_void_p * len(ys))(*[_dvec(y, o.space.num_dofs, name=f"ys[{i}]")
+                                           for i, (y, o) in enumerate(zip(ys, self.ops))])
         check(lib().dgop_batch_apply(self.handle, xa, ya, _stream(stream)))
 
     def close(self):
@@ -582,7 +618,9 @@ def element_dot(op, a, b, scale=None, out=None, stream=None):
     import torch
     if out is None:
         out = torch.empty(op.space.num_elements, dtype=torch.float64, device=a.device)
-    check(lib().dgop_element_dot(op.handle, _ptr(a), _ptr(b), None if scale is None else _ptr(scale), _ptr(out),
+    n, ne = op.space.num_dofs, op.space.num_elements
+    check(lib().dgop_element_dot(op.handle, _dvec(a, n, name="a"), _dvec(b, n, name="b"),
+                                 None if scale is None else _dvec(scale, ne, name="scale"), _dvec(out, ne, name="out"),
                                  _stream(stream)))
     return out
 

@@ -31,7 +31,7 @@ BASE_FLAGS = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "--expt-relaxed-conste
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 # Non-instantiation sources; gen_generic.cu is compiled once per (dimension, N).
-SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "kron_plan.cpp", "gen_kron3d.cu", "blas.cu", "krylov.cu", "host_io.cu", "batch.cu", "sipdg.cu"]
+SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "kron_plan.cpp", "gen_kron3d.cu", "krylov.cu", "host_io.cu", "batch.cu", "sipdg.cu"]
 
 
 def nvcc():
@@ -73,8 +73,9 @@ def _jobs(fast):
     jobs = []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        if os.path.exists(path):
-            jobs.append((src, path, []))
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"listed source {src} is missing from {CSRC}")
+        jobs.append((src, path, []))
     gnd = os.path.join(CSRC, "gen_kronnd.cu")
     for d in range(1, 7):
         jobs.append((f"gen_kronnd_d{d}.cu", gnd, [f"-DDGOP_GEN_D={d}"]))

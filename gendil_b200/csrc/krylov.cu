@@ -9,6 +9,7 @@
 // Scalars (alpha, beta, the Hessenberg column, Givens rotations, stopping tests) never leave the
 // device.  Inner products are deterministic: a fixed grid writes per-block partial sums with a
 // fixed reduction tree, and every consumer sums the partials in the same fixed order.
+#include <cuda.h>  // driver API types only; the functions come through cudaGetDriverEntryPointByVersion
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1108,27 +1109,78 @@ constexpr int64_t kStaticCgWords = 3 * (int64_t)DGOP_STATIC_CG_MAX_DOFS + 2 * kR
 static __device__ __align__(256) double g_static_cg_scratch[kStaticCgWords];
 
 std::mutex g_static_cg_mutex;
-double* g_static_cg_addr[64] = {};  // device address of the array, per device
+// Device address of the array per device, with the id of the CUDA context it was looked up in:
+// a device reset or a new primary context reloads the module at another address, so a cached
+// address is only used while the context it came from is still the current one.
+struct StaticCgAddr {
+  unsigned long long ctx_id = 0;
+  double* addr = nullptr;
+};
+StaticCgAddr g_static_cg_addr[64];
 thread_local int g_static_cg_flag[2];  // host copies of the `done` word (pageable; no allocation)
 
-// Device address of the array on the current device, looked up once per device.  In host code
-// the array's name is only a stand-in; the kernels must be given this address.
-int static_cg_scratch(double** out) {
+// Id of the calling thread's current CUDA context (0 when none is current).  The two driver
+// functions are fetched through the runtime, so the library needs no link against libcuda.
+int current_context_id(unsigned long long* id) {
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0);
+    if (e == cudaSuccess) e = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPointByVersion(cuCtxGetCurrent / cuCtxGetId)");
+    if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1) {
+      set_error("dgop_cg_solve_static: the driver does not provide cuCtxGetCurrent / cuCtxGetId");
+      return DGOP_ERR_CUDA;
+    }
+    get_current = reinterpret_cast<GetCurrentFn>(f0);
+    get_id = reinterpret_cast<GetIdFn>(f1);
+  }
+  CUcontext ctx = nullptr;
+  *id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return DGOP_OK;
+  unsigned long long v = 0;
+  if (get_id(ctx, &v) != CUDA_SUCCESS) return DGOP_OK;
+  *id = v;
+  return DGOP_OK;
+}
+
+// Device address of the array for the operator's device, which must be the current device.  In
+// host code the array's name is only a stand-in; the kernels must be given this address.  It is
+// looked up (cudaGetSymbolAddress) on the first call in a context and again whenever the current
+// context is not the one of the cached address.
+int static_cg_scratch(const dgop_operator* op, double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != op->device) {
+    set_error("dgop_cg_solve_static: the current device (" + std::to_string(dev) +
+              ") differs from the operator's device (" + std::to_string(op->device) + "); make it current first");
+    return DGOP_ERR_ARG;
+  }
   if (dev < 0 || dev >= 64) {
     set_error("dgop_cg_solve_static: device index out of range");
     return DGOP_ERR_ARG;
   }
   std::lock_guard<std::mutex> lock(g_static_cg_mutex);
-  if (!g_static_cg_addr[dev]) {
+  unsigned long long ctx = 0;
+  int rc = current_context_id(&ctx);
+  if (rc != DGOP_OK) return rc;
+  StaticCgAddr& c = g_static_cg_addr[dev];
+  if (!c.addr || ctx == 0 || ctx != c.ctx_id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_cg_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static CG workspace)");
-    g_static_cg_addr[dev] = static_cast<double*>(p);
+    rc = current_context_id(&ctx);  // the lookup binds the device's primary context if none was
+    if (rc != DGOP_OK) return rc;
+    c.addr = static_cast<double*>(p);
+    c.ctx_id = ctx;
   }
-  *out = g_static_cg_addr[dev];
+  *out = c.addr;
   return DGOP_OK;
 }
 
@@ -1151,7 +1203,7 @@ extern "C" int dgop_cg_solve_static(dgop_operator* op, const double* b, double* 
     return DGOP_ERR_ARG;
   }
   double* base = nullptr;
-  const int rc = static_cg_scratch(&base);
+  const int rc = static_cg_scratch(op, &base);
   if (rc != DGOP_OK) return rc;
   SolverImpl s;
   s.kind = 0;

@@ -253,8 +253,11 @@ int dgop_element_dot(const dgop_operator* op, const double* a, const double* b, 
  * vectors, partial sums and solver state live in one fixed device array inside the library
  * (about 6.3 MB, held on every GPU that loads the library until the process exits).
  *  - Operators with more than DGOP_STATIC_CG_MAX_DOFS DoFs are rejected with DGOP_ERR_ARG.
- *  - The first call on a device looks the array's device address up once (cudaGetSymbolAddress);
- *    make that first call before any stream capture on that device.
+ *  - The operator's device must be the current device (DGOP_ERR_ARG otherwise).
+ *  - The first call on a device looks the array's device address up (cudaGetSymbolAddress) and
+ *    keeps it for as long as the same CUDA context stays current; after a device reset or in a new
+ *    context the next call looks it up again.  Make the first call in a context before any
+ *    stream capture on that device.
  *  - Every call shares the one array: calls whose GPU work overlaps (other streams, other host
  *    threads on the same device) race and corrupt each other's results; serialize them.
  *  - Synchronizes `stream` before returning, like dgop_solver_solve. */
