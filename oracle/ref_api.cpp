@@ -10,6 +10,8 @@ extern "C" {
 int gref_mass_part_A( int, int, int, int, const long *, const double *, const double *, const int *, int, double, const double *, double * );
 int gref_mass_part_B( int, int, int, int, const long *, const double *, const double *, const int *, int, double, const double *, double * );
 int gref_mass_part_C( int, int, int, int, const long *, const double *, const double *, const int *, int, double, const double *, double * );
+int gref_mass_part_D( int, int, int, int, const long *, const double *, const double *, const int *, int, double, const double *, double * );
+int gref_mass_part_E( int, int, int, int, const long *, const double *, const double *, const int *, int, double, const double *, double * );
 #define GREF_ADV_DECL( P ) \
    int gref_adv_part_##P( int, int, int, int, const long *, const double *, const double *, const int *, int, int, const double *, double, int, double, const double *, double * );
 GREF_ADV_DECL( A )
@@ -17,6 +19,9 @@ GREF_ADV_DECL( B )
 GREF_ADV_DECL( C )
 GREF_ADV_DECL( D )
 GREF_ADV_DECL( E )
+GREF_ADV_DECL( F )
+GREF_ADV_DECL( G )
+GREF_ADV_DECL( H )
 
 int gref_mass_apply( int D, int P, int Q, int basis, const long * sizes, const double * h,
                      const double * origin, const int * periodic, int sigma_kind, double sigma_c,
@@ -26,7 +31,11 @@ int gref_mass_apply( int D, int P, int Q, int basis, const long * sizes, const d
    if ( rc != gref::GREF_UNSUPPORTED ) return rc;
    rc = gref_mass_part_B( D, P, Q, basis, sizes, h, origin, periodic, sigma_kind, sigma_c, x, y );
    if ( rc != gref::GREF_UNSUPPORTED ) return rc;
-   return gref_mass_part_C( D, P, Q, basis, sizes, h, origin, periodic, sigma_kind, sigma_c, x, y );
+   rc = gref_mass_part_C( D, P, Q, basis, sizes, h, origin, periodic, sigma_kind, sigma_c, x, y );
+   if ( rc != gref::GREF_UNSUPPORTED ) return rc;
+   rc = gref_mass_part_D( D, P, Q, basis, sizes, h, origin, periodic, sigma_kind, sigma_c, x, y );
+   if ( rc != gref::GREF_UNSUPPORTED ) return rc;
+   return gref_mass_part_E( D, P, Q, basis, sizes, h, origin, periodic, sigma_kind, sigma_c, x, y );
 }
 
 // mode: 0 advection without boundary faces, 1 advection with inflow value g, 2 mass + advection.
@@ -37,7 +46,8 @@ int gref_advection_apply( int D, int P, int Q, int basis, const long * sizes, co
 {
    int ( *parts[] )( int, int, int, int, const long *, const double *, const double *, const int *, int, int,
                      const double *, double, int, double, const double *, double * ) = {
-      gref_adv_part_A, gref_adv_part_B, gref_adv_part_C, gref_adv_part_D, gref_adv_part_E };
+      gref_adv_part_A, gref_adv_part_B, gref_adv_part_C, gref_adv_part_D, gref_adv_part_E,
+      gref_adv_part_F, gref_adv_part_G, gref_adv_part_H };
    for ( auto part : parts )
    {
       const int rc = part( D, P, Q, basis, sizes, h, origin, periodic, mode, beta_kind, beta_c, g, sigma_kind, sigma_c, x, y );

@@ -23,3 +23,16 @@
 
 #define GREF_CG_LIST(X) X(3,3,4,0) X(2,2,3,0) X(1,3,5,0)
 #define GREF_GMRES_LIST(X) X(3,3,4,0) X(2,2,3,0) X(1,2,4,0)
+
+// the shapes of the batched uneven instances (dimension 2..4, order 1..5, q = p + 2), mass and
+// advection; shapes already in the lists above are left out
+#define GREF_MASS_LIST_D(X) \
+   X(2,1,3,0) X(2,3,5,0) X(2,4,6,0) X(2,5,7,0) X(3,1,3,0) X(3,2,4,0) X(3,5,7,0)
+#define GREF_MASS_LIST_E(X) \
+   X(4,1,3,0) X(4,2,4,0) X(4,3,5,0) X(4,4,6,0) X(4,5,7,0) X(3,3,5,0) X(3,4,6,0)
+#define GREF_ADV_LIST_F(X) \
+   X(2,1,3,0) X(2,2,4,0) X(2,3,5,0) X(2,4,6,0) X(2,5,7,0) X(3,2,4,0) X(3,3,5,0)
+#define GREF_ADV_LIST_G(X) \
+   X(4,1,3,0) X(4,2,4,0) X(4,3,5,0) X(3,4,6,0) X(3,5,7,0)
+#define GREF_ADV_LIST_H(X) \
+   X(4,4,6,0) X(4,5,7,0)

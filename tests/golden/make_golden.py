@@ -141,6 +141,73 @@ def diffusion_cases():
     return c
 
 
+def c5_shapes():
+    """The element shapes of the batched uneven instances: dimension 2..4, order 1..5, q = p + 2,
+    constant velocity with components uniform in [-1, 1] (numpy seed 7), sigma = 1/dt = 1e3."""
+    rng = np.random.default_rng(7)
+    sizes = {2: [5, 4], 3: [3, 2, 3], 4: [2, 2, 2, 2]}
+    out = []
+    for D in (2, 3, 4):
+        for P in range(1, 6):
+            sz = [3, 2, 2, 2] if (D == 4 and P <= 2) else sizes[D]
+            beta = [float(v) for v in rng.uniform(-1.0, 1.0, D)]
+            out.append((f"c5_d{D}p{P}", dict(cube(D, 0, P, P + 2, sizes=sz), beta_kind=0, beta_c=beta, g=0.0,
+                                             sigma_kind=0, sigma_c=1e3)))
+    return out
+
+
+def sampled(arrays, key, v, stride):
+    """Every `stride`-th value of a large reference output and its max-norm, 2-norm and sum."""
+    arrays[f"{key}_sample"] = np.ascontiguousarray(v[::stride])
+    arrays[f"{key}_stats"] = np.array([np.abs(v).max(), np.linalg.norm(v), v.sum()])
+
+
+def config_fixtures(ref, cases, arrays):
+    """The benchmark configurations at their stated sizes, pinned against the reference:
+    C1 (16^3 mass, p = 3, q = 4: the apply and 20 CG iterations of M x = M u from x0 = 0),
+    C2 (64^3 implicit system sigma M + A, sigma = 1/dt = 1e3: GMRES(30) to 1e-10 from x0 = 0,
+    b = FillRandom(2); about 15 minutes on 8 cores), C3 (the 6D phase-space operator on a 4^6 mesh:
+    interior faces on every axis) and the shapes of C5 (full outputs).  Large outputs are stored as
+    strided samples plus norms."""
+    c1 = dict(cube(3, 16, 3, 4), sigma_kind=0, sigma_c=1.0, seed=0, cg_iters=20, cg_tol=0.0, stride=61)
+    u = ref.fill_random(num_dofs(c1), 0)
+    y = ref.mass_apply(c1, u)
+    sampled(arrays, "c1_y", y, c1["stride"])
+    # the reference's CG on this system amplifies rounding from about 8 iterations on (its own
+    # iterates at 1 and 3 OpenMP threads differ by 3e-14 after 5 iterations, 1.4e-11 after 8 and
+    # 4e-3 after 20), so the trace is stored at 5 and 8 iterations as well as at 20
+    traces = {}
+    for k in (5, 8, c1["cg_iters"]):
+        x, info = ref.mass_cg(c1, y, np.zeros_like(y), k, c1["cg_tol"])
+        sampled(arrays, f"c1_x{k}", x, c1["stride"])
+        traces[str(k)] = info
+    cases["configs"].append({"id": "c1", "kind": "mass_cg", **c1, "traces": traces})
+    print("c1", traces, flush=True)
+
+    c3 = dict(cube(6, 4, 2, 3, h=[0.25] * 3 + [0.5] * 3, origin=[0.0] * 3 + [-1.0] * 3), beta_kind=3, g=0.0,
+              seed=1, stride=97)
+    x3 = ref.fill_random(num_dofs(c3), 1)
+    sampled(arrays, "c3_y", ref.advection_apply(c3, x3, 1), c3["stride"])
+    cases["configs"].append({"id": "c3", "kind": "advection_apply", "mode": 1, **c3})
+    print("c3 done", flush=True)
+
+    for cid, case in c5_shapes():
+        case = dict(case, seed=1)
+        xc = ref.fill_random(num_dofs(case), 1)
+        arrays[f"{cid}_mass_y"] = ref.mass_apply(case, xc)
+        arrays[f"{cid}_adv_y"] = ref.advection_apply(case, xc, 1)
+        cases["configs"].append({"id": cid, "kind": "system_parts", **case})
+    print("c5 done", flush=True)
+
+    c2 = dict(cube(3, 64, 3, 4), beta_kind=2, g=0.0, sigma_c=1e3, seed=2, restart=30, tol=1e-10, max_iters=5000,
+              stride=4099)
+    b = ref.fill_random(num_dofs(c2), 2)
+    x2, info = ref.system_gmres(c2, b, np.zeros_like(b), c2["max_iters"], c2["restart"], c2["tol"])
+    sampled(arrays, "c2_x", x2, c2["stride"])
+    cases["configs"].append({"id": "c2", "kind": "system_gmres", **c2, **info, "threads": ref.num_threads()})
+    print("c2", info, flush=True)
+
+
 def main(only=None):
     """Write cases.json and golden.npz.  With `only` (a case kind), regenerate that kind alone and
     keep every other stored case and array as it is (the OpenMP reference solvers' last bits
@@ -150,6 +217,7 @@ def main(only=None):
             old_cases = json.load(f)
         with np.load(os.path.join(HERE, "golden.npz")) as z:
             old_arrays = {k: z[k] for k in z.files}
+        old_cases.setdefault("configs", [])
         new_cases, new_arrays = build(only)
         kinds = [only] + (["diffusion"] if only == "sipdg" else [])
         ids = {c["id"] for k in kinds for c in new_cases[k]}
@@ -174,10 +242,13 @@ def write(cases, arrays):
 
 def build(only):
     ref = Reference()
-    cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": [], "diffusion": []}
+    cases = {"mass": [], "advection": [], "cg": [], "gmres": [], "sipdg": [], "diffusion": [], "configs": []}
     arrays = {}
     if only == "sipdg":
         sipdg_fixtures(ref, cases, arrays)
+        return cases, arrays
+    if only == "configs":
+        config_fixtures(ref, cases, arrays)
         return cases, arrays
     for seed in (0, 1, 2, 3, 12345):
         arrays[f"rng_seed{seed}"] = ref.fill_random(256, seed)
@@ -198,6 +269,7 @@ def build(only):
             arrays[f"{cid}_mode{mode}_y"] = ref.advection_apply(case, x, mode)
         cases["advection"].append({"id": cid, **case})
     sipdg_fixtures(ref, cases, arrays)
+    config_fixtures(ref, cases, arrays)
     # CG on the mass operator: b = M u (u from seed 0), x0 = 0 (conjugategradient.hpp:125)
     for cid, case, iters, tol in (("cg1", dict(cube(3, 4, 3, 4), sigma_kind=0, sigma_c=1.0), 20, 1e-6),
                                   ("cg2", dict(cube(3, 4, 3, 4), sigma_kind=1), 500, 1e-12),
@@ -251,5 +323,5 @@ def sipdg_fixtures(ref, cases, arrays):
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["sipdg"], help="regenerate one case kind, keep the rest")
+    ap.add_argument("--only", choices=["sipdg", "configs"], help="regenerate one case kind, keep the rest")
     main(ap.parse_args().only)

