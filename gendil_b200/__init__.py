@@ -35,6 +35,7 @@ LIB_PATH = os.path.join(_PKG, "libdgop.so")
 GLL, GL = 0, 1
 BC_NONE, BC_INFLOW = 0, 1
 MAX_TERMS, MAX_DIM = 4, 6
+MAX_VARIANTS = 6  # DGOP_MAX_VARIANTS
 
 
 class DGOPError(RuntimeError):
@@ -93,11 +94,13 @@ def lib():
         L.dgop_operator_set_variant.argtypes = [vp, i]
         L.dgop_operator_variant_time.argtypes = [vp, i, ctypes.POINTER(ctypes.c_float)]
         L.dgop_operator_variant_f32.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_float)]
+        L.dgop_operator_device_error.argtypes = [vp, ctypes.POINTER(i)]
         L.dgop_cg_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.dgop_gmres_create.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.dgop_gmres_ir_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
         L.dgop_solver_set_graphs.argtypes = [vp, i]
         L.dgop_solver_set_transpose.argtypes = [vp, i]
+        L.dgop_solver_set_fused_dot.argtypes = [vp, i]
         L.dgop_solver_set_preconditioner.argtypes = [vp, vp]
         L.dgop_sipdg_create.argtypes = [vp, i, vp, ctypes.c_double, ctypes.c_double, i, ctypes.POINTER(vp)]
         L.dgop_mass_inverse_create.argtypes = [vp, i, vp, ctypes.POINTER(vp)]
@@ -133,6 +136,9 @@ def _ptr(t):
     return t.data_ptr()
 
 
+_TORCH_DTYPES = {}
+
+
 def _dvec(t, n, dtype="float64", name="vector"):
     """Device address of a contiguous CUDA tensor of exactly `n` values of `dtype`.  The kernels
     read and write `n` values through this address, so a CPU tensor, another dtype, a strided view
@@ -140,6 +146,15 @@ def _dvec(t, n, dtype="float64", name="vector"):
     A plain integer is taken as a raw device address whose size the caller vouches for."""
     if isinstance(t, int):
         return t
+    want = _TORCH_DTYPES.get(dtype)
+    if want is None:
+        import torch
+        want = _TORCH_DTYPES[dtype] = getattr(torch, dtype)
+    try:
+        if t.is_cuda and t.dtype is want and t.numel() == n and t.is_contiguous():
+            return t.data_ptr()
+    except AttributeError:
+        pass
     if not getattr(t, "is_cuda", False):
         raise ValueError(f"{name}: a CUDA tensor is required")
     if str(t.dtype) != f"torch.{dtype}":
@@ -292,7 +307,7 @@ class _Operator:
     def select_kernel(self, name):
         check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1, "kronnd": 2}[name]))
 
-    VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl")  # 3D register kernel ("kron")
+    VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl", "tma1-tile", "tma2-shfl", "tma2-tile")  # 3D ("kron")
     ND_VARIANTS = ("nd-passes", "nd-grouped2", "nd-grouped3")  # any-dimension kernel ("kronnd")
 
     def _variants(self):
@@ -311,10 +326,17 @@ class _Operator:
     def variant_f32(self):
         """(variant name, {name: autotuner ms or -1 when unusable}) of the FP32 kernel configuration."""
         v = ctypes.c_int()
-        ms = (ctypes.c_float * 3)()
+        ms = (ctypes.c_float * MAX_VARIANTS)()
         check(lib().dgop_operator_variant_f32(self.handle, ctypes.byref(v), ms))
         names = self._variants()
         return (None if v.value < 0 else names[v.value]), {n: ms[i] for i, n in enumerate(names)}
+
+    def device_error(self):
+        """Read and clear the operator's device error word (non-zero: a kernel's bounded wait for
+        an asynchronous copy ran out and that launch's results are invalid)."""
+        err = ctypes.c_int()
+        check(lib().dgop_operator_device_error(self.handle, ctypes.byref(err)))
+        return err.value
 
     def variant_times(self):
         """Autotuner time per launch (ms) of every variant (0.0: not available or not timed; the
@@ -478,6 +500,12 @@ class _Solver:
     def transpose(self, enable=True):
         """Solve with the transposed operator A^T (adjoint solves)."""
         check(lib().dgop_solver_set_transpose(self.handle, 1 if enable else 0))
+        return self
+
+    def fused_dot(self, enable=True):
+        """Form the first inner product of every iteration in the operator kernel's epilogue
+        (default; 3D Kronecker-form operators) or in a separate pass."""
+        check(lib().dgop_solver_set_fused_dot(self.handle, 1 if enable else 0))
         return self
 
     def use_graphs(self, enable=True):

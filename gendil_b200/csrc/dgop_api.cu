@@ -1,4 +1,5 @@
 // C-ABI implementation: spaces, operators, coefficient tables, launch configuration.
+#include <cuda.h>  // tensor-map types; cuTensorMapEncodeTiled comes through cudaGetDriverEntryPointByVersion
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,6 +14,7 @@
 
 #include "basis.h"
 #include "kron_plan.h"
+#include "kron_tma.h"
 #include "dgop_internal.h"
 
 namespace dgop {
@@ -249,6 +251,131 @@ SepCoef sep_of(const dgop_coef* c) {
   return s;
 }
 
+// cuTensorMapEncodeTiled, fetched from the driver once (no link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// One FP64 tensor map (dims, byte strides of dims 1.., box) over a 16-byte aligned vector.
+int encode_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+               const cuuint32_t* box, CUtensorMapSwizzle swizzle) {
+  const EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return DGOP_ERR_CUDA;
+  }
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void*>(base), dims, strides,
+                         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return DGOP_ERR_CUDA;
+  }
+  return DGOP_OK;
+}
+
+// The four maps of the bulk-tensor variants (kron3d_tma_kernel.cuh) for vectors x and y of
+// `nelem` elements of 4 x 4 x 4 values.
+int encode_tma_maps(KronTmaParams<double>& T, const double* x, double* y, int64_t nelem) {
+  const cuuint64_t rows = (cuuint64_t)nelem * 4;
+  const cuuint64_t d2[2] = {16, rows}, s2[1] = {128};
+  const cuuint32_t b2[2] = {16, 32};
+  const cuuint64_t d3[3] = {16, 4, (cuuint64_t)nelem}, s3[2] = {128, 512};
+  const cuuint32_t b3[3] = {16, 1, 8};
+  const cuuint64_t d4[4] = {4, 4, 4, (cuuint64_t)nelem}, s4[3] = {32, 128, 512};
+  const cuuint32_t b4[4] = {4, 1, 4, 8};
+  int rc = encode_map(&T.win, x, 2, d2, s2, b2, CU_TENSOR_MAP_SWIZZLE_128B);
+  if (rc == DGOP_OK) rc = encode_map(&T.zsl, x, 3, d3, s3, b3, CU_TENSOR_MAP_SWIZZLE_128B);
+  if (rc == DGOP_OK) rc = encode_map(&T.ysl, x, 4, d4, s4, b4, CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (rc == DGOP_OK) rc = encode_map(&T.out, y, 2, d2, s2, b2, CU_TENSOR_MAP_SWIZZLE_128B);
+  return rc;
+}
+
+// Launch kernel variant v of the 3D Kronecker form with parameters p (x, y, flags, range set).
+// Bulk-tensor variants need element ranges in whole groups of 8; other ranges take the fastest
+// variant without them.
+std::mutex g_map_cache_mutex;
+
+// The four maps for (x, y), from the operator's cache of recent pairs or freshly encoded.
+int tma_maps_cached(KronCfg<double>& K, KronTmaParams<double>& T, const double* x, double* y, int64_t nelem) {
+  static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
+  std::lock_guard<std::mutex> lock(g_map_cache_mutex);
+  for (const auto& m : K.map_cache) {
+    if (m.x == x && m.y == y) {
+      std::memcpy(&T.win, m.maps[0], 128);
+      std::memcpy(&T.zsl, m.maps[1], 128);
+      std::memcpy(&T.ysl, m.maps[2], 128);
+      std::memcpy(&T.out, m.maps[3], 128);
+      return DGOP_OK;
+    }
+  }
+  const int rc = encode_tma_maps(T, x, y, nelem);
+  if (rc != DGOP_OK) return rc;
+  auto& m = K.map_cache[K.map_next];
+  K.map_next = (K.map_next + 1) % 8;
+  std::memcpy(m.maps[0], &T.win, 128);
+  std::memcpy(m.maps[1], &T.zsl, 128);
+  std::memcpy(m.maps[2], &T.ysl, 128);
+  std::memcpy(m.maps[3], &T.out, 128);
+  m.x = x;
+  m.y = y;
+  return DGOP_OK;
+}
+
+template <typename Real>
+int launch_kron(const dgop_operator* op, KronCfg<Real>& K, int v, const KronParams<Real>& p, cudaStream_t s) {
+  const bool whole = p.e_begin % 8 == 0 && p.nelem % 8 == 0;
+  if (K.entry->v[v].launch_tma && !whole) v = K.fallback;
+  const KronVariant<Real>& kv = K.entry->v[v];
+  const auto& L = K.launch[v];
+  if (kv.launch_tma) {
+    if constexpr (sizeof(Real) == 8) {
+      KronTmaParams<double> T;
+      std::memset(&T, 0, sizeof(T));
+      T.k = p;
+      const int rc = tma_maps_cached(K, T, p.x, p.y, op->sp.nelem);
+      if (rc != DGOP_OK) return rc;
+      const int tr = (p.flags & kTranspose) ? 1 : 0;
+      T.eflags = K.d_eflags[tr];
+      T.gwords = K.d_gwords[tr];
+      T.err = K.d_err;
+      for (int& m : T.mat_index) m = -1;
+      T.nmat = 0;
+      for (int k = 0; k < 8; ++k)
+        if (p.vary[tma_yz_slot(k)]) T.mat_index[tma_yz_slot(k)] = T.nmat++;
+      kv.launch_tma(T, L.grid, L.block, L.smem, s);
+    }
+  } else {
+    kv.launch(p, L.grid, L.block, L.smem, s);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
+  return DGOP_OK;
+}
+
+// Let kernel f use dynamic shared memory up to the device's per-block opt-in limit, net of its
+// static shared memory (the attribute is rejected when static + dynamic exceed the limit).
+int allow_dynamic_smem(const void* f, int max_smem) {
+  cudaFuncAttributes attr;
+  DGOP_CUDA(cudaFuncGetAttributes(&attr, f));
+  DGOP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)attr.sharedSizeBytes));
+  return DGOP_OK;
+}
+
 template <typename Real>
 int upload(Real** dst, const double* src, size_t n) {
   std::vector<Real> tmp(src, src + n);
@@ -370,22 +497,41 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
   }
   // persistent grid: every warp walks groups of entry->epw consecutive elements; one launch
   // shape per kernel variant (their shared memory per warp differs)
-  const int threads = kKronThreads, warps = threads / 32;
   int max_smem = 0;
   DGOP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
   const bool sep = plan.has_adv && plan.has_mass && !plan.mass_merged;
   const int64_t groups = (s.nelem + entry->epw - 1) / entry->epw;
+  // bulk-tensor variants: groups of 8 elements inside one x-row, plane rows addressable by int
+  const bool tma_shape = entry->face_words && s.sizes[0] % 8 == 0 && s.nelem % 8 == 0 &&
+                         s.nelem < (int64_t(1) << 29) && tensor_map_encoder() != nullptr;
+  if (tma_shape) {
+    for (int tr = 0; tr < 2; ++tr) {
+      DGOP_CUDA(cudaMalloc(&K.d_eflags[tr], sizeof(uint32_t) * s.nelem));
+      DGOP_CUDA(cudaMalloc(&K.d_gwords[tr], sizeof(uint32_t) * (s.nelem / 8)));
+      KronParams<Real> q = tr ? K.params_t : p;
+      q.flags = op->flags | (tr ? kTranspose : 0);
+      entry->face_words(q, K.d_eflags[tr], K.d_gwords[tr], 0);
+      DGOP_CUDA(cudaGetLastError());
+    }
+    DGOP_CUDA(cudaMalloc(&K.d_err, sizeof(int)));
+    DGOP_CUDA(cudaMemset(K.d_err, 0, sizeof(int)));
+    DGOP_CUDA(cudaDeviceSynchronize());
+  }
   int usable = 0;
   for (int v = 0; v < kKronVariants; ++v) {
     const KronVariant<Real>& kv = entry->v[v];
     auto& L = K.launch[v];
     L.ok = false;
-    if (!kv.launch) continue;
+    if (!kv.launch && !(kv.launch_tma && tma_shape)) continue;
+    const int threads = kv.threads, warps = threads / 32;
     L.block = dim3(threads);
-    L.smem = (size_t)warps * kv.warp_smem * sizeof(Real);
-    if ((int)L.smem > max_smem) continue;
-    DGOP_CUDA(cudaFuncSetAttribute(kv.func, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    DGOP_CUDA(cudaFuncSetAttribute(kv.func_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    L.smem = kv.launch_tma ? (size_t)kv.warp_smem : (size_t)warps * kv.warp_smem * sizeof(Real);
+    if ((int)L.smem > max_smem - 1024) continue;  // 1 KB covers every variant's static shared memory
+    int arc = allow_dynamic_smem(kv.func, max_smem);
+    if (arc == DGOP_OK) arc = allow_dynamic_smem(kv.func_sep, max_smem);
+    for (const void* f : kv.func_dot)
+      if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
+    if (arc != DGOP_OK) return arc;
     int per_sm = 0;
     DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? kv.func_sep : kv.func, threads, L.smem));
     if (per_sm < 1) continue;
@@ -394,6 +540,7 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
     L.ok = true;
     ++usable;
   }
+  K.fallback = K.launch[1].ok ? 1 : 0;
   if (!usable) {
     set_error("Kronecker kernel shared memory exceeds the device limit");
     return DGOP_ERR_UNSUPPORTED;
@@ -433,11 +580,11 @@ int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
     p.beta_y = Real(0);
     p.flags = op->flags;
     p.skip = nullptr;
-    K.entry->v[v].launch(p, L.grid, L.block, L.smem, 0);
+    ok = launch_kron(op, K, v, p, 0) == DGOP_OK;
     cudaEventRecord(e0, 0);
-    for (int r = 0; r < 3; ++r) K.entry->v[v].launch(p, L.grid, L.block, L.smem, 0);
+    for (int r = 0; ok && r < 3; ++r) ok = launch_kron(op, K, v, p, 0) == DGOP_OK;
     cudaEventRecord(e1, 0);
-    ok = cudaEventSynchronize(e1) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    ok = ok && cudaEventSynchronize(e1) == cudaSuccess && cudaGetLastError() == cudaSuccess;
     float ms = 0.0f;
     if (ok) cudaEventElapsedTime(&ms, e0, e1);
     L.ms = ms / 3.0f;
@@ -445,6 +592,8 @@ int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
       best_ms = L.ms;
       best = v;
     }
+    if (ok && !K.entry->v[v].launch_tma && (K.launch[K.fallback].ms == 0.0f || L.ms < K.launch[K.fallback].ms))
+      K.fallback = v;
   }
   if (x) cudaFree(x);
   if (y) cudaFree(y);
@@ -801,6 +950,11 @@ void free_kronnd(KronNDCfg<Real>& K) {
 
 template <typename Real>
 void free_kron(KronCfg<Real>& K) {
+  for (int tr = 0; tr < 2; ++tr) {
+    if (K.d_eflags[tr]) cudaFree(K.d_eflags[tr]);
+    if (K.d_gwords[tr]) cudaFree(K.d_gwords[tr]);
+  }
+  if (K.d_err) cudaFree(K.d_err);
   if (K.d_mats) cudaFree(K.d_mats);
   if (K.d_phi) cudaFree(K.d_phi);
   if (K.d_sgn) cudaFree(K.d_sgn);
@@ -997,8 +1151,10 @@ __global__ void __launch_bounds__(256) copy_kernel(const Real* __restrict__ x, R
 template <typename Real>
 static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, KronNDCfg<Real>& KN,
                        KronDiffCfg<Real>& SD, Real alpha, const Real* x, Real beta_y, Real* y, int extra_flags,
-                       cudaStream_t s, const int* skip, int64_t e_begin = 0, int64_t e_end = -1) {
+                       cudaStream_t s, const int* skip, int64_t e_begin = 0, int64_t e_end = -1,
+                       const DotEpilogue* dot = nullptr) {
   if (e_end < 0) e_end = op->sp.nelem;
+  if (dot && dot->fused) *dot->fused = false;
   if (!x || !y) {
     set_error("null vector");
     return DGOP_ERR_ARG;
@@ -1082,11 +1238,23 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
     p.e_begin = e_begin;
     p.nelem = e_end;
     if (linear) p.g = Real(0);
-    const auto& KL = K.launch[K.variant];
-    K.entry->v[K.variant].launch(p, KL.grid, KL.block, KL.smem, s);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
-    return DGOP_OK;
+    p.dot_z = nullptr;
+    p.dot_partials = nullptr;
+    p.dot_count = 0;
+    if constexpr (sizeof(Real) == 8) {
+      // the fused inner product needs a 16-byte aligned z and a grid no larger than the reader's
+      // partial count (the fallback variant's grid when the element range forces it)
+      const bool whole = e_begin % 8 == 0 && e_end % 8 == 0;
+      const int v = (K.entry->v[K.variant].launch_tma && !whole) ? K.fallback : K.variant;
+      if (dot && dot->z && dot->partials && reinterpret_cast<uintptr_t>(dot->z) % 16 == 0 &&
+          (int64_t)K.launch[v].grid.x <= dot->count) {
+        p.dot_z = dot->z;
+        p.dot_partials = dot->partials;
+        p.dot_count = dot->count;
+        if (dot->fused) *dot->fused = true;
+      }
+    }
+    return launch_kron(op, K, K.variant, p, s);
   }
   if (!L.ready) {
     set_error("operator has no kernel for this precision");
@@ -1109,8 +1277,9 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
 }
 
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
-               cudaStream_t s, const int* skip) {
-  return launch_impl<double>(op, op->f64, op->k64, op->n64, op->s64, alpha, x, beta_y, y, extra_flags, s, skip);
+               cudaStream_t s, const int* skip, const DotEpilogue* dot) {
+  return launch_impl<double>(op, op->f64, op->k64, op->n64, op->s64, alpha, x, beta_y, y, extra_flags, s, skip, 0,
+                             -1, dot);
 }
 
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
@@ -1419,6 +1588,7 @@ int dgop_operator_variant_f32(const dgop_operator* op, int* variant, float* ms) 
     *variant = op->k32.variant;
     for (int v = 0; v < kKronVariants; ++v) ms[v] = op->k32.launch[v].ok ? op->k32.launch[v].ms : -1.0f;
   } else {
+    for (int v = 0; v < DGOP_MAX_VARIANTS; ++v) ms[v] = -1.0f;
     *variant = -1;
   }
   return DGOP_OK;
@@ -1434,6 +1604,26 @@ int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms) 
     return DGOP_ERR_ARG;
   }
   *ms = op->k64.launch[variant].ms;
+  return DGOP_OK;
+}
+
+static_assert(kKronVariants <= DGOP_MAX_VARIANTS && kKronNDVariants <= DGOP_MAX_VARIANTS, "variant table size");
+
+int dgop_operator_device_error(const dgop_operator* op, int* error) {
+  if (!op || !error) {
+    set_error("dgop_operator_device_error: null argument");
+    return DGOP_ERR_ARG;
+  }
+  *error = 0;
+  for (int* w : {op->k64.d_err, op->k32.d_err}) {
+    if (!w) continue;
+    int v = 0;
+    DGOP_CUDA(cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v) {
+      *error |= v;
+      DGOP_CUDA(cudaMemset(w, 0, sizeof(int)));
+    }
+  }
   return DGOP_OK;
 }
 

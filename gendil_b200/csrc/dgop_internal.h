@@ -48,10 +48,24 @@ struct KronCfg {
     float ms = 0.0f;  // autotuner timing (0: not timed)
   } launch[kKronVariants];
   int variant = 0;  // the kernel variant in use
+  int fallback = 1;  // fastest variant without bulk-tensor staging (element ranges not in whole groups)
   Real* d_mats = nullptr;
   Real* d_phi = nullptr;
   signed char* d_sgn = nullptr;
   Real* d_elem[4] = {};  // converted per-element factors (FP32 only)
+  // bulk-tensor variants: face words per element and slot words per group of 8 elements, for
+  // the forward [0] and transposed [1] operator; a device word set when a bounded wait gives up
+  uint32_t* d_eflags[2] = {};
+  uint32_t* d_gwords[2] = {};
+  int* d_err = nullptr;
+  // tensor maps of recent (x, y) pairs (opaque CUtensorMap bytes: group, z slices, y slices, out)
+  struct MapEntry {
+    const void* x = nullptr;
+    const void* y = nullptr;
+    alignas(64) unsigned char maps[4][128];
+  };
+  MapEntry map_cache[8];
+  int map_next = 0;
 };
 
 template <typename Real>
@@ -125,10 +139,19 @@ struct dgop_operator {
 };
 
 namespace dgop {
+// Optional epilogue of an FP64 apply: partials[b] = sum over CTA b's outputs of z . y in a fixed
+// order, entries past the grid zeroed up to `count`.  Kernels that provide it set `*fused`; for
+// the others the caller computes the product itself.
+struct DotEpilogue {
+  const double* z = nullptr;
+  double* partials = nullptr;
+  int count = 0;
+  bool* fused = nullptr;
+};
 // Launch the operator kernel: y = alpha * Op(x) + beta_y * y, with `extra_flags` or-ed in.
 // When `skip` (a device word) is non-zero at run time the launch does nothing.
 int launch_f64(dgop_operator* op, double alpha, const double* x, double beta_y, double* y, int extra_flags,
-               cudaStream_t s, const int* skip = nullptr);
+               cudaStream_t s, const int* skip = nullptr, const DotEpilogue* dot = nullptr);
 int launch_bf16(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,
                 cudaStream_t s, const int* skip);
 int launch_f32(dgop_operator* op, float alpha, const float* x, float beta_y, float* y, int extra_flags,

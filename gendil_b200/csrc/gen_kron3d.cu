@@ -1,17 +1,29 @@
 // Instantiations of the 3D Kronecker-form kernel, N = 1..5, FP64 and FP32, every variant.
 #include "kron3d_kernel.cuh"
+#include "kron3d_tma_kernel.cuh"
 #include "kron_registry.h"
+
+#include <type_traits>
 
 namespace dgop {
 
-const char* const kKronVariantNames[kKronVariants] = {"stage2-tile", "stage1-tile", "stage2-shfl"};
+const char* const kKronVariantNames[kKronVariants] = {"stage2-tile", "stage1-tile", "stage2-shfl",
+                                                      "tma1-tile",   "tma2-shfl",   "tma2-tile"};
 // (the any-dimension kernel's variants, kronnd_kernel.cuh, named here with the 3D kernel's)
 const char* const kKronNDVariantNames[kKronNDVariants] = {"nd-passes", "nd-grouped2", "nd-grouped3"};
 
 namespace {
 template <int N, typename Real, int STAGES, bool SHFL>
 void launch_kron3d(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
-  if (p.has_adv && p.has_mass && !p.mass_merged) kron3d_kernel<N, Real, true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+  const bool sep = p.has_adv && p.has_mass && !p.mass_merged;
+  if constexpr (std::is_same<Real, double>::value) {
+    if (p.dot_partials) {
+      if (sep) kron3d_kernel<N, Real, true, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+      else kron3d_kernel<N, Real, false, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+      return;
+    }
+  }
+  if (sep) kron3d_kernel<N, Real, true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
   else kron3d_kernel<N, Real, false, STAGES, SHFL><<<grid, block, smem, s>>>(p);
 }
 
@@ -20,7 +32,42 @@ void fill_variant(KronVariant<Real>& v) {
   v.launch = &launch_kron3d<N, Real, STAGES, SHFL>;
   v.func = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, STAGES, SHFL>);
   v.func_sep = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, STAGES, SHFL>);
+  if constexpr (std::is_same<Real, double>::value) {
+    v.func_dot[0] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, STAGES, SHFL, true>);
+    v.func_dot[1] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, STAGES, SHFL, true>);
+  }
   v.warp_smem = Kron3DShape<N, Real>::warp_smem(STAGES, SHFL);
+  v.threads = kKronThreads;
+}
+
+template <int STAGES, bool SHFL>
+void launch_tma(const KronTmaParams<double>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  const bool sep = p.k.has_adv && p.k.has_mass && !p.k.mass_merged;
+  if (p.k.dot_partials) {
+    if (sep) kron3d_tma_kernel<true, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+    else kron3d_tma_kernel<false, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+  } else {
+    if (sep) kron3d_tma_kernel<true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+    else kron3d_tma_kernel<false, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+  }
+}
+
+template <int STAGES, bool SHFL>
+void fill_tma(KronVariant<double>& v) {
+  v.launch_tma = &launch_tma<STAGES, SHFL>;
+  v.func = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, STAGES, SHFL>);
+  v.func_sep = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, STAGES, SHFL>);
+  v.func_dot[0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, STAGES, SHFL, true>);
+  v.func_dot[1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, STAGES, SHFL, true>);
+  v.warp_smem = kTmaWarps * tma_warp_bytes(STAGES, SHFL) + 1024;  // bytes per CTA, with the alignment slack
+  v.threads = kTmaWarps * 32;
+}
+
+template <typename Real>
+void face_words(const KronParams<Real>& p, uint32_t* eflags, uint32_t* gwords, cudaStream_t s) {
+  const int64_t groups = (p.nelem + 7) / 8;
+  const int64_t blocks = (groups * 32 + 255) / 256;
+  kron_face_words<Real><<<(unsigned)blocks, 256, 0, s>>>(p, eflags, gwords);
 }
 
 template <int N, typename Real>
@@ -29,6 +76,12 @@ void fill(KronEntry<Real>& d) {
   fill_variant<N, Real, 2, false>(d.v[0]);
   fill_variant<N, Real, 1, false>(d.v[1]);
   if constexpr (Kron3DShape<N, Real>::BUTTERFLY) fill_variant<N, Real, 2, true>(d.v[2]);
+  if constexpr (N == 4 && std::is_same<Real, double>::value) {
+    fill_tma<1, false>(d.v[3]);
+    fill_tma<2, true>(d.v[4]);
+    fill_tma<2, false>(d.v[5]);
+    d.face_words = &face_words<Real>;
+  }
 }
 
 template <int N>

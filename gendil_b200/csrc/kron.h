@@ -77,6 +77,11 @@ struct KronParams {
   const Real* elem[3];           // per-element beta_a factor or nullptr
   const Real* elem_mass;         // per-element sigma factor or nullptr
   const int* skip;               // device word; the launch does nothing when it is non-zero
+  // optional epilogue: dot_partials[b] = sum over CTA b's outputs of dot_z . y (fixed order),
+  // entries b >= gridDim.x of the first dot_count zeroed (dot_partials null: no epilogue)
+  const Real* dot_z;
+  double* dot_partials;
+  int dot_count;
 };
 
 // Launch parameters of the any-dimension kernel (kronnd_kernel.cuh).

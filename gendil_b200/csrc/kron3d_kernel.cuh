@@ -601,11 +601,14 @@ __device__ __forceinline__ void stage_group(const KronParams<Real>& P, int64_t e
   if (t == 0) *reinterpret_cast<uint32_t*>(rb + 12) = flags;
 }
 
+constexpr int kron_max_warps = 4;  // warps per CTA of kron3d_kernel (128 threads)
+
 // Kernel variants (chosen per operator by the autotuner):
 //   STAGES 2: the next group is staged while this one computes; 1: no overlap inside the warp,
 //   less shared memory per warp and so more warps per SM
 //   SHFL:    layout exchanges by shuffle butterflies (even N) instead of the shared tile
-template <int N, typename Real, bool SEP, int STAGES, bool SHFL>
+//   DOT:     the inner-product epilogue (P.dot_partials; FP64 solvers) is compiled in
+template <int N, typename Real, bool SEP, int STAGES, bool SHFL, bool DOT = false>
 __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ KronParams<Real> P) {
   using S = Kron3DShape<N, Real>;
   constexpr int NN = S::NN, NNN = S::NNN, EPW = S::EPW;
@@ -620,6 +623,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
   const bool adv = P.has_adv != 0;
   const bool slot = le < EPW;
   if (P.skip && *P.skip) return;  // a finished solve: nothing to do
+  [[maybe_unused]] double dot_acc = 0.0;
 
   int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if constexpr (STAGES == 2) {
@@ -839,11 +843,32 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
           for (int q = 0; q < S::CR; ++q) v[q] = alpha * v[q] + by * o[q];
         }
         vstore<Real, S::CR>(dst + d, v);
+        if constexpr (DOT) {
+          Real z[S::CR];
+          vldg<Real, S::CR>(P.dot_z + e0 * NNN + d, z);
+#pragma unroll
+          for (int q = 0; q < S::CR; ++q) dot_acc += (double)v[q] * (double)z[q];
+        }
       }
     }
     __syncwarp();  // the buffer is refilled by a later prefetch
   }
   cp_async_wait<0>();
+  if constexpr (DOT) {
+    // fixed-order sums: lanes (tree), warps (in order), one partial per CTA; entries past the grid
+    // are zeroed so a reader sums a fixed count
+    __shared__ double wsum[kron_max_warps];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dot_acc += __shfl_down_sync(0xffffffffu, dot_acc, o);
+    if (lane == 0) wsum[warp] = dot_acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += wsum[w];
+      P.dot_partials[blockIdx.x] = s;
+      for (int i = blockIdx.x + gridDim.x; i < P.dot_count; i += gridDim.x) P.dot_partials[i] = 0.0;
+    }
+  }
 }
 
 }  // namespace dgop

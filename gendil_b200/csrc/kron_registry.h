@@ -15,21 +15,32 @@ constexpr int kKronTCThreads = 128;  // tensor-core variant: four warps (element
 //   0: two staging stages, exchanges through the shared tile
 //   1: one staging stage (more warps per SM), exchanges through the shared tile
 //   2: two staging stages, exchanges by shuffle butterflies (even N only)
-constexpr int kKronVariants = 3;
+//   3-5: element groups moved by the Tensor Memory Accelerator (kron3d_tma_kernel.cuh; N = 4,
+//        FP64, x extent a multiple of 8): one stage + tile, two stages + shuffles, two stages + tile
+constexpr int kKronVariants = 6;
 extern const char* const kKronVariantNames[kKronVariants];
+
+template <typename Real>
+struct KronTmaParams;
 
 template <typename Real>
 struct KronVariant {
   void (*launch)(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  // bulk-tensor variants take the tensor maps and face words as well
+  void (*launch_tma)(const KronTmaParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func = nullptr;      // kernel symbol (mass merged or absent)
   const void* func_sep = nullptr;  // kernel symbol with a separate mass term
-  int warp_smem = 0;               // Real values of shared memory per warp
+  const void* func_dot[2] = {};    // with the inner-product epilogue (mass merged / separate; FP64)
+  int warp_smem = 0;               // Real values of shared memory per warp (bytes per CTA for bulk-tensor variants)
+  int threads = 0;                 // threads per CTA
 };
 
 template <typename Real>
 struct KronEntry {
   int epw = 0;  // elements per warp group
   KronVariant<Real> v[kKronVariants];
+  // per-element face words / per-group slot words of the bulk-tensor variants
+  void (*face_words)(const KronParams<Real>& p, uint32_t* eflags, uint32_t* gwords, cudaStream_t s) = nullptr;
 };
 
 KronEntry<double>& kron3d_slot_f64(int N);

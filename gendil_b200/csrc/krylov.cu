@@ -563,6 +563,9 @@ struct SolverImpl {
   int key_prec_version = -1;
   // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // the operator kernel forms the first inner product of an iteration (CG: p . Ap; GMRES:
+  // V_0 . w) in its epilogue when it can; off: a separate pass, as in the reference
+  bool fuse_dot = true;
 };
 
 }  // namespace dgop
@@ -705,8 +708,12 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
   const int* done = &cs->done;
   auto chunk = [&](cudaStream_t q) -> int {
     for (int kk = 0; kk < kCheckEvery; ++kk) {
-      DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, s.op_flags, q, done));
-      k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(p), static_cast<const double*>(tmp), n, pa, done);
+      // Ap = A p with p . Ap formed in the operator's epilogue (conjugategradient.hpp:176-179)
+      bool fused = false;
+      const DotEpilogue de{p, pa, kRB, &fused};
+      DGOP_TRY(launch_f64(s.op, 1.0, p, 0.0, tmp, s.op_flags, q, done, s.fuse_dot ? &de : nullptr));
+      if (!fused)
+        k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(p), static_cast<const double*>(tmp), n, pa, done);
       k_cg_update<<<kRB, kRT, 0, q>>>(kk, cs, x, r, p, tmp, n, pa, pb);
       k_cg_finish<<<kRB, kRT, 0, q>>>(kk, cs, r, p, n, pb);
     }
@@ -752,14 +759,19 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
     k_gm_scale<<<kRB, kRT, 0, q>>>(gs, static_cast<const double*>(V), V, n, -1);
     for (int j = 0; j < m; ++j) {
       double* vj = V + (int64_t)j * ld;
+      // w = A v_j (A P v_j) with the first modified Gram-Schmidt product V_0 . w formed in the
+      // operator's epilogue (gmres.hpp:157-165)
+      bool fused = false;
+      const DotEpilogue de{V, pa, kRB, &fused};
       if (s.prec) {
         double* z = static_cast<double*>(s.pz);
         DGOP_TRY(launch_f64(s.prec, 1.0, vj, 0.0, z, 0, q, inactive));
-        DGOP_TRY(launch_f64(s.op, 1.0, z, 0.0, w, s.op_flags, q, inactive));
+        DGOP_TRY(launch_f64(s.op, 1.0, z, 0.0, w, s.op_flags, q, inactive, s.fuse_dot ? &de : nullptr));
       } else {
-        DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, s.op_flags, q, inactive));
+        DGOP_TRY(launch_f64(s.op, 1.0, vj, 0.0, w, s.op_flags, q, inactive, s.fuse_dot ? &de : nullptr));
       }
-      k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(V), static_cast<const double*>(w), n, pa, inactive);
+      if (!fused)
+        k_dot<<<kRB, kRT, 0, q>>>(static_cast<const double*>(V), static_cast<const double*>(w), n, pa, inactive);
       double* pin = pa;
       double* pout = pb;
       for (int i = 0; i <= j; ++i) {
@@ -1081,6 +1093,16 @@ int dgop_element_dot(const dgop_operator* op, const double* a, const double* b, 
   k_element_dot<<<(unsigned)blocks, kRT, 0, (cudaStream_t)stream>>>(a, b, scale, out, nelem, nd);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "dgop_element_dot launch");
+  return DGOP_OK;
+}
+
+int dgop_solver_set_fused_dot(dgop_solver* sv, int enable) {
+  if (!sv) {
+    set_error("dgop_solver_set_fused_dot: null solver");
+    return DGOP_ERR_ARG;
+  }
+  sv->s.fuse_dot = enable != 0;
+  sv->s.key_version = -1;  // re-capture the segment graph
   return DGOP_OK;
 }
 

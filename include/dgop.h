@@ -126,9 +126,12 @@ const char* dgop_operator_kernel_note(const dgop_operator* op);
 int dgop_operator_select_kernel(dgop_operator* op, int kernel);
 /* Kronecker-kernel variants (no reference counterpart): 0 "stage2-tile" (next element group staged
  * while this one computes, layout exchanges through shared memory), 1 "stage1-tile" (one staging
- * buffer, more warps per SM), 2 "stage2-shfl" (exchanges by warp shuffles; even orders).  At
+ * buffer, more warps per SM), 2 "stage2-shfl" (exchanges by warp shuffles; even orders), and for
+ * p = 3 FP64 operators whose x extent is a multiple of 8, element groups moved by the Tensor
+ * Memory Accelerator: 3 "tma1-tile", 4 "tma2-shfl", 5 "tma2-tile".  At
  * creation the autotuner times every variant on scratch vectors (operators of at most 2^26 DoFs)
- * and keeps the fastest; all variants give bit-identical results.  dgop_operator_variant returns
+ * and keeps the fastest.  Variants 0-2 give bit-identical results, and so do variants 3-5; the two
+ * families differ in the last bits (3-5 accumulate each term's last pass onto the sum).  dgop_operator_variant returns
  * the FP64 variant in use (-1 without a Kronecker kernel); dgop_operator_set_variant forces one
  * (-1 re-runs the autotuner); dgop_operator_variant_time gives the autotuner's time per launch in
  * ms (0 when not timed). */
@@ -137,8 +140,13 @@ const char* dgop_operator_variant_name(const dgop_operator* op);
 int dgop_operator_set_variant(dgop_operator* op, int variant);
 int dgop_operator_variant_time(const dgop_operator* op, int variant, float* ms);
 /* The FP32 kernel configuration's variant and its autotuner times (ms[v]; -1: variant not usable;
- * ms holds 3 entries); variant -1 without a Kronecker kernel. */
+ * ms holds DGOP_MAX_VARIANTS entries); variant -1 without a Kronecker kernel. */
+#define DGOP_MAX_VARIANTS 6
 int dgop_operator_variant_f32(const dgop_operator* op, int* variant, float* ms);
+/* Reads and clears the operator's device error word: non-zero when a kernel gave up waiting for
+ * an asynchronous copy (its bounded waits ran out; the results of that launch are invalid).
+ * Synchronizes the device.  No reference counterpart. */
+int dgop_operator_device_error(const dgop_operator* op, int* error);
 
 /* y = alpha * A x + beta * y (beta == 0: y is not read).  FP64 device pointers, aligned to their
  * element size; the Kronecker-form kernel runs on 16-byte aligned vectors (any cudaMalloc'd or
@@ -231,6 +239,12 @@ int dgop_solver_set_graphs(dgop_solver* solver, int enable);
  * value 0; dgop_apply_transpose) with the same algorithm; used by adjoint solves.  No reference
  * counterpart. */
 int dgop_solver_set_transpose(dgop_solver* solver, int transpose);
+/* enable != 0 (the default): the first inner product of every iteration (CG: p . A p; GMRES:
+ * V_0 . w) is formed in the operator kernel's epilogue when the operator's kernel provides one
+ * (3D Kronecker form), saving a pass over two vectors; 0: a separate pass, as in the reference
+ * (conjugategradient.hpp:176-179, gmres.hpp:157-165).  The two sum the same products in different
+ * fixed orders, so iterates agree to rounding.  No reference counterpart. */
+int dgop_solver_set_fused_dot(dgop_solver* solver, int enable);
 /* Right preconditioning of a GMRES or refinement-GMRES solver: it solves A P z = b and returns
  * x = P z, so the stopping test and `relative_error` stay those of the unpreconditioned system
  * (|b - A x| / |b|).  P is an operator on the same space, typically dgop_mass_inverse_create's

@@ -269,3 +269,34 @@ def test_mass_preconditioned_gmres(cid, case, restart, plain_ok, inner):
         ref = g.GMRESSolver(A, restart).solve(b, x0, 5000, 1e-10)
         assert ref["success"] and ref["iterations"] > 2 * info["iterations"]
         assert rel_max(x.cpu().numpy(), x0.cpu().numpy()) < 1e-8
+
+
+@pytest.mark.parametrize("variant", ["stage1-tile", "tma1-tile", "tma2-shfl"])
+def test_fused_dot_matches_separate_pass(variant):
+    """The first inner product of each iteration formed in the operator kernel's epilogue (CG:
+    p . A p, GMRES: V_0 . w) sums the same products as the separate pass, in another fixed order:
+    the same iteration counts, iterates equal to rounding, and repeated solves bit-identical."""
+    case = {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [16, 4, 4], "h": [1 / 16, 0.25, 0.25],
+            "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "sigma_c": 1e3}
+    sp = make_space(case)
+    mass = g.MassOperator(sp, 4, C.sigma_preset(2, 3))
+    system = _system(case, sp)
+    for op in (mass, system):
+        assert op.kernel == "kron"
+        op.set_variant(variant)
+    b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 2)).cuda()
+
+    def solve(make, fused):
+        x = torch.zeros_like(b)
+        info = make().fused_dot(fused).solve(b, x, 5000, 1e-11)
+        return x, info
+
+    for make in (lambda: g.CGSolver(mass), lambda: g.GMRESSolver(system, 30)):
+        x1, i1 = solve(make, True)
+        x2, i2 = solve(make, True)
+        x0, i0 = solve(make, False)
+        assert i1["success"] and i0["success"]
+        assert torch.equal(x1, x2) and i1 == i2
+        assert abs(i1["iterations"] - i0["iterations"]) <= 1, (i1, i0)
+        assert rel_max(x1.cpu().numpy(), x0.cpu().numpy()) <= 1e-9
+    assert mass.device_error() == 0 and system.device_error() == 0

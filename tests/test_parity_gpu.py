@@ -166,33 +166,63 @@ VARIANT_CASES = [
                        "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 1, "sigma_kind": 2, "g": 0.0}, "adv", 2),
     ("mass_p1", {"D": 3, "P": 1, "Q": 2, "basis": 0, "sizes": [11, 3, 4], "h": [1 / 11, 1 / 3, 0.25],
                  "origin": [0.0] * 3, "periodic": [0, 1, 0], "sigma_kind": 1}, "mass", 1),
+    # p = 3 with the x extent a multiple of 8: the bulk-tensor (TMA) variants run too.  Inflow
+    # faces on both sides of every axis (the bubble velocity changes sign), periodic axes (wrapped
+    # neighbours come from global memory), a separate mass term, the mass operator alone, several
+    # x-rows per mesh
+    ("tma_adv_sincos", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [16, 3, 5], "h": [1 / 16, 1 / 3, 0.2],
+                        "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 2, "g": 0.5}, "adv", 1),
+    ("tma_adv_bubble_noBC", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [8, 6, 4], "h": [1 / 8, 1 / 6, 0.25],
+                             "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 1, "g": 0.0}, "adv", 0),
+    ("tma_adv_periodic", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [8, 4, 3], "h": [1 / 8, 0.25, 1 / 3],
+                          "origin": [-0.5, 0.0, 0.0], "periodic": [1, 1, 1], "beta_kind": 0,
+                          "beta_c": [-0.7, 0.4, -0.3], "g": 0.0}, "adv", 1),
+    ("tma_sys_sep", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [24, 2, 3], "h": [1 / 24, 0.5, 1 / 3],
+                     "origin": [0.0] * 3, "periodic": [0] * 3, "beta_kind": 1, "sigma_kind": 2, "g": 0.0}, "adv", 2),
+    ("tma_mass", {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [8, 5, 2], "h": [1 / 8, 0.2, 0.5],
+                  "origin": [0.0] * 3, "periodic": [0] * 3, "sigma_kind": 2}, "mass", 1),
 ]
+
+TMA_VARIANTS = ("tma1-tile", "tma2-shfl", "tma2-tile")
 
 
 @pytest.mark.parametrize("cid,case,kind,mode", VARIANT_CASES, ids=[c[0] for c in VARIANT_CASES])
 def test_kron_variants_are_bit_identical(cid, case, kind, mode):
-    """Every Kronecker-kernel variant the autotuner can pick computes the same bits (forward,
-    transposed and FP32 applies), and the forward apply meets the parity bar."""
+    """Every Kronecker-kernel variant the autotuner can pick computes the same bits as the others
+    of its family (forward, transposed and FP32 applies): the staged variants among themselves and
+    the bulk-tensor variants among themselves; the two families agree to a few ulps (the
+    bulk-tensor variants accumulate each term's last pass onto the sum), and every forward apply
+    meets the parity bar."""
     op = make_operator(case, kind, mode)
     if op.kernel != "kron":
         pytest.skip(op.kernel_note)
     assert op.variant in op.VARIANTS
     x = inputs(dict(case, seed=1))
-    ref = None
+    ref = {}
     for name in op.VARIANTS:
         try:
             op.set_variant(name)
         except RuntimeError:
-            assert name == "stage2-shfl" and case["P"] % 2 == 0  # shuffles need an even N = P + 1
+            # shuffles need an even N = P + 1; the bulk-tensor variants p = 3 and an x extent
+            # that is a multiple of 8
+            assert (name == "stage2-shfl" and case["P"] % 2 == 0) or \
+                (name in TMA_VARIANTS and (case["P"] != 3 or case["sizes"][0] % 8))
             continue
+        if name in TMA_VARIANTS:
+            assert case["P"] == 3 and case["sizes"][0] % 8 == 0
         got = (cuda_apply(op, x), cuda_apply(op, x, transpose=True), cuda_apply(op, x, f32=True))
-        if ref is None:
-            ref = got
-            want = oracle().mass_apply(case, x) if kind == "mass" else oracle().advection_apply(case, x, mode)
-            assert rel_max(got[0], want) <= APPLY_TOL
+        assert op.device_error() == 0, name
+        fam = name in TMA_VARIANTS
+        want = oracle().mass_apply(case, x) if kind == "mass" else oracle().advection_apply(case, x, mode)
+        assert rel_max(got[0], want) <= APPLY_TOL, name
+        if fam not in ref:
+            ref[fam] = got
         else:
-            for a, b in zip(got, ref):
+            for a, b in zip(got, ref[fam]):
                 assert np.array_equal(a, b), name
+    if len(ref) == 2:
+        for a, b in zip(ref[True][:2], ref[False][:2]):
+            assert rel_max(a, b) <= 1e-15
     op.set_variant(None)  # the autotuner again
     assert op.variant in op.VARIANTS
 
