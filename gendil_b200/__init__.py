@@ -26,7 +26,7 @@ from .coefficients import Coefficient, as_coefficient
 
 __all__ = ["Space", "MassOperator", "AdvectionOperator", "MassAdvectionOperator", "SystemOperator",
            "SIPDGOperator", "DiffusionOperator", "MassInverseOperator", "SpeedOfLightOperator", "CGSolver", "GMRESSolver", "GMRESIRSolver",
-           "Batch", "HostIO", "element_dot", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL",
+           "Batch", "BatchSolver", "HostIO", "element_dot", "Coefficient", "DGOPError", "lib", "fill_random", "GLL", "GL",
            "BC_NONE", "BC_INFLOW"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -114,6 +114,11 @@ def lib():
         L.dgop_batch_groups.argtypes = [vp]
         L.dgop_batch_apply.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
         L.dgop_batch_destroy.argtypes = [vp]
+        L.dgop_batch_solver_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), i, i, i, d, ctypes.POINTER(vp)]
+        L.dgop_batch_solver_waves.argtypes = [vp]
+        L.dgop_batch_solver_solve.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), i, d,
+                                              ctypes.POINTER(_SolveResult), ctypes.POINTER(d), vp]
+        L.dgop_batch_solver_destroy.argtypes = [vp]
         L.dgop_host_io_apply.argtypes = [vp, vp, vp, vp]
         L.dgop_host_io_destroy.argtypes = [vp]
         L.dgop_solver_solve.argtypes = [vp, vp, vp, i, d, ctypes.POINTER(_SolveResult), vp]
@@ -589,6 +594,59 @@ class Batch:
     def close(self):
         if self.handle:
             lib().dgop_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchSolver:
+    """Many independent systems A_i x_i = b_i solved together (dgop_batch_solver_*): restarted
+    GMRES(restart) with iterative refinement, inner cycles in `inner` precision ("fp32" or
+    "fp64"), FP64 residual and solution, right preconditioners `precs` (all or none), every
+    system's iterations in lockstep (one launch per vector operation over all systems, one apply
+    per system, restart cycles replayed from a CUDA graph), systems cut into waves whose workspace
+    fits `workspace_bytes` (0: half the free device memory).  No reference counterpart."""
+
+    def __init__(self, ops, precs=None, restart=20, inner="fp32", workspace_bytes=0):
+        self.ops = list(ops)
+        self.precs = list(precs) if precs is not None else None
+        if self.precs is not None and len(self.precs) != len(self.ops):
+            raise ValueError("BatchSolver: one preconditioner per operator")
+        n = len(self.ops)
+        oa = (ctypes.c_void_p * n)(*[o.handle for o in self.ops])
+        pa = None if self.precs is None else (ctypes.c_void_p * n)(*[p.handle for p in self.precs])
+        h = ctypes.c_void_p()
+        prec = {"fp32": 1, "fp64": 0}[inner]
+        check(lib().dgop_batch_solver_create(oa, pa, n, int(restart), prec, float(workspace_bytes), ctypes.byref(h)))
+        self.handle = h
+
+    @property
+    def waves(self):
+        return int(lib().dgop_batch_solver_waves(self.handle))
+
+    def solve(self, bs, xs, max_iters, tol, stream=None):
+        """Solve every system (x holds the initial guesses).  Returns (results, seconds): a
+        result dict per system as Solver.solve, and per system the time from the start of the call
+        until the end of the restart cycle after which it was found finished."""
+        bs, xs = list(bs), list(xs)
+        n = len(self.ops)
+        if not (len(bs) == len(xs) == n):
+            raise ValueError(f"BatchSolver.solve: {n} systems need as many right-hand sides and solutions")
+        ba = (ctypes.c_void_p * n)(*[_dvec(b, o.space.num_dofs, name=f"bs[{i}]") for i, (b, o) in enumerate(zip(bs, self.ops))])
+        xa = (ctypes.c_void_p * n)(*[_dvec(x, o.space.num_dofs, name=f"xs[{i}]") for i, (x, o) in enumerate(zip(xs, self.ops))])
+        res = (_SolveResult * n)()
+        sec = (ctypes.c_double * n)()
+        check(lib().dgop_batch_solver_solve(self.handle, ba, xa, int(max_iters), float(tol), res, sec, _stream(stream)))
+        return ([{"success": bool(r.success), "iterations": r.iterations, "relative_error": r.relative_error} for r in res],
+                list(sec))
+
+    def close(self):
+        if self.handle:
+            lib().dgop_batch_solver_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

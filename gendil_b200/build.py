@@ -31,7 +31,7 @@ BASE_FLAGS = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "--expt-relaxed-conste
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 # Non-instantiation sources; gen_generic.cu is compiled once per (dimension, N).
-SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "kron_plan.cpp", "gen_kron3d.cu", "krylov.cu", "host_io.cu", "batch.cu", "sipdg.cu"]
+SOURCES = ["dgop_api.cu", "registry.cu", "basis.cpp", "kron_plan.cpp", "gen_kron3d.cu", "krylov.cu", "host_io.cu", "batch.cu", "batch_solve.cu", "sipdg.cu"]
 
 
 def nvcc():

@@ -178,6 +178,7 @@ int dgop_batch_groups(const dgop_batch* batch);
 int dgop_batch_apply(dgop_batch* batch, const double* const* x, double* const* y, void* stream);
 int dgop_batch_destroy(dgop_batch* batch);
 
+
 /* Applies on HOST vectors (the reference's operator() on a host-resident Vector,
  * massoperator.hpp:209, advectionoperator.hpp:1070, where the data lives in host memory):
  * y_host = A x_host.  The host-to-device copy, the apply and the device-to-host copy are pipelined
@@ -278,6 +279,30 @@ int dgop_element_dot(const dgop_operator* op, const double* a, const double* b, 
 #define DGOP_STATIC_CG_MAX_DOFS 262144
 int dgop_cg_solve_static(dgop_operator* op, const double* b, double* x, int max_iters, double tol,
                          dgop_solve_result* result, void* stream);
+
+/* Many independent systems A_i x_i = b_i solved together (no reference counterpart; the
+ * reference solves one system per GMRES_no_alloc call, Solvers/gmres.hpp:74).  Restarted
+ * GMRES(restart) with iterative refinement: inner Krylov cycles with operator applies and basis in
+ * `inner_precision` (DGOP_FP32 or DGOP_FP64), the residual and the solution in FP64, right
+ * preconditioning by precs[i] (NULL array: none; otherwise every system has one), the stopping
+ * test and reported quantities of dgop_gmres_create's solver.  All systems advance in lockstep:
+ * each Krylov step is one apply per system plus one launch per vector operation over all of them,
+ * a restart cycle of all of them is replayed from one CUDA graph, and systems that finished stay
+ * idle.  The systems are cut, in the given order, into waves whose workspace fits
+ * `workspace_bytes` (<= 0: half the free device memory at creation); the workspace of the largest
+ * wave is allocated here.  The operators must outlive the solver. */
+typedef struct dgop_batch_solver dgop_batch_solver;
+int dgop_batch_solver_create(dgop_operator* const* ops, dgop_operator* const* precs, int count, int restart,
+                             int inner_precision, double workspace_bytes, dgop_batch_solver** out);
+/* Number of waves the systems were cut into. */
+int dgop_batch_solver_waves(const dgop_batch_solver* solver);
+/* Solve every system: b[i], x[i] device pointers (x[i] 16-byte aligned, the initial guess on
+ * entry); results[i] per system; seconds (NULL or count entries): per system, the time from the
+ * start of the call until the end of the restart cycle after which it was found finished.
+ * Synchronizes `stream`. */
+int dgop_batch_solver_solve(dgop_batch_solver* solver, const double* const* b, double* const* x, int max_iters,
+                            double tol, dgop_solve_result* results, double* seconds, void* stream);
+int dgop_batch_solver_destroy(dgop_batch_solver* solver);
 
 /* FillRandom (Algebra/vector.hpp:632): out[i] = std::uniform_real_distribution<double>(lo, hi)
  * draws from std::mt19937(seed), in order, into a HOST buffer of n values. */

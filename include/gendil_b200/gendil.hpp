@@ -1481,4 +1481,71 @@ class AdvectionSolveFunction {
   std::unique_ptr<Operator<D>> op_;
 };
 
+// Solve-based loss gradients for the interior-penalty DG diffusion operator with one
+// diffusivity per element, A(mu) u = f: the reference's SIPDG weak form with a per-element
+// coefficient field (tests/integration/gendil/test-sipdg-coefficient-field-inputs.cpp:547-569),
+// symmetric (sigma = -1), penalty kappa / h, Dirichlet-0 boundary terms when `boundary`.
+//   Forward(mu, f, u):  u = A(mu)^{-1} f by CG on the device.
+//   Backward(dJ/du, dJ/dmu, dJ/df):  lambda = A^{-1} dJ/du (A^T = A), then
+//     dJ/dmu_e = -lambda^T (dA/dmu_e) u   (dgop_sipdg_gradient: one kernel over all elements),
+//     dJ/df = lambda.
+// A is linear in mu and each element's diffusivity enters only its own rows and its faces' rows,
+// which the gradient kernel sums.  Forward keeps u and the operator; no Krylov iterate is stored.
+// No reference counterpart.
+template <Integer D>
+class DiffusionSolveFunction {
+ public:
+  DiffusionSolveFunction(const FiniteElementSpace<D>& fes, const IntegrationRule<D>& ir, Real kappa,
+                         bool boundary = true, Real tol = 1e-12, Integer max_iters = 100000)
+      : fes_(fes), q_(ir.q), kappa_(kappa), boundary_(boundary), tol_(tol), max_iters_(max_iters) {}
+
+  IterativeSolverResult Forward(const Vector& mu, const Vector& f, Vector& u) {
+    if (mu.Size() != fes_.GetNumberOfFiniteElements()) throw Error("DiffusionSolveFunction: one mu per element");
+    mu_ = mu;
+    release();
+    detail::check(dgop_sipdg_create(fes_.handle(), q_, mu_.ReadDeviceData(), -1.0, kappa_, boundary_ ? 1 : 0, &op_),
+                  "DiffusionSolveFunction operator");
+    detail::check(dgop_cg_create(op_, &cg_), "DiffusionSolveFunction CG");
+    u_ = Vector(f.Size());
+    u_ = 0.0;
+    const IterativeSolverResult r = detail::solve(cg_, f, u_, max_iters_, tol_);
+    u = u_;
+    return r;
+  }
+
+  IterativeSolverResult Backward(const Vector& grad_u, Vector& grad_mu, Vector& grad_f) {
+    if (!op_) throw Error("DiffusionSolveFunction: Backward before Forward");
+    grad_f = Vector(grad_u.Size());
+    grad_f = 0.0;
+    const IterativeSolverResult r = detail::solve(cg_, grad_u, grad_f, max_iters_, tol_);
+    grad_mu = Vector(fes_.GetNumberOfFiniteElements());
+    detail::check(dgop_sipdg_gradient(op_, u_.ReadDeviceData(), grad_f.ReadDeviceData(), nullptr,
+                                      grad_mu.WriteDeviceData(), nullptr),
+                  "coefficient gradient");
+    grad_mu *= -1.0;
+    return r;
+  }
+
+  ~DiffusionSolveFunction() { release(); }
+  DiffusionSolveFunction(const DiffusionSolveFunction&) = delete;
+  DiffusionSolveFunction& operator=(const DiffusionSolveFunction&) = delete;
+
+ private:
+  void release() {
+    if (cg_) dgop_solver_destroy(cg_);
+    if (op_) dgop_operator_destroy(op_);
+    cg_ = nullptr;
+    op_ = nullptr;
+  }
+  FiniteElementSpace<D> fes_;
+  int q_;
+  Real kappa_;
+  bool boundary_;
+  Real tol_;
+  Integer max_iters_;
+  Vector mu_, u_;
+  dgop_operator* op_ = nullptr;
+  dgop_solver* cg_ = nullptr;
+};
+
 }  // namespace gendil_b200

@@ -278,6 +278,37 @@ int run_mode(const char* path) {
     std::printf("check H_fd %.6g\n", worst / gmax);
     record("H_grad_theta", grad_theta);
   }
+  {  // K: adjoint gradient of J = |u - u*|^2 / 2 w.r.t. per-element diffusivities of the SIPDG
+     // operator (DiffusionSolveFunction), with central differences through the forward solve;
+     // J(mu+) - J(mu-) = (u+ - u-) . (u+ + u- - 2 u*) / 2 keeps the difference free of cancellation
+    CartesianMesh<3> mesh({3, 3, 2}, {1.0 / 3, 1.0 / 3, 0.5}, {0.0, 0.0, 0.0});
+    auto fes = MakeFiniteElementSpace(mesh, MakeLobattoFiniteElement(FiniteElementOrders<2, 2, 2>{}));
+    auto ir = MakeIntegrationRule(IntegrationRuleNumPoints<4, 4, 4>{});
+    DiffusionSolveFunction<3> fn(fes, ir, 90.0, true, 1e-13);
+    const Integer ne = fes.GetNumberOfFiniteElements();
+    Vector mu(ne), f(fes), target(fes), u(fes);
+    FillRandom(mu, 12, 0.5, 2.0);
+    FillRandom(f, 5);
+    FillRandom(target, 6);
+    report("K_forward", fn.Forward(mu, f, u));
+    Vector grad_u(fes), grad_mu, grad_f;
+    for (Integer i = 0; i < u.Size(); ++i) grad_u[i] = u[i] - target[i];
+    report("K_adjoint", fn.Backward(grad_u, grad_mu, grad_f));
+    const Real eps = 1e-6;
+    Real worst = 0.0;
+    for (Integer e = 0; e < ne; ++e) {
+      Vector mp = mu, mm = mu, up(fes), um(fes);
+      mp[e] += eps;
+      mm[e] -= eps;
+      fn.Forward(mp, f, up);
+      fn.Forward(mm, f, um);
+      Real dj = 0.0;
+      for (Integer i = 0; i < up.Size(); ++i) dj += 0.5 * (up[i] - um[i]) * (up[i] + um[i] - 2.0 * target[i]);
+      worst = std::max(worst, std::fabs(dj / (2 * eps) - grad_mu[e]) / std::fabs(grad_mu[e]));
+    }
+    std::printf("check K_fd_rel %.6g\n", worst);
+    record("K_grad_mu", grad_mu);
+  }
   {  // I: legacy interior-penalty diffusion, MakeDiffusionOperator(fes, ir, velocity, sigma, kappa):
      // periodic 3^3, p = 2, q = 4, diffusivity 2.5, sigma = -1, kappa = 90 (golden case d4)
     CartesianMesh<3> mesh({3, 3, 3}, {1.0 / 3, 1.0 / 3, 1.0 / 3}, {0.0, 0.0, 0.0}, true);

@@ -42,3 +42,69 @@ def test_batch_apply_equals_individual_applies():
         for y, w in zip(ys, want):
             assert torch.equal(y, w)
     batch.close()
+
+
+def _systems(specs, seed=7):
+    rng = np.random.default_rng(seed)
+    ops, precs, bs = [], [], []
+    for D, n, p in specs:
+        sp = _space(D, n, p)
+        beta = C.velocity_constant(list(rng.uniform(-1, 1, D)))
+        ops.append(g.SystemOperator(sp, p + 2, beta, sigma=1e3, bc=g.BC_INFLOW, g=0.0))
+        precs.append(g.MassInverseOperator(sp, p + 2, 1e3))
+        bs.append(torch.tensor(rng.uniform(-1, 1, sp.num_dofs), device="cuda"))
+    return ops, precs, bs
+
+
+SOLVE_SPECS = [(2, [40, 33], 3), (3, [12, 10, 9], 2), (4, [6, 5, 4, 5], 1), (3, [16, 8, 8], 3), (2, [25, 30], 5),
+               (4, [4, 4, 3, 3], 3), (3, [7, 9, 8], 4)]
+
+
+@pytest.mark.parametrize("inner", ["fp32", "fp64"])
+def test_batch_solver_matches_single_system_solves(inner):
+    """The lockstep batched refinement GMRES(20) reaches the same 1e-10 FP64 residual as the
+    single-system solver on every system, in the same number of iterations within one (their
+    inner products sum in different fixed orders), with solutions equal to rounding; the reported
+    residual is the true one."""
+    ops, precs, bs = _systems(SOLVE_SPECS)
+    batch = g.BatchSolver(ops, precs, restart=20, inner=inner)
+    xs = [torch.zeros_like(b) for b in bs]
+    res, secs = batch.solve(bs, xs, 2000, 1e-10)
+    for A, P, b, x, r, t in zip(ops, precs, bs, xs, res, secs):
+        assert r["success"] and r["relative_error"] <= 1e-10, r
+        ax = torch.empty_like(x)
+        A(x, ax)
+        true_rel = (torch.linalg.vector_norm(b - ax) / torch.linalg.vector_norm(b)).item()
+        assert abs(true_rel - r["relative_error"]) <= 1e-3 * r["relative_error"] + 1e-15
+        x1 = torch.zeros_like(b)
+        one = g.GMRESIRSolver(A, 20, inner=inner).precondition(P).solve(b, x1, 2000, 1e-10)
+        assert abs(one["iterations"] - r["iterations"]) <= 1, (one, r)
+        assert ((x - x1).abs().max() / x1.abs().max()).item() <= 1e-8
+        assert t > 0.0
+
+
+def test_batch_solver_waves_are_independent():
+    """Cutting the systems into several waves (a small workspace budget) changes nothing: every
+    system's computation depends on its own vectors and partial sums only (bit-identical)."""
+    ops, precs, bs = _systems(SOLVE_SPECS, seed=9)
+    one = g.BatchSolver(ops, precs, restart=20, inner="fp32")
+    many = g.BatchSolver(ops, precs, restart=20, inner="fp32", workspace_bytes=8e6)
+    assert one.waves == 1 and many.waves >= 3
+    xa = [torch.zeros_like(b) for b in bs]
+    xb = [torch.zeros_like(b) for b in bs]
+    ra, _ = one.solve(bs, xa, 2000, 1e-10)
+    rb, _ = many.solve(bs, xb, 2000, 1e-10)
+    assert ra == rb
+    for a, b in zip(xa, xb):
+        assert torch.equal(a, b)
+    # a second solve from the found solutions: the true residual is already below tol
+    rc, _ = one.solve(bs, xa, 2000, 1e-10)
+    assert all(r["success"] and r["iterations"] == 0 for r in rc)
+
+
+def test_batch_solver_reports_unconverged_systems():
+    ops, precs, bs = _systems(SOLVE_SPECS[:3], seed=11)
+    batch = g.BatchSolver(ops, precs, restart=5, inner="fp32")
+    xs = [torch.zeros_like(b) for b in bs]
+    res, _ = batch.solve(bs, xs, 3, 1e-14)
+    assert all(not r["success"] and r["iterations"] == 3 and r["relative_error"] > 1e-14 for r in res)

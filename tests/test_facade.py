@@ -139,6 +139,11 @@ def test_facade_operators_and_solvers_match_the_oracle(facade_bin, tmp_path):
     assert solves["H_forward"]["success"] and solves["H_adjoint"]["success"]
     assert checks["H_fd"] <= 1e-6
 
+    # diffusion coefficient gradient (DiffusionSolveFunction) against central differences, every
+    # element, relative to the element's own gradient
+    assert solves["K_forward"]["success"] and solves["K_adjoint"]["success"]
+    assert checks["K_fd_rel"] <= 1e-6
+
     # legacy diffusion operator (MakeDiffusionOperator) against the reference's own output
     assert rel_max(vec["I_diffusion"], arr["d4_y"]) <= APPLY_TOL
     assert checks["I_kernel_is_diffusion"] == 1 and checks["I_rejects_varying"] == 1
