@@ -508,8 +508,9 @@ def run_batch(args):
     """Configuration 5: independent implicit systems M/dt + A (dt = 1e-3, inflow 0), q = p + 2.
     (1) every operator applied once: one dgop_batch_apply (one persistent launch per (dimension,
     order) group) against one launch per instance; (2) every system solved to 1e-10 relative
-    residual with the element mass inverse as right preconditioner: FP32-inner refinement GMRES(20)
-    on `--streams` concurrent streams against FP64 GMRES(20) one instance after the other."""
+    residual with the element mass inverse as right preconditioner: all systems together by the
+    batched FP32-inner refinement GMRES(20) (dgop_batch_solver) against FP64 GMRES(20) one
+    instance after the other."""
     import threading
     import numpy as np
     import torch
@@ -550,6 +551,8 @@ def run_batch(args):
     batch.close()
 
     def solve_all(kind, streams):
+        """Every system solved by its own solver object, one after the other on `streams`
+        concurrent streams (the one-launch-each baseline)."""
         times = [0.0] * len(ops)
         iters = [0] * len(ops)
         ok = [False] * len(ops)
@@ -600,7 +603,39 @@ def run_batch(args):
                                "p99": float(np.percentile(ts, 99)), "max": float(ts.max())}}
 
     fp64 = solve_all("fp64", 1)
-    mixed = solve_all("mixed", args.streams)
+
+    # all systems together: lockstep refinement GMRES(20) with FP32 inner cycles (dgop_batch_solver)
+    t0 = time.time()
+    bsolver = g.BatchSolver(ops, precs, restart=20, inner="fp32")
+    bsolver_setup_s = time.time() - t0
+    xs = [torch.zeros_like(b) for b in bs]
+    torch.cuda.synchronize()
+    w0 = time.time()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    bres, bsecs = bsolver.solve(bs, xs, 2000, 1e-10)
+    e1.record()
+    torch.cuda.synchronize()
+    bwall = time.time() - w0
+    bdev = e0.elapsed_time(e1) * 1e-3
+    worst = 0.0
+    for A, b, x in zip(ops, bs, xs):
+        ax = torch.empty_like(x)
+        A(x, ax)
+        worst = max(worst, (torch.linalg.vector_norm(b - ax) / torch.linalg.vector_norm(b)).item())
+    ts = np.array(bsecs)
+    its = [r["iterations"] for r in bres]
+    batched = {"wall_s": bwall, "device_s": bdev, "solved_gdofs_per_s": total / bwall / 1e9,
+               "converged": int(sum(r["success"] for r in bres)), "max_true_relative_residual": worst,
+               "waves": bsolver.waves, "setup_s": bsolver_setup_s,
+               "iterations_median": float(np.median(its)), "iterations_max": int(max(its)),
+               "instance_completion_s": {"p50": float(np.percentile(ts, 50)), "p90": float(np.percentile(ts, 90)),
+                                         "p99": float(np.percentile(ts, 99)), "max": float(ts.max())},
+               "note": "every system advanced in lockstep: one launch per vector operation over all systems of a "
+                       "wave, one apply per system, restart cycles replayed from one CUDA graph; completion "
+                       "time = end of the restart cycle after which the system was found finished"}
+    bsolver.close()
+    del xs
     kinds = {}
     for o in ops:
         kinds[o.kernel] = kinds.get(o.kernel, 0) + 1
@@ -613,8 +648,8 @@ def run_batch(args):
             "apply": {"batched_ms": ms_batch, "one_launch_each_ms": ms_each,
                       "batched_gdofs_per_s": total / ms_batch / 1e6, "one_launch_each_gdofs_per_s": total / ms_each / 1e6},
             "solve": {"tol": 1e-10, "preconditioner": "element mass inverse (right)",
-                      "fp64_gmres20_sequential": fp64, f"mixed_ir_gmres20_{args.streams}_streams": mixed,
-                      "fp64_over_mixed_wall": fp64["wall_s"] / mixed["wall_s"]}}
+                      "fp64_gmres20_one_launch_each": fp64, "batched_mixed_ir_gmres20": batched,
+                      "fp64_over_batched_wall": fp64["wall_s"] / batched["wall_s"]}}
     print(json.dumps(line))
     return 0
 
@@ -788,7 +823,6 @@ def main():
                          "batch: 512 uneven implicit systems; sipdg: 32^3 p=4 diffusion apply, solve and gradient")
     ap.add_argument("--fd", type=int, default=64, help="sipdg workload: elements checked by central differences")
     ap.add_argument("--instances", type=int, default=512, help="batch workload: number of instances")
-    ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent solve streams")
     args = ap.parse_args()
     args.size_6d = args.size or 8
     args.size_sipdg = args.size or 32

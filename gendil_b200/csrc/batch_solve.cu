@@ -8,7 +8,9 @@
 // values that carry their system's index.  Inner products are reduced per chunk and then per
 // system in a fixed order (deterministic).  The scalar steps (Hessenberg column, Givens
 // rotations, stopping tests, back-substitution) are those of the single-system solver
-// (gmres_steps.cuh), one block per system.  A restart cycle of the whole wave is captured once as
+// (gmres_steps.cuh), one block per system.  The per-system applies of a step are independent
+// branches (16 streams forked and joined), so small systems share the GPU.  A restart cycle of
+// the whole wave is captured once as
 // a CUDA graph and replayed until every system of the wave has finished; the host reads the wave's
 // done flags once per cycle.  Systems that finish early stay idle (their launches return at once).
 //
@@ -281,6 +283,10 @@ struct dgop_batch_solver {
   int* h_done = nullptr;                // pinned
   cudaStream_t cap = nullptr;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
+  // the per-system applies of one step run as parallel branches of the graph: forked from the
+  // capture stream onto kBranches streams and joined back (most systems fill only a few CTAs)
+  cudaStream_t branch[16] = {};
+  cudaEvent_t fork = nullptr, join[16] = {};
 };
 
 namespace {
@@ -304,6 +310,11 @@ void release(dgop_batch_solver* s) {
   if (s->cap) cudaStreamDestroy(s->cap);
   if (s->t0) cudaEventDestroy(s->t0);
   if (s->t1) cudaEventDestroy(s->t1);
+  for (int k = 0; k < 16; ++k) {
+    if (s->branch[k]) cudaStreamDestroy(s->branch[k]);
+    if (s->join[k]) cudaEventDestroy(s->join[k]);
+  }
+  if (s->fork) cudaEventDestroy(s->fork);
 }
 
 template <typename T>
@@ -348,6 +359,26 @@ int setup(dgop_batch_solver* s, double budget_bytes) {
   DGOP_CUDA_BS(cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking));
   DGOP_CUDA_BS(cudaEventCreate(&s->t0));
   DGOP_CUDA_BS(cudaEventCreate(&s->t1));
+  DGOP_CUDA_BS(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+  for (int k = 0; k < 16; ++k) {
+    DGOP_CUDA_BS(cudaStreamCreateWithFlags(&s->branch[k], cudaStreamNonBlocking));
+    DGOP_CUDA_BS(cudaEventCreateWithFlags(&s->join[k], cudaEventDisableTiming));
+  }
+  return DGOP_OK;
+}
+
+// Run body(k, stream) for every system k of a wave, spread over the branch streams after a fork
+// from q and joined back into q (inside a capture these become parallel graph branches).
+template <typename F>
+int per_system(dgop_batch_solver* s, int count, cudaStream_t q, F&& body) {
+  const int nb = std::min(count, 16);
+  DGOP_CUDA_BS(cudaEventRecord(s->fork, q));
+  for (int k = 0; k < nb; ++k) DGOP_CUDA_BS(cudaStreamWaitEvent(s->branch[k], s->fork, 0));
+  for (int k = 0; k < count; ++k) DGOP_TRY_BS(body(k, s->branch[k % nb]));
+  for (int k = 0; k < nb; ++k) {
+    DGOP_CUDA_BS(cudaEventRecord(s->join[k], s->branch[k]));
+    DGOP_CUDA_BS(cudaStreamWaitEvent(q, s->join[k], 0));
+  }
   return DGOP_OK;
 }
 
@@ -403,8 +434,9 @@ int solve_wave(dgop_batch_solver* s, const std::vector<int>& wave, const double*
   const unsigned sysb = (unsigned)((count + kBT - 1) / kBT);
 
   auto residual = [&](int phase, cudaStream_t q) -> int {
-    for (int k = 0; k < count; ++k)
-      DGOP_TRY_BS(launch_f64(s->ops[wave[k]], 1.0, sys[k].x, 0.0, sys[k].w64, 0, q, &sys[k].st->done));
+    DGOP_TRY_BS(per_system(s, count, q, [&](int k, cudaStream_t b) {
+      return launch_f64(s->ops[wave[k]], 1.0, sys[k].x, 0.0, sys[k].w64, 0, b, &sys[k].st->done);
+    }));
     kb_sub_norm<T><<<nch, kBT, 0, q>>>(dsys, s->d_chunks, s->part, pw);
     kb_resid<T><<<count, kBT, 0, q>>>(dsys, s->part, pw, phase);
     DGOP_CUDA_BS(cudaGetLastError());
@@ -414,17 +446,16 @@ int solve_wave(dgop_batch_solver* s, const std::vector<int>& wave, const double*
     kb_cycle_start<T><<<sysb, kBT, 0, q>>>(dsys, count, m);
     kb_scale_v0<T><<<nch, kBT, 0, q>>>(dsys, s->d_chunks);
     for (int j = 0; j < m; ++j) {
-      for (int k = 0; k < count; ++k) {
+      DGOP_TRY_BS(per_system(s, count, q, [&](int k, cudaStream_t b) {
         const int i = wave[k];
         const int* skip = &sys[k].st->inactive;
         T* vj = sys[k].V + (int64_t)j * sys[k].ld;
         if (s->precs[i]) {
-          DGOP_TRY_BS(inner_apply(s->precs[i], vj, sys[k].z, q, skip));
-          DGOP_TRY_BS(inner_apply(s->ops[i], sys[k].z, sys[k].w, q, skip));
-        } else {
-          DGOP_TRY_BS(inner_apply(s->ops[i], vj, sys[k].w, q, skip));
+          DGOP_TRY_BS(inner_apply(s->precs[i], vj, sys[k].z, b, skip));
+          return inner_apply(s->ops[i], sys[k].z, sys[k].w, b, skip);
         }
-      }
+        return inner_apply(s->ops[i], vj, sys[k].w, b, skip);
+      }));
       kb_gs_dots<T><<<dim3(nch, (j + kDotsPerBlock) / kDotsPerBlock), kBT, 0, q>>>(dsys, s->d_chunks, j, s->part, pw);
       kb_gs_h<T><<<dim3(count, j + 1), kBT, 0, q>>>(dsys, j, m, s->part, pw);
       kb_gs_update<T><<<nch, kBT, 0, q>>>(dsys, s->d_chunks, j, m, s->part, pw);
@@ -436,8 +467,9 @@ int solve_wave(dgop_batch_solver* s, const std::vector<int>& wave, const double*
     if (s->precs[wave[0]]) {
       // x += P (sum y_i V_i) (every system has a preconditioner: dgop_batch_solver_create)
       kb_update<T><<<nch, kBT, 0, q>>>(dsys, s->d_chunks, 0);
-      for (int k = 0; k < count; ++k)
-        DGOP_TRY_BS(launch_f64(s->precs[wave[k]], 1.0, sys[k].pt, 1.0, sys[k].x, 0, q, &sys[k].st->done));
+      DGOP_TRY_BS(per_system(s, count, q, [&](int k, cudaStream_t b) {
+        return launch_f64(s->precs[wave[k]], 1.0, sys[k].pt, 1.0, sys[k].x, 0, b, &sys[k].st->done);
+      }));
     } else {
       kb_update<T><<<nch, kBT, 0, q>>>(dsys, s->d_chunks, 1);
     }

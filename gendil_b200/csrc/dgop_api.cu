@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <new>
 #include <random>
 #include <string>
@@ -551,6 +553,35 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
   return DGOP_OK;
 }
 
+// Autotuner decisions, shared by the operators of one kernel shape: (kernel family, dimension, N,
+// quadrature, precision, term structure, usable variants, element count within a factor 8).  The first operator of a shape is
+// timed; later ones take its variant (dgop_operator_set_variant(-1) times again and replaces it).
+struct TuneKey {
+  int family, D, N, Q, precision, structure, usable, size_class;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(family, D, N, Q, precision, structure, usable, size_class) <
+           std::tie(o.family, o.D, o.N, o.Q, o.precision, o.structure, o.usable, o.size_class);
+  }
+};
+struct TuneRecord {
+  int variant = 0, fallback = 1;
+  float ms[8] = {};
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneRecord> g_tune_cache;
+thread_local bool g_tune_force = false;  // set by dgop_operator_set_variant(-1)
+
+template <typename Real>
+TuneKey tune_key(const dgop_operator* op, int family, int usable, int has_adv, int has_mass, int merged) {
+  // element counts in classes of a factor 8 (launch shapes and tails change with the size)
+  int size_class = 0;
+  for (int64_t e = op->sp.nelem; e >= 8; e /= 8) ++size_class;
+  return TuneKey{family, op->sp.D, op->sp.n, op->q, (int)sizeof(Real),
+                 (op->flags & (kAdvCell | kFaceInt | kFaceBnd | kInvMass | kMass)) | (has_adv << 8) |
+                     (has_mass << 9) | (merged << 10),
+                 usable, size_class};
+}
+
 // Autotuner: times every usable kernel variant of the operator on scratch vectors (three
 // launches after one warm-up, CUDA events) and keeps the fastest.  Operators above
 // kTuneMaxDofs keep the default variant (the scratch vectors would cost more than they save).
@@ -558,9 +589,23 @@ constexpr int64_t kTuneMaxDofs = int64_t(1) << 26;
 
 template <typename Real>
 int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
-  int usable = 0;
-  for (const auto& L : K.launch) usable += L.ok ? 1 : 0;
+  int usable = 0, mask = 0;
+  for (int v = 0; v < kKronVariants; ++v) {
+    usable += K.launch[v].ok ? 1 : 0;
+    mask |= K.launch[v].ok ? 1 << v : 0;
+  }
   if (!K.ready || usable < 2 || op->sp.ndofs > kTuneMaxDofs) return DGOP_OK;
+  const TuneKey key = tune_key<Real>(op, 0, mask, K.params.has_adv, K.params.has_mass, K.params.mass_merged);
+  if (!g_tune_force) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      K.variant = it->second.variant;
+      K.fallback = it->second.fallback;
+      for (int v = 0; v < kKronVariants; ++v) K.launch[v].ms = it->second.ms[v];
+      return DGOP_OK;
+    }
+  }
   const int64_t n = op->sp.ndofs;
   Real* x = nullptr;
   Real* y = nullptr;
@@ -604,6 +649,12 @@ int autotune_kron(dgop_operator* op, KronCfg<Real>& K) {
     return DGOP_OK;  // keep the default variant
   }
   K.variant = best;
+  TuneRecord rec;
+  rec.variant = best;
+  rec.fallback = K.fallback;
+  for (int v = 0; v < kKronVariants; ++v) rec.ms[v] = K.launch[v].ms;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache[key] = rec;
   return DGOP_OK;
 }
 
@@ -888,9 +939,22 @@ void launch_kronnd_variant(const KronNDCfg<Real>& K, int v, KronNDParams<Real> p
 constexpr int64_t kTuneElems = 16384;
 template <typename Real>
 int autotune_kronnd(dgop_operator* op, KronNDCfg<Real>& K) {
-  int usable = 0;
-  for (const auto& L : K.var) usable += L.ok ? 1 : 0;
+  int usable = 0, mask = 0;
+  for (int v = 0; v < kKronNDVariants; ++v) {
+    usable += K.var[v].ok ? 1 : 0;
+    mask |= K.var[v].ok ? 1 << v : 0;
+  }
   if (!K.ready || usable < 2) return DGOP_OK;
+  const TuneKey key = tune_key<Real>(op, 1, mask, K.params.has_adv, K.params.has_mass, K.params.mass_merged);
+  if (!g_tune_force) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      K.variant = it->second.variant;
+      for (int v = 0; v < kKronNDVariants; ++v) K.var[v].ms = it->second.ms[v];
+      return DGOP_OK;
+    }
+  }
   const int64_t n = op->sp.ndofs;
   Real* x = nullptr;
   Real* y = nullptr;
@@ -933,6 +997,11 @@ int autotune_kronnd(dgop_operator* op, KronNDCfg<Real>& K) {
     return DGOP_OK;  // keep the default variant
   }
   K.variant = best;
+  TuneRecord rec;
+  rec.variant = best;
+  for (int v = 0; v < kKronNDVariants; ++v) rec.ms[v] = K.var[v].ms;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache[key] = rec;
   return DGOP_OK;
 }
 
@@ -1539,8 +1608,10 @@ int dgop_operator_set_variant(dgop_operator* op, int variant) {
       return DGOP_ERR_ARG;
     }
     if (variant == -1) {
+      g_tune_force = true;
       autotune_kronnd(op, op->n64);
       autotune_kronnd(op, op->n32);
+      g_tune_force = false;
     } else {
       if (!op->n64.var[variant].ok) {
         set_error(std::string("kernel variant ") + kKronNDVariantNames[variant] +
@@ -1562,8 +1633,10 @@ int dgop_operator_set_variant(dgop_operator* op, int variant) {
     return DGOP_ERR_UNSUPPORTED;
   }
   if (variant == -1) {
+    g_tune_force = true;
     autotune_kron(op, op->k64);
     autotune_kron(op, op->k32);
+    g_tune_force = false;
   } else {
     if (!op->k64.launch[variant].ok) {
       set_error(std::string("kernel variant ") + kKronVariantNames[variant] + " is not available for this operator");

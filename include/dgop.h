@@ -130,11 +130,13 @@ int dgop_operator_select_kernel(dgop_operator* op, int kernel);
  * p = 3 FP64 operators whose x extent is a multiple of 8, element groups moved by the Tensor
  * Memory Accelerator: 3 "tma1-tile", 4 "tma2-shfl", 5 "tma2-tile".  At
  * creation the autotuner times every variant on scratch vectors (operators of at most 2^26 DoFs)
- * and keeps the fastest.  Variants 0-2 give bit-identical results, and so do variants 3-5; the two
+ * and keeps the fastest; operators of the same kernel shape (dimension, order, quadrature,
+ * precision, terms, element count within a factor 8) reuse the first one's choice.  Variants 0-2
+ * give bit-identical results, and so do variants 3-5; the two
  * families differ in the last bits (3-5 accumulate each term's last pass onto the sum).  dgop_operator_variant returns
  * the FP64 variant in use (-1 without a Kronecker kernel); dgop_operator_set_variant forces one
- * (-1 re-runs the autotuner); dgop_operator_variant_time gives the autotuner's time per launch in
- * ms (0 when not timed). */
+ * (-1 times the variants of this operator again and makes its choice the shape's);
+ * dgop_operator_variant_time gives the autotuner's time per launch in ms (0 when not timed). */
 int dgop_operator_variant(const dgop_operator* op);
 const char* dgop_operator_variant_name(const dgop_operator* op);
 int dgop_operator_set_variant(dgop_operator* op, int variant);
