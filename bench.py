@@ -219,50 +219,67 @@ def run_reference(args):
 
 def mass_c1(g, torch, dev, steps, warmup, hbm):
     """Configuration 1's apply: FP64 mass, 16^3 hexahedra, p = 3 GLL, q = 4 GL, sigma = 1, input
-    FillRandom(seed 0).  Its 2 MB vectors fit in L2, so two figures: back-to-back applies
-    (L2-resident, the way a solver's iterations see it) and single applies each after a 256 MB
-    L2 flush (inputs cold in HBM: the HBM roofline applies to this one)."""
+    FillRandom(seed 0).  A launch of its 262,144 DoFs lasts a few microseconds, so the applies
+    are replayed from CUDA graphs (no host launch cost in the timing).  Its 2 MB vectors fit in
+    L2, so two figures: back-to-back applies (L2-resident, the way a solver's iterations see them)
+    and applies each after a 256 MB L2 flush (cold inputs: the HBM roofline applies to these),
+    timed as graph(flush; apply) x K minus graph(flush) x K."""
     space = g.Space(3, [16] * 3, order=3)
     op = g.MassOperator(space, 4, 1.0)
     nd = space.num_dofs
     x = torch.from_numpy(g.fill_random(nd, 0)).to(dev)
     y = torch.empty_like(x)
-    stream = torch.cuda.current_stream()
-    for _ in range(warmup):
-        op(x, y)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = max(steps, 100)
-    e0.record(stream)
-    for _ in range(reps):
-        op(x, y)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_warm = e0.elapsed_time(e1) / reps
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
-    cold = []
-    for _ in range(max(steps, 20)):
-        flush.fill_(1.0)  # evicts x and y from the 126 MB L2
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        op(x, y)
-        b.record(stream)
+    reps = max(steps, 50)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(warmup):
+            op(x, y)  # the operator's launches, and torch's, before capture
+            flush.fill_(1.0)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+
+    def capture(body):
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr):
+            for _ in range(reps):
+                body()
+        return gr
+
+    def timed(gr):
+        gr.replay()
         torch.cuda.synchronize()
-        cold.append(a.elapsed_time(b))
-    del flush
-    ms_cold = statistics.median(cold)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        gr.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    g_apply = capture(lambda: op(x, y))
+    g_flush = capture(lambda: flush.fill_(1.0))
+
+    def flush_apply():
+        flush.fill_(1.0)
+        op(x, y)
+
+    g_both = capture(flush_apply)
+    ms_warm = timed(g_apply) / reps
+    ms_cold = max(timed(g_both) - timed(g_flush), 0.0) / reps
+    del g_apply, g_flush, g_both, flush
     alg = 16.0 * nd
     out = {"workload": "fp64 mass apply, 3D 16^3 hex, p=3 GLL, q=4 GL, sigma=1 (FillRandom seed 0)", "dofs": nd,
            "kernel": op.kernel, "variant": op.variant,
            "l2_resident": {"ms_per_apply": ms_warm, "gdofs_per_s": nd / (ms_warm * 1e-3) / 1e9,
                            "gbs": alg / (ms_warm * 1e-3) / 1e9, "applies": reps,
-                           "note": "back-to-back applies; x and y (2 MB each) stay in L2, no HBM roofline"},
+                           "note": "back-to-back applies replayed from a CUDA graph; x and y (2 MB each) stay "
+                                   "in L2, no HBM roofline"},
            "after_l2_flush": {"ms_per_apply": ms_cold, "gdofs_per_s": nd / (ms_cold * 1e-3) / 1e9,
                               "roofline": {"bound": "hbm", "achieved": alg / (ms_cold * 1e-3) / 1e9, "peak": hbm,
                                            "unit": "GB/s", "frac": alg / (ms_cold * 1e-3) / 1e9 / hbm},
-                              "applies": len(cold),
-                              "note": "median of single applies, each after a 256 MB write that flushes L2; "
-                                      "a 4 MB launch is short enough that launch latency is part of it"}}
+                              "applies": reps,
+                              "note": "graph(256 MB flush; apply) x K minus graph(flush) x K, per apply"}}
     op.close()
     return out
 
@@ -454,6 +471,9 @@ def run_ours(args):
         if op.variant:
             line["kernel"]["variant"] = op.variant
             line["kernel"]["autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in op.variant_times().items() if v}
+            v32, ms32 = op.variant_f32()
+            line["kernel"]["fp32_variant"] = v32
+            line["kernel"]["fp32_autotuner_ms_per_launch"] = {k: round(v, 4) for k, v in ms32.items() if v > 0}
         if not six and world == 1:
             line["mass_c1"] = mass_c1(g, torch, dev, args.steps, args.warmup, hbm)
         if world == 1 and not args.no_solve:

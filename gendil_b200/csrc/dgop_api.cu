@@ -752,6 +752,31 @@ bool build_tc_tiles(const dgop_space& s, const KronPlanHost& plan, KronNDCfg<flo
 }
 
 // Any-dimension Kronecker kernel: matrix tables, face tables and launch shape.
+// The paired variant's condition (kronnd_paired_kernel): even D, every term pair (a, a + D/2)
+// with the same factor tables on the other D - 2 axes, and a separate mass term with the last
+// pair's factors outside that pair.  Compared value by value over every element coordinate.
+bool pairs_share_factors(const KronPlanHost& plan, const dgop_space& s) {
+  const int D = s.D, N = s.n;
+  if (D % 2 || D < 2) return false;
+  const int H = D / 2;
+  auto same = [&](const KronMat& x, const KronMat& y, int k) {
+    if (x.off < 0 || y.off < 0) return false;
+    const int64_t count = (x.stride || y.stride) ? s.sizes[k] : 1;
+    for (int64_t e = 0; e < count; ++e)
+      for (int q = 0; q < N * N; ++q)
+        if (plan.mats[x.off + e * x.stride + q] != plan.mats[y.off + e * y.stride + q]) return false;
+    return true;
+  };
+  if (plan.has_adv)
+    for (int a = 0; a < H; ++a)
+      for (int k = 0; k < D; ++k)
+        if (k != a && k != a + H && !same(plan.T[a][k], plan.T[a + H][k], k)) return false;
+  if (plan.has_adv && plan.has_mass && !plan.mass_merged)
+    for (int k = 0; k < D; ++k)
+      if (k != H - 1 && k != D - 1 && !same(plan.MT[k], plan.T[H - 1][k], k)) return false;
+  return true;
+}
+
 template <typename Real>
 int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan, const double* elem_sigma,
                  const double* const* elem_beta) {
@@ -865,9 +890,10 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
   K.var[0] = {true, eb, K.grid, K.smem, 0.0f};
   // grouped variants: elements per CTA so that the blocks of the largest group give every
   // thread about one block, within ~110 KB of shared memory (two CTAs per SM)
+  const bool paired = pairs_share_factors(plan, s);
   for (int v = 1; v < kKronNDVariants; ++v) {
-    const int G = v + 1;
-    if (!entry->launch_g[v - 1]) continue;
+    const int G = v == 3 ? 2 : v + 1;  // the paired variant's blocks span two axes
+    if (!entry->launch_g[v - 1] || (v == 3 && !paired)) continue;
     int64_t gsz = 1;
     for (int k = 0; k < std::min(G, D); ++k) gsz *= N;
     const int64_t ipe = (s.ndofs / s.nelem) / gsz;  // blocks per element

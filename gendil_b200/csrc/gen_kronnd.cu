@@ -38,6 +38,11 @@ void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, 
 }
 
 template <int D, int N, typename Real>
+void launch_kronnd_paired(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_paired_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
+}
+
+template <int D, int N, typename Real>
 void launch_kronnd_diff(const KronDiffParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   kronnd_diff_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
 }
@@ -69,6 +74,10 @@ void fill(KronNDEntry<Real>& d) {
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);
       }
+    }
+    if constexpr (D % 2 == 0 && N >= 2 && N * N <= 27) {
+      d.launch_g[2] = &launch_kronnd_paired<D, N, Real>;
+      d.func_g[2] = reinterpret_cast<const void*>(&kronnd_paired_kernel<D, N, Real>);
     }
     if constexpr (sizeof(Real) == 4 && KronTCShape<D, N>::OK && KronTCShape<D, N>::WARP_BYTES * 4 <= 200 * 1024) {
       d.launch_tc = &launch_kronnd_tc<D, N>;

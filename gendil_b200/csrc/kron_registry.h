@@ -49,8 +49,9 @@ void register_kron3d();
 
 // Kronecker form, any dimension, shared-memory kernel (kronnd_kernel.cuh).  Variants (the
 // autotuner picks one per operator): 0 one shared-memory pass per axis; 1, 2 groups of 2 or 3
-// axes per pass in registers.
-constexpr int kKronNDVariants = 3;
+// axes per pass in registers; 3 axes a and a + D/2 paired, the two terms of a pair run together
+// (even D, operators whose term pairs share their other factors).
+constexpr int kKronNDVariants = 4;
 extern const char* const kKronNDVariantNames[kKronNDVariants];
 
 template <typename Real>
@@ -62,9 +63,10 @@ struct KronNDEntry {
                                         dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
   const void* func_batch[kKronNDVariants] = {};
   int per_elem = 0;  // Real values of shared memory per element
-  // grouped variants (kronnd_grouped_kernel), groups of 2 and 3 axes: same parameters and layout
-  void (*launch_g[2])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
-  const void* func_g[2] = {};
+  // grouped variants (kronnd_grouped_kernel), groups of 2 and 3 axes, and the paired variant
+  // (kronnd_paired_kernel): same parameters and layout
+  void (*launch_g[3])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
+  const void* func_g[3] = {};
   // BF16 tensor-core variant (kronnd_tc_kernel.cuh; FP32 parameters, even D, N^(D/2) <= 32)
   void (*launch_tc)(const KronNDParams<float>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_tc = nullptr;

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "dgop_params.h"
 #include "generic_kernel.cuh"
@@ -464,6 +465,217 @@ __global__ void __launch_bounds__(kKronNDThreads)
   for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
     kronnd_grouped_block<D, N, G>(P, P.x, P.y, e0, ne, base, ecoord);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Paired variant (even D, H = D / 2): axis a is grouped with axis a + H, and the two terms whose
+// own axes form a pair run together.  Valid when their factors on the other D - 2 axes are the
+// same matrices (the planner checks the tables: phase-space advection beta = (v, -x + 0.5) has
+// terms a and a + H weighted only along the pair) and, for a separate mass term, when its factors
+// outside the last pair equal that pair's terms' (it then runs with them).  Term pair g makes one
+// shared-memory round trip per pair: the own step on the (g, g + H) blocks sums
+//   (D_g (+ faces) then T_{g, g+H})  +  (D_{g+H} (+ faces) then T_{g+H, g})  [+ MD then MT_g]
+// in registers, and the other pairs' steps apply the shared factors, the last accumulating into
+// Y: D / 2 round trips per pair instead of D / G per term.  Results agree with the other variants
+// to rounding (the terms are summed before, not after, their common factors).
+// ------------------------------------------------------------------------------------------
+template <int D, int N, int PG, int ST, typename Real>
+__device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const Real* __restrict__ xin, Real* base,
+                                             int ne, int64_t e0, const int (*ecoord)[kMaxDim]) {
+  using S = KronNDShape<D, N>;
+  constexpr int H = D / 2;
+  constexpr int g = ST == 0 ? PG : (ST - 1 < PG ? ST - 1 : ST);  // the pair this step runs on
+  constexpr int A = g, B = g + H;
+  constexpr int SA = kpow(N, A), SB = kpow(N, B);
+  constexpr int IPE = S::ND / (N * N);  // blocks per element
+  constexpr bool OWN = ST == 0, LAST = ST == H - 1;
+  constexpr bool WITH_MASS = PG == H - 1;  // the separate mass term runs with the last pair
+  const bool mass = WITH_MASS && P.has_mass && !(P.has_adv && P.mass_merged);
+  const int total = ne * IPE;
+  for (int it = threadIdx.x; it < total; it += blockDim.x) {
+    const int b = it / IPE;
+    int r = it - b * IPE;
+    // offset of the block: the other axes' indices, in increasing axis order
+    int off = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      if (k == A || k == B) continue;
+      const int q = r / N;
+      off += (r - q * N) * kpow(N, k);
+      r = q;
+    }
+    Real* el = base + (size_t)b * S::PER_ELEM;
+    const Real* mats = el + 3 * S::ND;
+    const Real* src = OWN ? el : el + S::ND;
+    Real v[N][N];  // v[i][j]: index i along A, j along B
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) v[i][j] = src[off + i * SA + j * SB];
+    Real acc[N][N];
+    if constexpr (OWN) {
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) acc[i][j] = Real(0);
+      const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+      const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
+      // own term of axis X (X == A: along the first index) then its factor along the other
+      auto own_term = [&](auto xc) {
+        constexpr int X = decltype(xc)::value;
+        constexpr bool FIRST = X == A;
+        constexpr int Y = FIRST ? B : A;
+        const PassMat<N, Real> dm(mats + (X * D + X) * S::MAT);
+        const PassMat<N, Real> tm(mats + (X * D + Y) * S::MAT);
+        const Real scale = P.elem[X] ? P.elem[X][e0 + b] : Real(1);
+        Real w[N][N];
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int j = 0; j < N; ++j) {
+            Real s = Real(0);
+#pragma unroll
+            for (int k = 0; k < N; ++k) s += FIRST ? dm(i, k) * v[k][j] : dm(j, k) * v[i][k];
+            w[i][j] = P.elem[X] ? s * scale : s;
+          }
+        if (P.has_adv) {
+#pragma unroll
+          for (int sd = 0; sd < 2; ++sd) {
+            const int fi = X * 2 + sd;
+            const uint32_t f = fb[fi];
+            if (!f) continue;
+            const int sl = sd ? N - 1 : 0;
+            int64_t en = 0;
+            if (f & 2u) {
+              const int64_t n = P.sizes[X];
+              const int64_t ca = ecoord[b][X];
+              const int64_t cn = sd ? (ca + 1 == n ? 0 : ca + 1) : (ca == 0 ? n - 1 : ca - 1);
+              en = e0 + b + (cn - ca) * P.estride[X];
+            }
+#pragma unroll
+            for (int t = 0; t < N; ++t) {
+              Real add = Real(0);
+              const Real own = FIRST ? v[sl][t] : v[t][sl];
+              if (f & 1u) add += rec[2 * fi] * own;
+              if (f & 2u) {
+                const int nidx = FIRST ? off + (N - 1 - sl) * SA + t * SB : off + t * SA + (N - 1 - sl) * SB;
+                add += rec[2 * fi + 1] * xin[en * S::ND + nidx];
+              } else if (f & 4u) {
+                add += rec[2 * fi + 1] * P.g;
+              }
+              if (FIRST) w[sl][t] += add;
+              else w[t][sl] += add;
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int j = 0; j < N; ++j) {
+            Real s = Real(0);
+#pragma unroll
+            for (int k = 0; k < N; ++k) s += FIRST ? tm(j, k) * w[i][k] : tm(i, k) * w[k][j];
+            acc[i][j] += s;
+          }
+      };
+      if (P.has_adv) {
+        own_term(std::integral_constant<int, A>{});
+        own_term(std::integral_constant<int, B>{});
+      }
+      if (mass) {
+        // MD along the last axis (B of the last pair, scaled), then MT along A
+        const PassMat<N, Real> md(mats + (D * D + B) * S::MAT);
+        const PassMat<N, Real> mt(mats + (D * D + A) * S::MAT);
+        const Real scale = P.elem_mass ? P.elem_mass[e0 + b] : Real(1);
+        Real w[N][N];
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int j = 0; j < N; ++j) {
+            Real s = Real(0);
+#pragma unroll
+            for (int k = 0; k < N; ++k) s += md(j, k) * v[i][k];
+            w[i][j] = P.elem_mass ? s * scale : s;
+          }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+          for (int j = 0; j < N; ++j) {
+            Real s = Real(0);
+#pragma unroll
+            for (int k = 0; k < N; ++k) s += mt(i, k) * w[k][j];
+            acc[i][j] += s;
+          }
+      }
+    } else {
+      // the pair's shared factors along A and B (term PG's; equal to term PG + H's)
+      const int t0 = P.has_adv ? PG : D;  // the mass term alone: its own factors
+      const PassMat<N, Real> fa(mats + (t0 < D ? t0 * D + A : D * D + A) * S::MAT);
+      const PassMat<N, Real> fbm(mats + (t0 < D ? t0 * D + B : D * D + B) * S::MAT);
+      Real w[N][N];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          Real s = Real(0);
+#pragma unroll
+          for (int k = 0; k < N; ++k) s += fa(i, k) * v[k][j];
+          w[i][j] = s;
+        }
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          Real s = Real(0);
+#pragma unroll
+          for (int k = 0; k < N; ++k) s += fbm(j, k) * w[i][k];
+          acc[i][j] = s;
+        }
+    }
+    Real* dst = el + (LAST ? 2 : 1) * S::ND;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        if constexpr (LAST) dst[off + i * SA + j * SB] += acc[i][j];
+        else dst[off + i * SA + j * SB] = acc[i][j];
+      }
+  }
+}
+
+// One batch of ne elements starting at e0 with the paired steps.
+template <int D, int N, typename Real>
+__device__ __forceinline__ void kronnd_paired_block(const KronNDParams<Real>& P, const Real* __restrict__ xin,
+                                                    Real* __restrict__ yout, int64_t e0, int ne, Real* base,
+                                                    int (*ecoord)[kMaxDim]) {
+  constexpr int H = D / 2;
+  nd_setup<D, N>(P, xin, e0, ne, base, ecoord);
+  static_for<0, H>([&](auto pc) {
+    constexpr int PG = decltype(pc)::value;
+    // a pair runs when it has advection terms, or the mass term alone (operators without
+    // advection: the last pair carries it)
+    if (P.has_adv || (PG == H - 1 && P.has_mass)) {
+      static_for<0, H>([&](auto sc) {
+        nd_pair_step<D, N, PG, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+        __syncthreads();
+      });
+    }
+  });
+  nd_output<D, N>(P, yout, e0, ne, base);
+}
+
+template <int D, int N, typename Real>
+__global__ void __launch_bounds__(kKronNDThreads, 3)
+    kronnd_paired_kernel(const __grid_constant__ KronNDParams<Real> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* base = reinterpret_cast<Real*>(smem_raw);
+  __shared__ int ecoord[64][kMaxDim];
+  if (P.skip && *P.skip) return;
+  const int EB = P.eb;
+  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    kronnd_paired_block<D, N>(P, P.x, P.y, e0, ne, base, ecoord);
   }
 }
 

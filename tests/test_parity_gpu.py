@@ -268,8 +268,9 @@ ND_VARIANT_CASES = [(f"{c['id']}_mode{m}", c, "adv", m) for c in CASES["advectio
 @pytest.mark.parametrize("cid,case,kind,mode", ND_VARIANT_CASES, ids=[c[0] for c in ND_VARIANT_CASES])
 def test_kronnd_variants(cid, case, kind, mode):
     """Every variant of the any-dimension kernel (one pass per axis; groups of 2 or 3 axes per
-    register block) meets the parity bar against the reference's golden outputs, forward,
-    transposed and FP32, and agrees with the per-axis variant to rounding."""
+    register block; axes a and a + D/2 paired where the terms share their other factors) meets the
+    parity bar against the reference's golden outputs, forward, transposed and FP32, and agrees
+    with the per-axis variant to rounding."""
     import gendil_b200 as g
     op = make_operator(case, kind, mode)
     try:
