@@ -78,6 +78,10 @@ void fill(KronNDEntry<Real>& d) {
     if constexpr (D % 2 == 0 && N >= 2 && N * N <= 27) {
       d.launch_g[2] = &launch_kronnd_paired<D, N, Real>;
       d.func_g[2] = reinterpret_cast<const void*>(&kronnd_paired_kernel<D, N, Real>);
+      if constexpr (sizeof(Real) == 8) {
+        d.launch_batch[3] = &launch_kronnd_batch<D, N, 3, Real>;
+        d.func_batch[3] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 3, Real>);
+      }
     }
     if constexpr (sizeof(Real) == 4 && KronTCShape<D, N>::OK && KronTCShape<D, N>::WARP_BYTES * 4 <= 200 * 1024) {
       d.launch_tc = &launch_kronnd_tc<D, N>;

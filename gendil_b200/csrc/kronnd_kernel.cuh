@@ -680,7 +680,7 @@ __global__ void __launch_bounds__(kKronNDThreads, 3)
 }
 
 // Many operators of one (D, N) and kernel variant V (0: one pass per axis, 1 / 2: groups of 2 / 3
-// axes) in one persistent launch: table[i] holds instance i's parameters (forward operator, x / y
+// axes, 3: paired axes) in one persistent launch: table[i] holds instance i's parameters (forward operator, x / y
 // set per apply), its element batches are the global batch indices [first[i], first[i + 1]);
 // every CTA walks the global batches.
 template <int D, int N, int V, typename Real>
@@ -703,6 +703,7 @@ __global__ void __launch_bounds__(kKronNDThreads)
     const int64_t e0 = (gb - first[lo]) * EB;
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
     if constexpr (V == 0) kronnd_block<D, N>(P, P.x, P.y, e0, ne, EB, base, escale, ecoord);
+    else if constexpr (V == 3) kronnd_paired_block<D, N>(P, P.x, P.y, e0, ne, base, ecoord);
     else kronnd_grouped_block<D, N, V + 1>(P, P.x, P.y, e0, ne, base, ecoord);
   }
 }
