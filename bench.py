@@ -39,7 +39,8 @@ FALLBACK_HBM_GBS = 6650.0
 HOST_SLABS = 4  # slabs of z planes per host-vector apply (consecutive steps overlap, so few slabs suffice)
 # DRAM bytes (read + write) of one launch measured by ncu (one-pass capture of the full workload),
 # by (workload, kernel variant, elements per axis)
-TRAFFIC_BYTES = {("3d", "stage1-tile", 64): 221.3e6, ("6d", "nd-grouped2", 8): 4.25e9}
+TRAFFIC_BYTES = {("3d", "stage1-tile", 64): 221.3e6, ("3d", "tma1-tile", 64): 223.3e6,
+                 ("6d", "nd-grouped2", 8): 4.25e9}
 
 
 def workload_config(world, n=N_AXIS):
