@@ -514,8 +514,11 @@ class _Solver:
         return self
 
     def use_graphs(self, enable=True):
-        """Replay solver segments from CUDA graphs (default) or launch every kernel directly."""
-        check(lib().dgop_solver_set_graphs(self.handle, 1 if enable else 0))
+        """Replay solver segments from CUDA graphs (True, the default), run the whole solve as one
+        graph launch with a conditional WHILE node ("whole"), or launch every kernel directly
+        (False).  All three give the same results bit for bit."""
+        mode = 2 if enable == "whole" else (1 if enable else 0)
+        check(lib().dgop_solver_set_graphs(self.handle, mode))
         return self
 
     def close(self):

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
 #include <new>
 #include <string>
 #include <mutex>
@@ -428,6 +429,29 @@ __global__ void __launch_bounds__(kRT) k_element_dot(const double* __restrict__ 
 
 }  // namespace
 
+// Whole-solve loop control: loop[0] counts the segments run in this launch, loop[1] is the
+// limit.  k_loop_next runs after every segment and keeps the WHILE node going while the solve
+// is not done and fewer than loop[1] segments have run, so the loop ends after at most loop[1]
+// segments whatever the solver state holds.
+__global__ void k_loop_reset(int* loop, int limit) {
+  loop[0] = 0;
+  loop[1] = limit;
+}
+__global__ void k_loop_next(cudaGraphConditionalHandle h, const int* done, int* loop) {
+  const int c = ++loop[0];
+  cudaGraphSetConditional(h, (*done == 0 && c < loop[1]) ? 1u : 0u);
+}
+
+// What a captured solver graph depends on besides device state: b, x, the operator's kernel
+// selection and flags, and the preconditioner's.
+struct GraphKey {
+  const void* b = nullptr;
+  const void* x = nullptr;
+  int version = -1, flags = -1;
+  const dgop_operator* prec = nullptr;
+  int prec_version = -1;
+};
+
 struct SolverImpl {
   int kind = 0;  // 0: CG, 1: GMRES, 2: GMRES with FP32 inner cycles and FP64 refinement
   int restart = 0;
@@ -442,21 +466,22 @@ struct SolverImpl {
   double* wide = nullptr;      // refinement solver: (restart + 1) x kRB projection partials
   // Segments (a CG chunk, a GMRES cycle) are replayed from one CUDA graph, captured for the
   // current (b, x, operator version) and re-captured when any of them changes (tolerance and
-  // iteration limit are device state).
+  // iteration limit are device state).  With `whole`, the solve is ONE graph launch: a
+  // conditional WHILE node replays the segment until the solve is done or the segment limit is
+  // reached, with no host round trip between segments.
   bool use_graphs = true;
+  bool whole = false;
   cudaStream_t cap = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  const void* key_b = nullptr;
-  const void* key_x = nullptr;
-  int key_version = -1, key_flags = -1;
-  int op_flags = 0;  // extra operator flags of every apply (kTranspose: solve with A^T)
+  cudaGraphExec_t exec = nullptr;   // one segment
+  cudaGraphExec_t wexec = nullptr;  // the whole solve
+  GraphKey key, wkey;
+  int* loop = nullptr;  // device: segments run, segment limit (whole-solve graphs)
+  int op_flags = 0;     // extra operator flags of every apply (kTranspose: solve with A^T)
   // right preconditioner (GMRES): A P z = b, x = P z; scratch vectors z (inner precision, stride
   // ir_stride(n) for the refinement solver) and t (FP64)
   dgop_operator* prec = nullptr;
   void* pz = nullptr;
   double* pt = nullptr;
-  const dgop_operator* key_prec = nullptr;
-  int key_prec_version = -1;
   // done-flag reads run one segment behind the enqueued work (no events: read synchronously)
   cudaEvent_t ev[2] = {nullptr, nullptr};
   // the operator kernel forms the first inner product of an iteration (CG: p . Ap; GMRES:
@@ -510,10 +535,20 @@ void solver_free(dgop_solver* sv) {
   if (s.pz) cudaFree(s.pz);
   if (s.pt) cudaFree(s.pt);
   if (s.exec) cudaGraphExecDestroy(s.exec);
+  if (s.wexec) cudaGraphExecDestroy(s.wexec);
+  if (s.loop) cudaFree(s.loop);
   if (s.cap) cudaStreamDestroy(s.cap);
   for (auto e : s.ev)
     if (e) cudaEventDestroy(e);
   s = SolverImpl{};
+}
+
+bool key_matches(const GraphKey& k, const SolverImpl& s, const void* b, const void* x) {
+  return k.b == b && k.x == x && k.version == s.op->version && k.flags == s.op_flags && k.prec == s.prec &&
+         (!s.prec || k.prec_version == s.prec->version);
+}
+GraphKey key_of(const SolverImpl& s, const void* b, const void* x) {
+  return GraphKey{b, x, s.op->version, s.op_flags, s.prec, s.prec ? s.prec->version : -1};
 }
 
 // Enqueues one segment on `st`: replays the cached graph, capturing it first when the key
@@ -521,10 +556,7 @@ void solver_free(dgop_solver* sv) {
 template <typename F>
 int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&& enqueue) {
   if (!s.use_graphs) return enqueue(st);
-  const bool same =
-      s.exec && s.key_b == b && s.key_x == x && s.key_version == s.op->version && s.key_flags == s.op_flags &&
-      s.key_prec == s.prec && (!s.prec || s.key_prec_version == s.prec->version);
-  if (!same) {
+  if (!(s.exec && key_matches(s.key, s, b, x))) {
     if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
     DGOP_CUDA_S(cudaStreamBeginCapture(s.cap, cudaStreamCaptureModeThreadLocal));
     const int rc = enqueue(s.cap);
@@ -536,21 +568,66 @@ int run_segment(SolverImpl& s, cudaStream_t st, const void* b, const void* x, F&
     }
     if (s.exec) cudaGraphExecDestroy(s.exec);
     s.exec = nullptr;
-    s.key_version = -1;
+    s.key = GraphKey{};
     const cudaError_t e2 = cudaGraphInstantiateWithFlags(&s.exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) {
       s.exec = nullptr;
       return cuda_fail(e2, "solver graph instantiation");
     }
-    s.key_b = b;
-    s.key_x = x;
-    s.key_version = s.op->version;
-    s.key_flags = s.op_flags;
-    s.key_prec = s.prec;
-    s.key_prec_version = s.prec ? s.prec->version : -1;
+    s.key = key_of(s, b, x);
   }
   DGOP_CUDA_S(cudaGraphLaunch(s.exec, st));
+  return DGOP_OK;
+}
+
+// Enqueues the rest of the solve on `st` as ONE graph launch: a conditional WHILE node whose
+// body is one segment followed by k_loop_next (captured into the node's body graph), run at
+// most `limit` times.  The graph is built for the current key and rebuilt when it changes; the
+// limit is set by a kernel before each launch, so it needs no rebuild.  Same kernels in the same
+// order as the segment-by-segment loop, hence the same results bit for bit.
+template <typename F>
+int run_whole(SolverImpl& s, cudaStream_t st, const void* b, const void* x, const int* done, int limit,
+              F&& enqueue) {
+  if (!s.loop) DGOP_CUDA_S(cudaMalloc(&s.loop, 2 * sizeof(int)));
+  if (!(s.wexec && key_matches(s.wkey, s, b, x))) {
+    if (!s.cap) DGOP_CUDA_S(cudaStreamCreateWithFlags(&s.cap, cudaStreamNonBlocking));
+    if (s.wexec) cudaGraphExecDestroy(s.wexec);
+    s.wexec = nullptr;
+    s.wkey = GraphKey{};
+    cudaGraph_t graph = nullptr;
+    DGOP_CUDA_S(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h{};
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node = nullptr;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+    }
+    int rc = DGOP_OK;
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s.cap, cp.conditional.phGraph_out[0], nullptr, nullptr,
+                                                            0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = enqueue(s.cap);
+      k_loop_next<<<1, 1, 0, s.cap>>>(h, done, s.loop);
+      cudaGraph_t body = nullptr;
+      e = cudaStreamEndCapture(s.cap, &body);
+    }
+    if (rc == DGOP_OK && e == cudaSuccess) e = cudaGraphInstantiateWithFlags(&s.wexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (rc != DGOP_OK || e != cudaSuccess) {
+      s.wexec = nullptr;
+      return rc != DGOP_OK ? rc : cuda_fail(e, "whole-solve graph");
+    }
+    s.wkey = key_of(s, b, x);
+  }
+  k_loop_reset<<<1, 1, 0, st>>>(s.loop, limit);
+  DGOP_CUDA_S(cudaGetLastError());
+  DGOP_CUDA_S(cudaGraphLaunch(s.wexec, st));
   return DGOP_OK;
 }
 
@@ -617,11 +694,16 @@ int cg_solve(SolverImpl& s, const double* b, double* x, int max_iters, double to
     DGOP_CUDA_S(cudaGetLastError());
     return DGOP_OK;
   };
-  for (int c = 0; (int64_t)c * kCheckEvery < max_iters; ++c) {
-    DGOP_TRY(run_segment(s, st, b, x, chunk));
-    bool stop = false;
-    DGOP_TRY(segment_done(s, st, c, &stop));
-    if (stop) break;
+  const int64_t chunks = ((int64_t)std::max(max_iters, 0) + kCheckEvery - 1) / kCheckEvery;
+  if (s.whole && s.use_graphs) {
+    if (chunks > 0) DGOP_TRY(run_whole(s, st, b, x, done, (int)std::min<int64_t>(chunks, INT32_MAX), chunk));
+  } else {
+    for (int c = 0; c < chunks; ++c) {
+      DGOP_TRY(run_segment(s, st, b, x, chunk));
+      bool stop = false;
+      DGOP_TRY(segment_done(s, st, c, &stop));
+      if (stop) break;
+    }
   }
   return finish<CGState>(s, st, res);
 }
@@ -699,11 +781,15 @@ int gmres_solve(SolverImpl& s, const double* b, double* x, int max_iters, double
   } else {
     DGOP_TRY(residual(0, st));
     // every cycle performs at least one iteration or finishes the solve
-    for (int c = 0; c <= max_iters; ++c) {
-      DGOP_TRY(run_segment(s, st, b, x, cycle));
-      bool stop = false;
-      DGOP_TRY(segment_done(s, st, c, &stop));
-      if (stop) break;
+    if (s.whole && s.use_graphs) {
+      DGOP_TRY(run_whole(s, st, b, x, done, max_iters < INT32_MAX ? max_iters + 1 : INT32_MAX, cycle));
+    } else {
+      for (int c = 0; c <= max_iters; ++c) {
+        DGOP_TRY(run_segment(s, st, b, x, cycle));
+        bool stop = false;
+        DGOP_TRY(segment_done(s, st, c, &stop));
+        if (stop) break;
+      }
     }
   }
   return finish<GMState>(s, st, res);
@@ -799,11 +885,15 @@ int gmres_ir_solve(SolverImpl& s, const double* b, double* x, int max_iters, dou
     DGOP_TRY(residual(2, st));
   } else {
     DGOP_TRY(residual(0, st));
-    for (int c = 0; c <= max_iters; ++c) {
-      DGOP_TRY(run_segment(s, st, b, x, cycle));
-      bool stop = false;
-      DGOP_TRY(segment_done(s, st, c, &stop));
-      if (stop) break;
+    if (s.whole && s.use_graphs) {
+      DGOP_TRY(run_whole(s, st, b, x, done, max_iters < INT32_MAX ? max_iters + 1 : INT32_MAX, cycle));
+    } else {
+      for (int c = 0; c <= max_iters; ++c) {
+        DGOP_TRY(run_segment(s, st, b, x, cycle));
+        bool stop = false;
+        DGOP_TRY(segment_done(s, st, c, &stop));
+        if (stop) break;
+      }
     }
   }
   return finish<GMState>(s, st, res);
@@ -936,7 +1026,12 @@ int dgop_solver_set_graphs(dgop_solver* sv, int enable) {
     set_error("dgop_solver_set_graphs: null solver");
     return DGOP_ERR_ARG;
   }
-  sv->s.use_graphs = enable != 0;
+  if (enable < 0 || enable > DGOP_GRAPHS_WHOLE) {
+    set_error("dgop_solver_set_graphs: enable must be DGOP_GRAPHS_OFF, DGOP_GRAPHS_SEGMENTS or DGOP_GRAPHS_WHOLE");
+    return DGOP_ERR_ARG;
+  }
+  sv->s.use_graphs = enable != DGOP_GRAPHS_OFF;
+  sv->s.whole = enable == DGOP_GRAPHS_WHOLE;
   return DGOP_OK;
 }
 
@@ -998,7 +1093,8 @@ int dgop_solver_set_fused_dot(dgop_solver* sv, int enable) {
     return DGOP_ERR_ARG;
   }
   sv->s.fuse_dot = enable != 0;
-  sv->s.key_version = -1;  // re-capture the segment graph
+  sv->s.key = GraphKey{};  // re-capture the solver graphs
+  sv->s.wkey = GraphKey{};
   return DGOP_OK;
 }
 

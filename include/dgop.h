@@ -233,10 +233,20 @@ int dgop_gmres_ir_create(dgop_operator* op, int restart, int inner_precision, dg
 int dgop_solver_solve(dgop_solver* solver, const double* b, double* x, int max_iters, double tol,
                       dgop_solve_result* result, void* stream);
 int dgop_solver_destroy(dgop_solver* solver);
-/* Solver segments (a chunk of CG iterations, a GMRES restart cycle) are captured once as a CUDA
- * graph and replayed; the graph is re-captured when b, x or the operator's kernel selection
- * change (tolerance and iteration limit live in device memory).  enable = 0 launches every kernel directly instead (same results, bit for
- * bit).  No reference counterpart. */
+/* How a solve is launched (no reference counterpart; the three give the same results, bit for
+ * bit):
+ *   DGOP_GRAPHS_SEGMENTS (1, the default): each segment (a chunk of CG iterations, a GMRES
+ *     restart cycle) is captured once as a CUDA graph and replayed, the host reading the done
+ *     word one segment behind the queued work;
+ *   DGOP_GRAPHS_WHOLE (2): the whole solve is ONE graph launch, a conditional WHILE node that
+ *     replays the segment until the solve is done or max_iters is exhausted, with no host round
+ *     trip between segments (the loop is bounded by the segment count max_iters allows);
+ *   DGOP_GRAPHS_OFF (0): every kernel is launched directly.
+ * Graphs are re-captured when b, x or the operator's kernel selection change (tolerance and
+ * iteration limit live in device memory). */
+#define DGOP_GRAPHS_OFF 0
+#define DGOP_GRAPHS_SEGMENTS 1
+#define DGOP_GRAPHS_WHOLE 2
 int dgop_solver_set_graphs(dgop_solver* solver, int enable);
 /* transpose != 0: the solver solves A^T x = b (the adjoint of the operator's linear part, inflow
  * value 0; dgop_apply_transpose) with the same algorithm; used by adjoint solves.  No reference

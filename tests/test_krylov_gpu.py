@@ -174,29 +174,55 @@ def _solvers(op):
             "ir32": lambda: g.GMRESIRSolver(op, 10, inner="fp32"), "ir64": lambda: g.GMRESIRSolver(op, 10, inner="fp64")}
 
 
+@pytest.mark.parametrize("mode", [True, "whole"], ids=["segments", "whole"])
 @pytest.mark.parametrize("kind", ["cg", "gmres", "ir32", "ir64"])
-def test_graph_replay_equals_direct_launches(kind):
-    """Graph-replayed segments give the same iterates, bit for bit, as direct launches, also when
-    the graph has to be re-captured for new vectors, a new tolerance or a new kernel selection."""
+def test_graph_replay_equals_direct_launches(kind, mode):
+    """Graph-replayed segments, and the whole solve as one graph launch (a conditional WHILE
+    node), give the same iterates, bit for bit, as direct launches, also when the graph has to be
+    re-captured for new vectors, a new tolerance or a new kernel selection, and when the
+    iteration limit ends the solve."""
     case = {"D": 3, "P": 2, "Q": 3, "basis": 0, "sizes": [5, 4, 6], "h": [0.2, 0.25, 1 / 6], "origin": [0.0] * 3,
             "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "sigma_c": 30.0}
     sp = make_space(case)
     op = g.MassOperator(sp, 3, C.sigma_preset(1, 3, 1.0)) if kind == "cg" else _system(case, sp)
     direct = _solvers(op)[kind]().use_graphs(False)
-    graphed = _solvers(op)[kind]()
-    for seed, tol in ((2, 1e-10), (3, 1e-10), (3, 1e-6)):
+    graphed = _solvers(op)[kind]().use_graphs(mode)
+    for seed, tol, its in ((2, 1e-10, 300), (3, 1e-10, 300), (3, 1e-6, 300), (2, 1e-14, 13), (2, 1e-10, 0)):
         b = torch.from_numpy(oracle().fill_random(sp.num_dofs, seed)).cuda()
         x0 = torch.zeros_like(b)
         x1 = torch.zeros_like(b)
-        r0 = direct.solve(b, x0, 300, tol)
-        r1 = graphed.solve(b, x1, 300, tol)
+        r0 = direct.solve(b, x0, its, tol)
+        r1 = graphed.solve(b, x1, its, tol)
         assert r0 == r1
         assert torch.equal(x0, x1)
+        if its == 13:
+            assert r1["iterations"] <= 13 and (r1["success"] or r1["iterations"] == 13)
     if op.kernel == "kron":
         op.select_kernel("generic")
         b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 4)).cuda()
         x0, x1 = torch.zeros_like(b), torch.zeros_like(b)
         assert direct.solve(b, x0, 300, 1e-10) == graphed.solve(b, x1, 300, 1e-10)
+        assert torch.equal(x0, x1)
+
+
+@pytest.mark.parametrize("inner", ["fp64", "fp32"])
+def test_whole_solve_graph_with_preconditioner(inner):
+    """The preconditioned refinement solve (mass inverse as right preconditioner) as one graph
+    launch equals direct launches bit for bit, on the 3D Kronecker kernel and on repeat."""
+    case = {"D": 3, "P": 3, "Q": 4, "basis": 0, "sizes": [8, 8, 8], "h": [0.125] * 3, "origin": [0.0] * 3,
+            "periodic": [0] * 3, "beta_kind": 2, "g": 0.0, "sigma_c": 100.0}
+    sp = make_space(case)
+    op = _system(case, sp)
+    prec = g.MassInverseOperator(sp, 4, 100.0)
+    direct = g.GMRESIRSolver(op, 20, inner=inner).precondition(prec).use_graphs(False)
+    whole = g.GMRESIRSolver(op, 20, inner=inner).precondition(prec).use_graphs("whole")
+    b = torch.from_numpy(oracle().fill_random(sp.num_dofs, 5)).cuda()
+    x0 = torch.zeros_like(b)
+    r0 = direct.solve(b, x0, 500, 1e-10)
+    assert r0["success"]
+    for _ in range(2):
+        x1 = torch.zeros_like(b)
+        assert whole.solve(b, x1, 500, 1e-10) == r0
         assert torch.equal(x0, x1)
 
 
