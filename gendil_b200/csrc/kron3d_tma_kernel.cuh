@@ -119,24 +119,44 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // Double index of value c (0..15) of plane row r in a 128 B-swizzled, 1024-byte aligned buffer.
 __device__ __forceinline__ int swz(int r, int c) { return r * 16 + ((((c >> 1) ^ (r & 7))) << 1) + (c & 1); }
 
+// 16-byte shared-memory accesses by byte address.  In a 1024-byte aligned buffer, chunk k of
+// row r sits at base + r * 128 + ((k ^ (r & 7)) << 4), and since base + r * 128 has bits 4-6
+// clear that is ((base + r * 128) | ((r & 7) << 4)) ^ (k << 4): one XOR per access with a
+// per-lane row address computed once.
+__device__ __forceinline__ double2 lds_v2(uint32_t a) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts_v2(uint32_t a, double x, double y) {
+  asm volatile("st.shared.v2.f64 [%0], {%1, %2};\n" ::"r"(a), "d"(x), "d"(y) : "memory");
+}
+// Row address of plane row r with its swizzle pattern folded in (see above).
+__device__ __forceinline__ uint32_t swz_row(uint32_t base, int r) {
+  return (base + (uint32_t)r * 128u) | ((uint32_t)(r & 7) << 4);
+}
+
 // Plane t of group element le in layout Z (values [x][y]) / layout Y (plane y = t, values [x][z]).
-__device__ __forceinline__ void tma_plane_z(const double* grp, int le, int t, double (&u)[4][4]) {
-  const int r = 4 * le + t;
+__device__ __forceinline__ void tma_plane_z(uint32_t grp_sa, int le, int t, double (&u)[4][4]) {
+  const uint32_t row = swz_row(grp_sa, 4 * le + t);
 #pragma unroll
   for (int y = 0; y < 4; ++y)
 #pragma unroll
     for (int x = 0; x < 4; x += 2) {
-      const double2 v = *reinterpret_cast<const double2*>(grp + swz(r, 4 * y + x));
+      const double2 v = lds_v2(row ^ ((uint32_t)(2 * y + x / 2) << 4));  // chunk (4 y + x) / 2
       u[x][y] = v.x;
       u[x + 1][y] = v.y;
     }
 }
-__device__ __forceinline__ void tma_plane_y(const double* grp, int le, int t, double (&u)[4][4]) {
+// Rows 4 le + z, chunk 2 t + x / 2: with l = le & 1 the swizzled chunk is (2 t ^ 4 l) ^ (x / 2 ^ z),
+// a per-lane part and a compile-time part; row z adds z * 128 (bits 7-8, clear in the base).
+__device__ __forceinline__ void tma_plane_y(uint32_t grp_sa, int le, int t, double (&u)[4][4]) {
+  const uint32_t row = (grp_sa + (uint32_t)le * 512u) | ((uint32_t)((2 * t) ^ (4 * (le & 1))) << 4);
 #pragma unroll
   for (int z = 0; z < 4; ++z)
 #pragma unroll
     for (int x = 0; x < 4; x += 2) {
-      const double2 v = *reinterpret_cast<const double2*>(grp + swz(4 * le + z, 4 * t + x));
+      const double2 v = lds_v2((row ^ ((uint32_t)((x / 2) ^ z) << 4)) + (uint32_t)z * 128u);
       u[x][z] = v.x;
       u[x + 1][z] = v.y;
     }
@@ -331,6 +351,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     kron_coords(P, (uint32_t)e, c);
     const uint32_t ef = adv ? __ldg(T.eflags + e) : 0u;
     const double* grp = reinterpret_cast<const double*>(area + st * kTmaStageBytes);
+    const uint32_t grp_sa = smem_addr(grp);
     const double* zslot = grp + kTmaGroupBytes / 8;
     const double* yslot = zslot + kTmaSlotBytes / 8;
     const double* mats = yslot + kTmaSlotBytes / 8;
@@ -347,7 +368,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     // ------------------------------------------------------------ layout Z (plane z = t)
     if (adv) {
       double u[N][N];
-      tma_plane_z(grp, le, t, u);
+      tma_plane_z(grp_sa, le, t, u);
       {
         double px[N][N];
         tma_apply<kSlotDX, true, false>(T, c[0], mats, u, px);
@@ -414,7 +435,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
         tma_apply<kSlotTYX, true, true>(T, c[0], mats, qx, out);   // out += Tyx (Tyz py)
       }
       double u[N][N], pz[N][N];
-      tma_plane_y(grp, le, t, u);
+      tma_plane_y(grp_sa, le, t, u);
       tma_apply<kSlotDZ, false, false>(T, c[2], mats, u, pz);
       if (adv) {
         const double elz = P.elem[2] ? P.elem[2][e] : 1.0;
@@ -495,7 +516,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     }
     __syncwarp();  // every lane is done reading this stage's planes and slices
     double* gout = const_cast<double*>(grp);
-    const int r = 4 * le + t;
+    const uint32_t orow = swz_row(grp_sa, 4 * le + t);  // this lane's plane row (layout Z)
     if constexpr (DOT) {
       double acc = 0.0;
       const double* zp = P.dot_z + e * 64 + 16 * t;
@@ -503,7 +524,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
       for (int j = 0; j < N; ++j)
 #pragma unroll
         for (int i = 0; i < N; i += 2) {
-          const double2 z = dot_in ? *reinterpret_cast<const double2*>(gout + swz(r, 4 * j + i))
+          const double2 z = dot_in ? lds_v2(orow ^ ((uint32_t)(2 * j + i / 2) << 4))
                                    : *reinterpret_cast<const double2*>(zp + 4 * j + i);
           acc += res[i][j] * z.x;
           acc += res[i + 1][j] * z.y;
@@ -513,8 +534,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
     for (int j = 0; j < N; ++j)
 #pragma unroll
-      for (int i = 0; i < N; i += 2)
-        *reinterpret_cast<double2*>(gout + swz(r, 4 * j + i)) = make_double2(res[i][j], res[i + 1][j]);
+      for (int i = 0; i < N; i += 2) sts_v2(orow ^ ((uint32_t)(2 * j + i / 2) << 4), res[i][j], res[i + 1][j]);
     fence_proxy_async_smem();
     __syncwarp();
     if (lane == 0) {
