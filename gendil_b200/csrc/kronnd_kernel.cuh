@@ -35,9 +35,14 @@ struct KronNDShape {
   static constexpr int NS = D * D + D;   // matrix slots: D terms x D axes, plus the mass term
   static constexpr int MAT = N * N;
   // per element: U, W, Y, the slot matrices, and 2D face records (corner, neighbour / inflow
-  // coefficient) + one flag byte per face (16 bytes, whatever the Real)
+  // coefficient) + one flag byte per face (16 bytes, whatever the Real).  The matrix area and
+  // every matrix start on a multiple of 4 values (16 bytes in FP32, 32 in FP64), so a pass reads
+  // its matrix with 16-byte loads.
+  static constexpr int MATP = (MAT + 3) / 4 * 4;    // stride of the slot matrices
+  static constexpr int MOFF = (3 * ND + 3) / 4 * 4;  // offset of the matrix area
+  static constexpr int ROFF = MOFF + NS * MATP;       // offset of the face records
   static constexpr int REC = 4 * D + 16 / (int)sizeof(float);
-  static constexpr int PER_ELEM = 3 * ND + NS * MAT + REC;
+  static constexpr int PER_ELEM = (ROFF + REC + 3) / 4 * 4;
 };
 
 // Matrix of a pass: in registers for N <= 4 (loaded once per pass), read from shared memory
@@ -60,6 +65,36 @@ struct PassMat<N, Real, false> {
   __device__ __forceinline__ Real operator()(int j, int i) const { return m[j * N + i]; }
 };
 
+// A slot matrix of the per-element matrix area (KronNDShape::MATP: 16-byte aligned, padded to a
+// multiple of 4 values): in registers for N <= 4, read with 16-byte loads; as PassMat otherwise.
+template <int N, typename Real, bool REG = (N <= 4)>
+struct SlotMat : PassMat<N, Real, false> {
+  __device__ __forceinline__ explicit SlotMat(const Real* p) : PassMat<N, Real, false>(p) {}
+};
+template <int N, typename Real>
+struct SlotMat<N, Real, true> {
+  static constexpr int V = 16 / (int)sizeof(Real);  // values per 16-byte load
+  static constexpr int NV = (N * N + V - 1) / V;    // loads (within the padded slot)
+  Real a[NV * V];
+  __device__ __forceinline__ explicit SlotMat(const Real* m) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      if constexpr (V == 4) {
+        const float4 w = reinterpret_cast<const float4*>(m)[k];
+        a[4 * k] = w.x;
+        a[4 * k + 1] = w.y;
+        a[4 * k + 2] = w.z;
+        a[4 * k + 3] = w.w;
+      } else {
+        const double2 w = reinterpret_cast<const double2*>(m)[k];
+        a[2 * k] = w.x;
+        a[2 * k + 1] = w.y;
+      }
+    }
+  }
+  __device__ __forceinline__ Real operator()(int j, int i) const { return a[j * N + i]; }
+};
+
 // One pass along axis A over the batch: the CTA's threads form EB groups of blockDim / EB, group
 // b runs the lines of element b with the element's matrix held in registers.
 //   FIRST: W <- M U (times the element factor when escale is given)
@@ -74,7 +109,7 @@ __device__ __forceinline__ void nd_pass(Real* base, int ne, int eb, int slot, co
   Real* el = base + (size_t)b * S::PER_ELEM;
   const Real* in = FIRST ? el : el + S::ND;
   Real* out = ACC ? el + 2 * S::ND : el + S::ND;
-  const PassMat<N, Real> m(el + 3 * S::ND + slot * S::MAT);
+  const SlotMat<N, Real> m(el + S::MOFF + slot * S::MATP);
   const Real f = (FIRST && escale) ? escale[b] : Real(1);
   for (int r = threadIdx.x - b * tpe; r < S::NL; r += tpe) {
     const int o = r / INNER;
@@ -152,7 +187,7 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
     const int p = l - b * S::NL;  // point of the slice: (o, t) with the axis index removed
     const int o = p / INNER, t = p - o * INNER;
     Real* el = base + (size_t)b * S::PER_ELEM;
-    const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+    const Real* rec = el + S::ROFF;
     const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -210,12 +245,12 @@ __device__ __forceinline__ void nd_setup(const KronNDParams<Real>& P, const Real
     const KronMat m = a < D ? P.slot[a][k] : P.mslot[k];
     Real v = Real(0);
     if (m.off >= 0) v = P.mats[m.off + (int64_t)ecoord[b][k] * m.stride + q];
-    base[(size_t)b * S::PER_ELEM + 3 * S::ND + r] = v;
+    base[(size_t)b * S::PER_ELEM + S::MOFF + sl * S::MATP + q] = v;
   }
   if (adv) {
     for (int l = threadIdx.x; l < ne * 2 * D; l += blockDim.x) {
       const int b = l / (2 * D), fi = l - b * (2 * D);
-      Real* rec = base + (size_t)b * S::PER_ELEM + 3 * S::ND + S::NS * S::MAT;
+      Real* rec = base + (size_t)b * S::PER_ELEM + S::ROFF;
       nd_face_record<D>(P, e0 + b, ecoord[b], fi, rec, reinterpret_cast<uint8_t*>(rec + 4 * D) + fi);
     }
   }
@@ -369,7 +404,7 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
       constexpr int k = GR::axis(g, decltype(kc)::value, FIRST, AX);
       constexpr int SK = kpow(N, k - LO);  // stride of axis k inside the block
       constexpr bool OWN = FIRST && k == AX;
-      const PassMat<N, Real> m(el + 3 * S::ND + (MASS ? D * D + k : TERM * D + k) * S::MAT);
+      const SlotMat<N, Real> m(el + S::MOFF + (MASS ? D * D + k : TERM * D + k) * S::MATP);
       Real scale = Real(1);
       if constexpr (OWN) {
         const Real* ef = MASS ? P.elem_mass : P.elem[AX];
@@ -393,7 +428,7 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
           }
           if constexpr (!MASS) {
             // face terms of axis AX on the line's two ends (GLL: the trace is the end value)
-            const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+            const Real* rec = el + S::ROFF;
             const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
 #pragma unroll
             for (int sd = 0; sd < 2; ++sd) {
@@ -506,7 +541,7 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
       r = q;
     }
     Real* el = base + (size_t)b * S::PER_ELEM;
-    const Real* mats = el + 3 * S::ND;
+    const Real* mats = el + S::MOFF;
     const Real* src = OWN ? el : el + S::ND;
     Real v[N][N];  // v[i][j]: index i along A, j along B
 #pragma unroll
@@ -519,15 +554,15 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
       for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int j = 0; j < N; ++j) acc[i][j] = Real(0);
-      const Real* rec = el + 3 * S::ND + S::NS * S::MAT;
+      const Real* rec = el + S::ROFF;
       const uint8_t* fb = reinterpret_cast<const uint8_t*>(rec + 4 * D);
       // own term of axis X (X == A: along the first index) then its factor along the other
       auto own_term = [&](auto xc) {
         constexpr int X = decltype(xc)::value;
         constexpr bool FIRST = X == A;
         constexpr int Y = FIRST ? B : A;
-        const PassMat<N, Real> dm(mats + (X * D + X) * S::MAT);
-        const PassMat<N, Real> tm(mats + (X * D + Y) * S::MAT);
+        const SlotMat<N, Real> dm(mats + (X * D + X) * S::MATP);
+        const SlotMat<N, Real> tm(mats + (X * D + Y) * S::MATP);
         const Real scale = P.elem[X] ? P.elem[X][e0 + b] : Real(1);
         Real w[N][N];
 #pragma unroll
@@ -585,8 +620,8 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
       }
       if (mass) {
         // MD along the last axis (B of the last pair, scaled), then MT along A
-        const PassMat<N, Real> md(mats + (D * D + B) * S::MAT);
-        const PassMat<N, Real> mt(mats + (D * D + A) * S::MAT);
+        const SlotMat<N, Real> md(mats + (D * D + B) * S::MATP);
+        const SlotMat<N, Real> mt(mats + (D * D + A) * S::MATP);
         const Real scale = P.elem_mass ? P.elem_mass[e0 + b] : Real(1);
         Real w[N][N];
 #pragma unroll
@@ -611,8 +646,8 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
     } else {
       // the pair's shared factors along A and B (term PG's; equal to term PG + H's)
       const int t0 = P.has_adv ? PG : D;  // the mass term alone: its own factors
-      const PassMat<N, Real> fa(mats + (t0 < D ? t0 * D + A : D * D + A) * S::MAT);
-      const PassMat<N, Real> fbm(mats + (t0 < D ? t0 * D + B : D * D + B) * S::MAT);
+      const SlotMat<N, Real> fa(mats + (t0 < D ? t0 * D + A : D * D + A) * S::MATP);
+      const SlotMat<N, Real> fbm(mats + (t0 < D ? t0 * D + B : D * D + B) * S::MATP);
       Real w[N][N];
 #pragma unroll
       for (int i = 0; i < N; ++i)
