@@ -874,7 +874,7 @@ def run_sipdg(args):
     return 0
 
 
-def main():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
@@ -890,12 +890,17 @@ def main():
                          "batch: 512 uneven implicit systems; sipdg: 32^3 p=4 diffusion apply, solve and gradient")
     ap.add_argument("--fd", type=int, default=64, help="sipdg workload: elements checked by central differences")
     ap.add_argument("--instances", type=int, default=512, help="batch workload: number of instances")
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
     args.size_6d = args.size or 8
     args.size_sipdg = args.size or 32
     args.size = args.size or N_AXIS
     if args.warmup < 3:
         args.warmup = 3
+    return args
+
+
+def main():
+    args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
