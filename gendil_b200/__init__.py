@@ -313,7 +313,7 @@ class _Operator:
         check(lib().dgop_operator_select_kernel(self.handle, {"generic": 0, "kron": 1, "kronnd": 2}[name]))
 
     VARIANTS = ("stage2-tile", "stage1-tile", "stage2-shfl", "tma1-tile", "tma2-shfl", "tma2-tile")  # 3D ("kron")
-    ND_VARIANTS = ("nd-passes", "nd-grouped2", "nd-grouped3", "nd-paired")  # any-dimension kernel ("kronnd")
+    ND_VARIANTS = ("nd-passes", "nd-grouped2", "nd-grouped3", "nd-paired", "nd-mass")  # any-dimension kernel
 
     def _variants(self):
         return self.ND_VARIANTS if self.kernel == "kronnd" else self.VARIANTS

@@ -10,7 +10,8 @@ namespace dgop {
 const char* const kKronVariantNames[kKronVariants] = {"stage2-tile", "stage1-tile", "stage2-shfl",
                                                       "tma1-tile",   "tma2-shfl",   "tma2-tile"};
 // (the any-dimension kernel's variants, kronnd_kernel.cuh, named here with the 3D kernel's)
-const char* const kKronNDVariantNames[kKronNDVariants] = {"nd-passes", "nd-grouped2", "nd-grouped3", "nd-paired"};
+const char* const kKronNDVariantNames[kKronNDVariants] = {"nd-passes", "nd-grouped2", "nd-grouped3", "nd-paired",
+                                                          "nd-mass"};
 
 namespace {
 template <int N, typename Real, int STAGES, bool SHFL>

@@ -38,6 +38,11 @@ void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, 
 }
 
 template <int D, int N, typename Real>
+void launch_kronnd_mass(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  kronnd_mass_kernel<D, N, 2, Real><<<grid, block, smem, s>>>(p);
+}
+
+template <int D, int N, typename Real>
 void launch_kronnd_paired(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   kronnd_paired_kernel<D, N, Real><<<grid, block, smem, s>>>(p);
 }
@@ -70,6 +75,9 @@ void fill(KronNDEntry<Real>& d) {
     if constexpr (D >= 2 && N >= 2 && N * N <= 27) {
       d.launch_g[0] = &launch_kronnd_grouped<D, N, 2, Real>;
       d.func_g[0] = reinterpret_cast<const void*>(&kronnd_grouped_kernel<D, N, 2, Real>);
+      d.launch_m = &launch_kronnd_mass<D, N, Real>;
+      d.func_m = reinterpret_cast<const void*>(&kronnd_mass_kernel<D, N, 2, Real>);
+      d.per_elem_m = KronNDMassShape<D, N>::PER_ELEM;
       if constexpr (sizeof(Real) == 8) {
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);

@@ -50,8 +50,9 @@ void register_kron3d();
 // Kronecker form, any dimension, shared-memory kernel (kronnd_kernel.cuh).  Variants (the
 // autotuner picks one per operator): 0 one shared-memory pass per axis; 1, 2 groups of 2 or 3
 // axes per pass in registers; 3 axes a and a + D/2 paired, the two terms of a pair run together
-// (even D, operators whose term pairs share their other factors).
-constexpr int kKronNDVariants = 4;
+// (even D, operators whose term pairs share their other factors); 4 operators without advection
+// terms (mass, mass inverse): groups of 2 axes passed in place, a third of the shared memory.
+constexpr int kKronNDVariants = 5;
 extern const char* const kKronNDVariantNames[kKronNDVariants];
 
 template <typename Real>
@@ -67,6 +68,10 @@ struct KronNDEntry {
   // (kronnd_paired_kernel): same parameters and layout
   void (*launch_g[3])(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = {};
   const void* func_g[3] = {};
+  // mass-only variant (kronnd_mass_kernel, its own layout of per_elem_m values per element)
+  void (*launch_m)(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
+  const void* func_m = nullptr;
+  int per_elem_m = 0;
   // BF16 tensor-core variant (kronnd_tc_kernel.cuh; FP32 parameters, even D, N^(D/2) <= 32)
   void (*launch_tc)(const KronNDParams<float>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_tc = nullptr;
