@@ -285,11 +285,12 @@ def mass_c1(g, torch, dev, steps, warmup, hbm):
     return out
 
 
-def mass_large(g, torch, dev, steps, warmup, hbm, n):
-    """The FP64 mass apply (p = 3 GLL, q = 4, sigma = 1) on the bench's n^3 mesh: 16 B/DoF moved
-    per apply with inputs larger than L2, the regime where the HBM roofline binds."""
-    space = g.Space(3, [n] * 3, order=3)
-    op = g.MassOperator(space, 4, 1.0)
+def mass_large(g, torch, dev, steps, warmup, hbm, n, space=None, q=4, label=None):
+    """The FP64 mass apply (sigma = 1) on the bench's mesh (3D n^3 p = 3 GLL, q = 4 unless `space`,
+    `q` and `label` name another): 16 B/DoF moved per apply with inputs larger than L2, the regime
+    where the HBM roofline binds."""
+    space = space or g.Space(3, [n] * 3, order=3)
+    op = g.MassOperator(space, q, 1.0)
     nd = space.num_dofs
     x = torch.from_numpy(g.fill_random(nd, 0)).to(dev)
     y = torch.empty_like(x)
@@ -304,7 +305,8 @@ def mass_large(g, torch, dev, steps, warmup, hbm, n):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     alg = 16.0 * nd
-    out = {"workload": f"fp64 mass apply, 3D {n}^3 hex, p=3 GLL, q=4 GL, sigma=1", "dofs": nd, "kernel": op.kernel,
+    out = {"workload": label or f"fp64 mass apply, 3D {n}^3 hex, p=3 GLL, q=4 GL, sigma=1", "dofs": nd,
+           "kernel": op.kernel,
            "variant": op.variant, "ms_per_apply": ms, "gdofs_per_s": nd / (ms * 1e-3) / 1e9,
            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                         "frac": alg / (ms * 1e-3) / 1e9 / hbm},
@@ -523,6 +525,9 @@ def run_ours(args):
         if not six and world == 1:
             line["mass_c1"] = mass_c1(g, torch, dev, args.steps, args.warmup, hbm)
             line["mass_64cubed"] = mass_large(g, torch, dev, args.steps, args.warmup, hbm, args.size)
+        if six and world == 1:
+            line["mass_6d"] = mass_large(g, torch, dev, min(args.steps, 20), args.warmup, hbm, n6, space=space, q=3,
+                                         label=f"fp64 mass apply, 6D {n6}^6 hypercubes, p=2 GLL, q=3 GL, sigma=1")
         if world == 1 and not args.no_solve:
             if six:
                 # configuration 3: dt = 5e-3, inner GMRES(20), b from seed 3.  The unpreconditioned

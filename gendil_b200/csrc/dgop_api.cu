@@ -897,7 +897,8 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     const int G = (v == 3 || mass_only) ? 2 : v + 1;  // the paired variant's blocks span two axes
     const void* fn = mass_only ? entry->func_m : entry->func_g[v - 1];
     if (!fn || (v == 3 && !paired) || (mass_only && (plan.has_adv || !plan.has_mass))) continue;
-    const size_t pv = mass_only ? (size_t)entry->per_elem_m * sizeof(Real) : per;
+    // the mass-only kernel holds two batches (the next one's input arrives during this one's passes)
+    const size_t pv = mass_only ? 2 * (size_t)entry->per_elem_m * sizeof(Real) : per;
     int64_t gsz = 1;
     for (int k = 0; k < std::min(G, D); ++k) gsz *= N;
     const int64_t ipe = (s.ndofs / s.nelem) / gsz;  // blocks per element

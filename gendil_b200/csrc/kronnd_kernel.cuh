@@ -785,6 +785,21 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
   }
 }
 
+// Asynchronous copy of one value from global to shared memory (4 or 8 bytes).
+template <typename Real>
+__device__ __forceinline__ void cp_async_value(Real* dst, const Real* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(Real) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// The CTA's batches alternate between two buffers of EB elements: while a batch computes in one,
+// the next batch's input arrives in the other by asynchronous copies (issued at the start of the
+// batch, one commit group per batch, awaited at the start of the next), so the input loads of a
+// batch overlap the previous batch's passes.  The kernel is bound by registers, not shared
+// memory, so the second buffer costs no resident warps.
 template <int D, int N, int G, typename Real>
 __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __grid_constant__ KronNDParams<Real> P) {
   using S = KronNDShape<D, N>;
@@ -795,40 +810,55 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __gri
   __shared__ int ecoord[64][kMaxDim];
   if (P.skip && *P.skip) return;
   const int EB = P.eb;
-  for (int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB; e0 < P.nelem; e0 += (int64_t)gridDim.x * EB) {
-    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
-    __syncthreads();  // the previous batch's output has been read
-    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-      const int b = l / S::ND, i = l - b * S::ND;
-      base[(size_t)b * M::PER_ELEM + i] = P.x[e0 * S::ND + l];
+  const int64_t stride = (int64_t)gridDim.x * EB;
+  // input of the batch starting at e0 into buffer buf (one commit group, possibly empty)
+  auto stage = [&](int64_t e0, int buf) {
+    if (e0 < P.nelem) {
+      const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+      Real* dst = base + (size_t)buf * EB * M::PER_ELEM;
+      for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
+        const int b = l / S::ND, i = l - b * S::ND;
+        cp_async_value(dst + (size_t)b * M::PER_ELEM + i, P.x + e0 * S::ND + l);
+      }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB;
+  stage(e0, 0);
+  for (int k = 0; e0 < P.nelem; e0 += stride, ++k) {
+    const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
+    Real* cur = base + (size_t)(k & 1) * EB * M::PER_ELEM;
+    __syncthreads();  // the previous batch is done with the other buffer (its output was read)
+    stage(e0 + stride, (k + 1) & 1);
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this batch's copies (this thread's)
     if (threadIdx.x < ne) {
       const int64_t e = e0 + threadIdx.x;
 #pragma unroll
-      for (int k = 0; k < D; ++k) ecoord[threadIdx.x][k] = (int)((e / P.estride[k]) % P.sizes[k]);
+      for (int kk = 0; kk < D; ++kk) ecoord[threadIdx.x][kk] = (int)((e / P.estride[kk]) % P.sizes[kk]);
     }
     __syncthreads();
     for (int l = threadIdx.x; l < ne * D * S::MAT; l += blockDim.x) {
       const int b = l / (D * S::MAT);
       const int r = l - b * (D * S::MAT);
-      const int k = r / S::MAT, q = r - k * S::MAT;
-      const KronMat mk = P.mslot[k];
+      const int kk = r / S::MAT, q = r - kk * S::MAT;
+      const KronMat mk = P.mslot[kk];
       Real v = Real(0);
-      if (mk.off >= 0) v = P.mats[mk.off + (int64_t)ecoord[b][k] * mk.stride + q];
-      base[(size_t)b * M::PER_ELEM + M::MOFF + k * S::MATP + q] = v;
+      if (mk.off >= 0) v = P.mats[mk.off + (int64_t)ecoord[b][kk] * mk.stride + q];
+      cur[(size_t)b * M::PER_ELEM + M::MOFF + kk * S::MATP + q] = v;
     }
     __syncthreads();
     static_for<0, GR::NG>([&](auto sc) {
-      nd_mass_step<D, N, G, decltype(sc)::value>(P, base, ne, e0);
+      nd_mass_step<D, N, G, decltype(sc)::value>(P, cur, ne, e0);
       __syncthreads();
     });
     for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
       const int b = l / S::ND, i = l - b * S::ND;
-      const Real v = base[(size_t)b * M::PER_ELEM + i];
+      const Real v = cur[(size_t)b * M::PER_ELEM + i];
       Real* dst = P.y + e0 * S::ND + l;
       *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
     }
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy outlives the kernel
 }
 
 // Many operators of one (D, N) and kernel variant V (0: one pass per axis, 1 / 2: groups of 2 / 3
