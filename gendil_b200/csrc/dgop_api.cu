@@ -898,13 +898,15 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     const void* fn = mass_only ? entry->func_m : entry->func_g[v - 1];
     if (!fn || (v == 3 && !paired) || (mass_only && (plan.has_adv || !plan.has_mass))) continue;
     // the mass-only kernel holds two batches (the next one's input arrives during this one's passes)
+    // and one copy of the D mass matrices when they are the same for every element
     const size_t pv = mass_only ? 2 * (size_t)entry->per_elem_m * sizeof(Real) : per;
+    const size_t extra = mass_only ? (size_t)D * ((N * N + 3) / 4 * 4) * sizeof(Real) : 0;
     int64_t gsz = 1;
     for (int k = 0; k < std::min(G, D); ++k) gsz *= N;
     const int64_t ipe = (s.ndofs / s.nelem) / gsz;  // blocks per element
     int ebv = (int)std::max<int64_t>(1, std::min<int64_t>(64, (kKronNDThreads + ipe / 2) / ipe));
-    while (ebv > 1 && pv * ebv > std::min<size_t>((size_t)max_smem, 110 * 1024)) --ebv;
-    if (pv * ebv > (size_t)max_smem) continue;
+    while (ebv > 1 && pv * ebv + extra > std::min<size_t>((size_t)max_smem, 110 * 1024)) --ebv;
+    if (pv * ebv + extra > (size_t)max_smem) continue;
     cudaFuncAttributes fv{};
     if (cudaFuncGetAttributes(&fv, fn) != cudaSuccess) {
       cudaGetLastError();
@@ -913,13 +915,13 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     int max_v = 0;
     DGOP_CUDA(cudaDeviceGetAttribute(&max_v, cudaDevAttrMaxSharedMemoryPerBlockOptin, op->device));
     max_v -= (int)fv.sharedSizeBytes;
-    if (pv * ebv > (size_t)max_v) continue;
+    if (pv * ebv + extra > (size_t)max_v) continue;
     DGOP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_v));
     int per_sm_v = 0;
-    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, fn, kKronNDThreads, pv * ebv));
+    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, fn, kKronNDThreads, pv * ebv + extra));
     if (per_sm_v < 1) continue;
     const int64_t cv = std::min<int64_t>((s.nelem + ebv - 1) / ebv, (int64_t)device_sm_count(op->device) * per_sm_v);
-    K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), pv * ebv, 0.0f};
+    K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), pv * ebv + extra, 0.0f};
   }
   K.variant = 0;
   if constexpr (sizeof(Real) == 4) {
@@ -967,7 +969,7 @@ void launch_kronnd_variant(const KronNDCfg<Real>& K, int v, KronNDParams<Real> p
 
 // Time every usable variant on scratch vectors over the first elements (at most kTuneElems, so
 // that the cost stays bounded on large meshes) and keep the fastest.
-constexpr int64_t kTuneElems = 16384;
+constexpr int64_t kTuneElems = 65536;
 template <typename Real>
 int autotune_kronnd(dgop_operator* op, KronNDCfg<Real>& K) {
   int usable = 0, mask = 0;

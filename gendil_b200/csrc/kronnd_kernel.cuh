@@ -731,7 +731,8 @@ struct KronNDMassShape {
 };
 
 template <int D, int N, int G, int ST, typename Real>
-__device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* base, int ne, int64_t e0) {
+__device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* base, int ne, int64_t e0,
+                                             const Real* cm) {
   using S = KronNDShape<D, N>;
   using M = KronNDMassShape<D, N>;
   using GR = KronGroups<D, N, G>;
@@ -754,7 +755,7 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
       constexpr int k = GR::axis(g, decltype(kc)::value, FIRST, AX);
       constexpr int SK = kpow(N, k - LO);
       constexpr bool OWN = FIRST && k == AX;
-      const SlotMat<N, Real> m(el + M::MOFF + k * S::MATP);
+      const SlotMat<N, Real> m((cm ? cm : el + M::MOFF) + k * S::MATP);
       Real scale = Real(1);
       if constexpr (OWN) {
         if (P.elem_mass) scale = P.elem_mass[e0 + b];
@@ -823,32 +824,47 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __gri
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
+  // mass matrices that are the same for every element (constant coefficient, the usual case):
+  // one copy per CTA after the two buffers, instead of one per element and batch
+  bool shared_mats = true;
+#pragma unroll
+  for (int kk = 0; kk < D; ++kk) shared_mats = shared_mats && (P.mslot[kk].off < 0 || P.mslot[kk].stride == 0);
+  Real* cm = shared_mats ? base + (size_t)2 * EB * M::PER_ELEM : nullptr;
+  if (shared_mats) {
+    for (int l = threadIdx.x; l < D * S::MAT; l += blockDim.x) {
+      const int kk = l / S::MAT, q = l - kk * S::MAT;
+      const KronMat mk = P.mslot[kk];
+      cm[kk * S::MATP + q] = mk.off >= 0 ? P.mats[mk.off + q] : Real(0);
+    }
+  }
   int64_t e0 = P.e_begin + (int64_t)blockIdx.x * EB;
   stage(e0, 0);
   for (int k = 0; e0 < P.nelem; e0 += stride, ++k) {
     const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
     Real* cur = base + (size_t)(k & 1) * EB * M::PER_ELEM;
-    __syncthreads();  // the previous batch is done with the other buffer (its output was read)
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // this batch's copies (this thread's)
+    __syncthreads();  // every thread's copies landed; the previous batch is done with the other buffer
     stage(e0 + stride, (k + 1) & 1);
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this batch's copies (this thread's)
-    if (threadIdx.x < ne) {
-      const int64_t e = e0 + threadIdx.x;
+    if (!shared_mats) {
+      if (threadIdx.x < ne) {
+        const int64_t e = e0 + threadIdx.x;
 #pragma unroll
-      for (int kk = 0; kk < D; ++kk) ecoord[threadIdx.x][kk] = (int)((e / P.estride[kk]) % P.sizes[kk]);
+        for (int kk = 0; kk < D; ++kk) ecoord[threadIdx.x][kk] = (int)((e / P.estride[kk]) % P.sizes[kk]);
+      }
+      __syncthreads();
+      for (int l = threadIdx.x; l < ne * D * S::MAT; l += blockDim.x) {
+        const int b = l / (D * S::MAT);
+        const int r = l - b * (D * S::MAT);
+        const int kk = r / S::MAT, q = r - kk * S::MAT;
+        const KronMat mk = P.mslot[kk];
+        Real v = Real(0);
+        if (mk.off >= 0) v = P.mats[mk.off + (int64_t)ecoord[b][kk] * mk.stride + q];
+        cur[(size_t)b * M::PER_ELEM + M::MOFF + kk * S::MATP + q] = v;
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    for (int l = threadIdx.x; l < ne * D * S::MAT; l += blockDim.x) {
-      const int b = l / (D * S::MAT);
-      const int r = l - b * (D * S::MAT);
-      const int kk = r / S::MAT, q = r - kk * S::MAT;
-      const KronMat mk = P.mslot[kk];
-      Real v = Real(0);
-      if (mk.off >= 0) v = P.mats[mk.off + (int64_t)ecoord[b][kk] * mk.stride + q];
-      cur[(size_t)b * M::PER_ELEM + M::MOFF + kk * S::MATP + q] = v;
-    }
-    __syncthreads();
     static_for<0, GR::NG>([&](auto sc) {
-      nd_mass_step<D, N, G, decltype(sc)::value>(P, cur, ne, e0);
+      nd_mass_step<D, N, G, decltype(sc)::value>(P, cur, ne, e0, cm);
       __syncthreads();
     });
     for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
