@@ -887,14 +887,14 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
   }
   const int64_t ctas = std::min<int64_t>((s.nelem + eb - 1) / eb, (int64_t)device_sm_count(op->device) * per_sm);
   K.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
-  K.var[0] = {true, eb, K.grid, K.smem, 0.0f};
+  K.var[0] = {true, eb, K.grid, K.smem, 0.0f, kKronNDThreads};
   // grouped variants: elements per CTA so that the blocks of the largest group give every
   // thread about one block, within ~110 KB of shared memory (two CTAs per SM)
   const bool paired = pairs_share_factors(plan, s);
   // the mass-only variant (4): operators without advection terms, its own smaller layout
   for (int v = 1; v < kKronNDVariants; ++v) {
     const bool mass_only = v == 4;
-    const int G = (v == 3 || mass_only) ? 2 : v + 1;  // the paired variant's blocks span two axes
+    const int G = mass_only ? entry->mass_g : (v == 3 ? 2 : v + 1);  // paired blocks span two axes
     const void* fn = mass_only ? entry->func_m : entry->func_g[v - 1];
     if (!fn || (v == 3 && !paired) || (mass_only && (plan.has_adv || !plan.has_mass))) continue;
     // the mass-only kernel holds two batches (the next one's input arrives during this one's passes)
@@ -904,7 +904,10 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     int64_t gsz = 1;
     for (int k = 0; k < std::min(G, D); ++k) gsz *= N;
     const int64_t ipe = (s.ndofs / s.nelem) / gsz;  // blocks per element
-    int ebv = (int)std::max<int64_t>(1, std::min<int64_t>(64, (kKronNDThreads + ipe / 2) / ipe));
+    // the mass-only kernel: 128 threads, whole blocks of 3 axes for every thread
+    const int threads = mass_only ? 128 : kKronNDThreads;
+    int ebv = mass_only ? (int)std::max<int64_t>(1, std::min<int64_t>(64, threads / ipe))
+                        : (int)std::max<int64_t>(1, std::min<int64_t>(64, (kKronNDThreads + ipe / 2) / ipe));
     while (ebv > 1 && pv * ebv + extra > std::min<size_t>((size_t)max_smem, 110 * 1024)) --ebv;
     if (pv * ebv + extra > (size_t)max_smem) continue;
     cudaFuncAttributes fv{};
@@ -918,10 +921,10 @@ int setup_kronnd(dgop_operator* op, KronNDCfg<Real>& K, const KronPlanHost& plan
     if (pv * ebv + extra > (size_t)max_v) continue;
     DGOP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_v));
     int per_sm_v = 0;
-    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, fn, kKronNDThreads, pv * ebv + extra));
+    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, fn, threads, pv * ebv + extra));
     if (per_sm_v < 1) continue;
     const int64_t cv = std::min<int64_t>((s.nelem + ebv - 1) / ebv, (int64_t)device_sm_count(op->device) * per_sm_v);
-    K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), pv * ebv + extra, 0.0f};
+    K.var[v] = {true, ebv, dim3((unsigned)std::max<int64_t>(cv, 1)), pv * ebv + extra, 0.0f, threads};
   }
   K.variant = 0;
   if constexpr (sizeof(Real) == 4) {
@@ -963,7 +966,7 @@ void launch_kronnd_variant(const KronNDCfg<Real>& K, int v, KronNDParams<Real> p
   const auto& L = K.var[v];
   p.eb = L.eb;
   if (v == 0) K.entry->launch(p, L.grid, K.block, L.smem, st);
-  else if (v == 4) K.entry->launch_m(p, L.grid, K.block, L.smem, st);
+  else if (v == 4) K.entry->launch_m(p, L.grid, dim3(L.threads), L.smem, st);
   else K.entry->launch_g[v - 1](p, L.grid, K.block, L.smem, st);
 }
 

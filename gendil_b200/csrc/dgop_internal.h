@@ -87,6 +87,7 @@ struct KronNDCfg {
     dim3 grid;
     size_t smem = 0;
     float ms = 0.0f;  // autotuner's time per launch (0: not timed)
+    int threads = kKronNDThreads;
   } var[kKronNDVariants];
   int variant = 0;
   // BF16 tensor-core launch (FP32 configuration only) and its Kronecker tile tables

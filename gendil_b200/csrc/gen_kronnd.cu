@@ -37,9 +37,15 @@ void launch_kronnd_batch(const KronNDParams<Real>* table, const int64_t* first, 
   kronnd_batch_kernel<D, N, V, Real><<<grid, block, smem, s>>>(table, first, count, eb);
 }
 
+// blocks of 3 axes for the mass-only kernel while they stay 27 values, else 2
+template <int N>
+constexpr int mass_groups() {
+  return N * N * N <= 27 ? 3 : 2;
+}
+
 template <int D, int N, typename Real>
 void launch_kronnd_mass(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
-  kronnd_mass_kernel<D, N, 2, Real><<<grid, block, smem, s>>>(p);
+  kronnd_mass_kernel<D, N, mass_groups<N>(), Real><<<grid, block, smem, s>>>(p);
 }
 
 template <int D, int N, typename Real>
@@ -76,8 +82,9 @@ void fill(KronNDEntry<Real>& d) {
       d.launch_g[0] = &launch_kronnd_grouped<D, N, 2, Real>;
       d.func_g[0] = reinterpret_cast<const void*>(&kronnd_grouped_kernel<D, N, 2, Real>);
       d.launch_m = &launch_kronnd_mass<D, N, Real>;
-      d.func_m = reinterpret_cast<const void*>(&kronnd_mass_kernel<D, N, 2, Real>);
+      d.func_m = reinterpret_cast<const void*>(&kronnd_mass_kernel<D, N, mass_groups<N>(), Real>);
       d.per_elem_m = KronNDMassShape<D, N>::PER_ELEM;
+      d.mass_g = mass_groups<N>();
       if constexpr (sizeof(Real) == 8) {
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);

@@ -72,6 +72,7 @@ struct KronNDEntry {
   void (*launch_m)(const KronNDParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_m = nullptr;
   int per_elem_m = 0;
+  int mass_g = 2;  // axes per block of the mass-only kernel (3 when N^3 <= 27)
   // BF16 tensor-core variant (kronnd_tc_kernel.cuh; FP32 parameters, even D, N^(D/2) <= 32)
   void (*launch_tc)(const KronNDParams<float>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) = nullptr;
   const void* func_tc = nullptr;
