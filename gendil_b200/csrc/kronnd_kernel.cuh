@@ -718,10 +718,11 @@ __global__ void __launch_bounds__(kKronNDThreads, 3)
 // Mass-only variant (operators without advection terms: the mass operator, the mass inverse):
 // the element's values are passed in place in ONE shared-memory array, next to the D mass
 // matrices, so an element needs about a third of the layout above (6.4 instead of 21.7 KB at 6D
-// p = 2 in FP64) and the SM keeps more elements resident.  The passes are the grouped kernel's
-// steps of the mass term in the same order (the last axis first, scaled by the element factor,
-// then the groups in increasing order); blocks of one step are disjoint, so each thread writes
-// its block back where it read it.
+// p = 2 in FP64) and the SM keeps more elements resident.  The passes run group by group from
+// axis 0 (scaled by the element factor) up; blocks of one step are disjoint, so each thread
+// writes its block back where it read it, and the last step writes its block straight to y
+// (its values lie INNER = N^(first axis of the group) apart, so consecutive threads write
+// consecutive addresses).
 // ------------------------------------------------------------------------------------------
 template <int D, int N>
 struct KronNDMassShape {
@@ -736,11 +737,11 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
   using S = KronNDShape<D, N>;
   using M = KronNDMassShape<D, N>;
   using GR = KronGroups<D, N, G>;
-  constexpr int AX = D - 1;
+  constexpr int AX = 0;
   constexpr int g = GR::group(AX, ST);
   constexpr int LO = GR::lo(g), HI = GR::hi(g), GSZ = GR::size(g), INNER = GR::inner(g);
   constexpr int IPE = S::ND / GSZ;  // blocks per element
-  constexpr bool FIRST = ST == 0;
+  constexpr bool FIRST = ST == 0, LAST = ST == GR::NG - 1;
   const int total = ne * IPE;
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     const int b = it / IPE;
@@ -781,8 +782,15 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
         for (int j = 0; j < N; ++j) v[p0 + j * SK] = w[j];
       }
     });
+    if constexpr (LAST) {
+      Real* dst = P.y + (e0 + b) * S::ND + off;
 #pragma unroll
-    for (int j = 0; j < GSZ; ++j) el[off + j * INNER] = v[j];
+      for (int j = 0; j < GSZ; ++j)
+        dst[j * INNER] = (P.beta_y == Real(0)) ? P.alpha * v[j] : P.alpha * v[j] + P.beta_y * dst[j * INNER];
+    } else {
+#pragma unroll
+      for (int j = 0; j < GSZ; ++j) el[off + j * INNER] = v[j];
+    }
   }
 }
 
@@ -863,16 +871,11 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __gri
       }
       __syncthreads();
     }
+    // the last step writes y; the barrier after it (or the next batch's first one) frees `cur`
     static_for<0, GR::NG>([&](auto sc) {
       nd_mass_step<D, N, G, decltype(sc)::value>(P, cur, ne, e0, cm);
-      __syncthreads();
+      if constexpr (decltype(sc)::value + 1 < GR::NG) __syncthreads();
     });
-    for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-      const int b = l / S::ND, i = l - b * S::ND;
-      const Real v = cur[(size_t)b * M::PER_ELEM + i];
-      Real* dst = P.y + e0 * S::ND + l;
-      *dst = (P.beta_y == Real(0)) ? P.alpha * v : P.alpha * v + P.beta_y * *dst;
-    }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy outlives the kernel
 }
