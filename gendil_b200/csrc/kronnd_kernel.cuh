@@ -724,10 +724,25 @@ __global__ void __launch_bounds__(kKronNDThreads, 3)
 // (its values lie INNER = N^(first axis of the group) apart, so consecutive threads write
 // consecutive addresses).
 // ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Values of Real by which an element's first value lies past a 16-byte boundary in global memory;
+// the element's slot in shared memory starts that many values into its (16-byte aligned) area, so
+// the two copies have the same 16-byte phase and whole chunks move by 16-byte copies.
+template <typename Real>
+__device__ __forceinline__ int nd_phase(const Real* p) {
+  return (int)((reinterpret_cast<uintptr_t>(p) / sizeof(Real)) & (16 / sizeof(Real) - 1));
+}
+
 template <int D, int N>
 struct KronNDMassShape {
   using S = KronNDShape<D, N>;
-  static constexpr int MOFF = (S::ND + 3) / 4 * 4;  // the D mass matrices (16-byte aligned)
+  // the element's values (starting up to 3 values in, see nd_phase), then the D mass matrices
+  // (16-byte aligned)
+  static constexpr int MOFF = (S::ND + 6) / 4 * 4;
   static constexpr int PER_ELEM = MOFF + D * S::MATP;
 };
 
@@ -749,9 +764,10 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
     const int o = loc / INNER, t = loc - o * INNER;
     const int off = o * GSZ * INNER + t;
     Real* el = base + (size_t)b * M::PER_ELEM;
+    Real* u = el + nd_phase(P.x + (e0 + b) * S::ND);  // the element's values (see nd_phase)
     Real v[GSZ];
 #pragma unroll
-    for (int j = 0; j < GSZ; ++j) v[j] = el[off + j * INNER];
+    for (int j = 0; j < GSZ; ++j) v[j] = u[off + j * INNER];
     static_for<0, HI - LO>([&](auto kc) {
       constexpr int k = GR::axis(g, decltype(kc)::value, FIRST, AX);
       constexpr int SK = kpow(N, k - LO);
@@ -789,7 +805,7 @@ __device__ __forceinline__ void nd_mass_step(const KronNDParams<Real>& P, Real* 
         dst[j * INNER] = (P.beta_y == Real(0)) ? P.alpha * v[j] : P.alpha * v[j] + P.beta_y * dst[j * INNER];
     } else {
 #pragma unroll
-      for (int j = 0; j < GSZ; ++j) el[off + j * INNER] = v[j];
+      for (int j = 0; j < GSZ; ++j) u[off + j * INNER] = v[j];
     }
   }
 }
@@ -821,13 +837,28 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __gri
   const int EB = P.eb;
   const int64_t stride = (int64_t)gridDim.x * EB;
   // input of the batch starting at e0 into buffer buf (one commit group, possibly empty)
+  // element b's values occupy [a, a + ND) of its area (a = nd_phase); the area's 16-byte chunks
+  // inside that range are whole 16-byte copies, the two partial ones value by value
+  constexpr int R = 16 / (int)sizeof(Real);
+  constexpr int NC = (S::ND + 2 * (R - 1)) / R + 1;  // chunks per element area, at most
+  static_assert(M::MOFF >= S::ND + R - 1, "the values and their phase fit before the matrices");
   auto stage = [&](int64_t e0, int buf) {
     if (e0 < P.nelem) {
       const int ne = (int)((P.nelem - e0) < EB ? (P.nelem - e0) : EB);
       Real* dst = base + (size_t)buf * EB * M::PER_ELEM;
-      for (int l = threadIdx.x; l < ne * S::ND; l += blockDim.x) {
-        const int b = l / S::ND, i = l - b * S::ND;
-        cp_async_value(dst + (size_t)b * M::PER_ELEM + i, P.x + e0 * S::ND + l);
+      for (int l = threadIdx.x; l < ne * NC; l += blockDim.x) {
+        const int b = l / NC, k = l - b * NC;
+        const Real* src = P.x + (e0 + b) * S::ND;  // the element's first value
+        const int a = nd_phase(src);
+        const int lo = k * R, hi = lo + R;  // the chunk, in values of the area
+        if (hi <= a || lo >= a + S::ND) continue;
+        Real* d = dst + (size_t)b * M::PER_ELEM;
+        if (lo >= a && hi <= a + S::ND) {
+          cp_async_16(d + lo, src + (lo - a));
+        } else {
+          for (int i = lo; i < hi; ++i)
+            if (i >= a && i < a + S::ND) cp_async_value(d + i, src + (i - a));
+        }
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
