@@ -215,11 +215,22 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
   }
 }
 
+// How the last step of a term writes its block into the accumulator Y: bit 0 set, the term is the
+// first to reach Y and stores (Y is not zeroed beforehand); bit 1 set, the term is the last and
+// writes y = alpha (Y + block) + beta y to global memory instead of Y (no separate output pass).
+enum : int { kYAdd = 0, kYStore = 1, kYOut = 2 };
+template <typename Real>
+__device__ __forceinline__ void nd_y_write(const KronNDParams<Real>& P, int ymode, Real* yl, Real* yg, Real v) {
+  const Real t = (ymode & kYStore) ? v : *yl + v;
+  if (ymode & kYOut) *yg = (P.beta_y == Real(0)) ? P.alpha * t : P.alpha * t + P.beta_y * *yg;
+  else *yl = t;
+}
+
 // Shared-memory setup of one batch of ne elements starting at e0: U (the input), Y = 0, the
 // element coordinates, every element's slot matrices and face records.
 template <int D, int N, typename Real>
 __device__ __forceinline__ void nd_setup(const KronNDParams<Real>& P, const Real* __restrict__ xin, int64_t e0, int ne,
-                                         Real* base, int (*ecoord)[kMaxDim]) {
+                                         Real* base, int (*ecoord)[kMaxDim], bool zero_y = true) {
   using S = KronNDShape<D, N>;
   const bool adv = P.has_adv != 0;
   __syncthreads();
@@ -228,7 +239,7 @@ __device__ __forceinline__ void nd_setup(const KronNDParams<Real>& P, const Real
     const int b = l / S::ND, i = l - b * S::ND;
     Real* el = base + (size_t)b * S::PER_ELEM;
     el[i] = xin[e0 * S::ND + l];
-    el[2 * S::ND + i] = Real(0);
+    if (zero_y) el[2 * S::ND + i] = Real(0);
   }
   if (threadIdx.x < ne) {
     const int64_t e = e0 + threadIdx.x;
@@ -380,7 +391,8 @@ struct KronGroups {
 // of its group, for the ne elements of the batch.
 template <int D, int N, int G, int TERM, int ST, typename Real>
 __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const Real* __restrict__ xin, Real* base,
-                                              int ne, int64_t e0, const int (*ecoord)[kMaxDim]) {
+                                              int ne, int64_t e0, const int (*ecoord)[kMaxDim], int ymode = kYAdd,
+                                              Real* __restrict__ yout = nullptr) {
   using S = KronNDShape<D, N>;
   using GR = KronGroups<D, N, G>;
   constexpr bool MASS = TERM == D;
@@ -458,7 +470,7 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
     Real* dst = el + (LAST ? 2 : 1) * S::ND;
 #pragma unroll
     for (int j = 0; j < GSZ; ++j) {
-      if constexpr (LAST) dst[off + j * INNER] += v[j];
+      if constexpr (LAST) nd_y_write(P, ymode, dst + off + j * INNER, yout + (e0 + b) * S::ND + off + j * INNER, v[j]);
       else dst[off + j * INNER] = v[j];
     }
   }
@@ -470,23 +482,27 @@ __device__ __forceinline__ void kronnd_grouped_block(const KronNDParams<Real>& P
                                                      Real* __restrict__ yout, int64_t e0, int ne, Real* base,
                                                      int (*ecoord)[kMaxDim]) {
   using GR = KronGroups<D, N, G>;
-  nd_setup<D, N>(P, xin, e0, ne, base, ecoord);
+  // the first term to reach Y stores its block, the last writes y (nd_y_write): no zeroing of Y
+  // and no output pass
+  const bool sep_mass = P.has_mass && !(P.has_adv && P.mass_merged);
+  nd_setup<D, N>(P, xin, e0, ne, base, ecoord, false);
   if (P.has_adv) {
     static_for<0, D>([&](auto ac) {
       constexpr int a = decltype(ac)::value;
+      const int ymode = (a == 0 ? kYStore : kYAdd) | ((a == D - 1 && !sep_mass) ? kYOut : kYAdd);
       static_for<0, GR::NG>([&](auto sc) {
-        nd_group_step<D, N, G, a, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+        nd_group_step<D, N, G, a, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
         __syncthreads();
       });
     });
   }
-  if (P.has_mass && !(P.has_adv && P.mass_merged)) {
+  if (sep_mass) {
+    const int ymode = (P.has_adv ? kYAdd : kYStore) | kYOut;
     static_for<0, GR::NG>([&](auto sc) {
-      nd_group_step<D, N, G, D, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+      nd_group_step<D, N, G, D, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
       __syncthreads();
     });
   }
-  nd_output<D, N>(P, yout, e0, ne, base);
 }
 
 template <int D, int N, int G, typename Real>
@@ -517,7 +533,8 @@ __global__ void __launch_bounds__(kKronNDThreads)
 // ------------------------------------------------------------------------------------------
 template <int D, int N, int PG, int ST, typename Real>
 __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const Real* __restrict__ xin, Real* base,
-                                             int ne, int64_t e0, const int (*ecoord)[kMaxDim]) {
+                                             int ne, int64_t e0, const int (*ecoord)[kMaxDim], int ymode = kYAdd,
+                                             Real* __restrict__ yout = nullptr) {
   using S = KronNDShape<D, N>;
   constexpr int H = D / 2;
   constexpr int g = ST == 0 ? PG : (ST - 1 < PG ? ST - 1 : ST);  // the pair this step runs on
@@ -673,8 +690,9 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
     for (int i = 0; i < N; ++i)
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        if constexpr (LAST) dst[off + i * SA + j * SB] += acc[i][j];
-        else dst[off + i * SA + j * SB] = acc[i][j];
+        const int q = off + i * SA + j * SB;
+        if constexpr (LAST) nd_y_write(P, ymode, dst + q, yout + (e0 + b) * S::ND + q, acc[i][j]);
+        else dst[q] = acc[i][j];
       }
   }
 }
@@ -685,19 +703,19 @@ __device__ __forceinline__ void kronnd_paired_block(const KronNDParams<Real>& P,
                                                     Real* __restrict__ yout, int64_t e0, int ne, Real* base,
                                                     int (*ecoord)[kMaxDim]) {
   constexpr int H = D / 2;
-  nd_setup<D, N>(P, xin, e0, ne, base, ecoord);
+  nd_setup<D, N>(P, xin, e0, ne, base, ecoord, false);
   static_for<0, H>([&](auto pc) {
     constexpr int PG = decltype(pc)::value;
     // a pair runs when it has advection terms, or the mass term alone (operators without
-    // advection: the last pair carries it)
+    // advection: the last pair carries it); the first pair to reach Y stores, the last writes y
     if (P.has_adv || (PG == H - 1 && P.has_mass)) {
+      const int ymode = ((PG == 0 || !P.has_adv) ? kYStore : kYAdd) | (PG == H - 1 ? kYOut : kYAdd);
       static_for<0, H>([&](auto sc) {
-        nd_pair_step<D, N, PG, decltype(sc)::value>(P, xin, base, ne, e0, ecoord);
+        nd_pair_step<D, N, PG, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
         __syncthreads();
       });
     }
   });
-  nd_output<D, N>(P, yout, e0, ne, base);
 }
 
 template <int D, int N, typename Real>
