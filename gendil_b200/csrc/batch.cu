@@ -59,11 +59,37 @@ void release(dgop_batch* b) {
 }
 
 int setup(dgop_batch* b) {
+  int sms = 0, dev = 0;
+  DGOP_CUDA_B(cudaGetDevice(&dev));
+  DGOP_CUDA_B(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int max_smem = 0;
+  DGOP_CUDA_B(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  std::map<const void*, int> per_sm_of;  // resident CTAs per SM of each batch kernel used
   std::map<std::tuple<int, int, int>, int> index;
   for (int i = 0; i < (int)b->ops.size(); ++i) {
     dgop_operator* op = b->ops[i];
     const int v = op->n64.variant;
     if (op->kernel != DGOP_KERNEL_KRONND || !op->n64.ready || !op->n64.entry->launch_batch[v]) {
+      b->singles.push_back(i);
+      continue;
+    }
+    const void* fn = op->n64.entry->func_batch[v];
+    auto pit = per_sm_of.find(fn);
+    if (pit == per_sm_of.end()) {
+      cudaFuncAttributes fa{};
+      DGOP_CUDA_B(cudaFuncGetAttributes(&fa, fn));
+      DGOP_CUDA_B(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       max_smem - (int)fa.sharedSizeBytes));
+      int per_sm = 0;
+      DGOP_CUDA_B(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)op->n64.block.x,
+                                                                op->n64.var[v].smem));
+      pit = per_sm_of.emplace(fn, per_sm < 1 ? 1 : per_sm).first;
+    }
+    // an instance whose element batches fill every CTA slot twice over keeps its own launch (its
+    // parameters in constant memory, no per-batch instance lookup): the persistent kernel gains
+    // nothing there and measured a few per cent slower
+    const int64_t eb = op->n64.var[v].eb;
+    if ((op->sp.nelem + eb - 1) / eb >= 2 * (int64_t)sms * pit->second) {
       b->singles.push_back(i);
       continue;
     }
@@ -80,11 +106,6 @@ int setup(dgop_batch* b) {
     }
     b->groups[it->second].members.push_back(i);
   }
-  int sms = 0, dev = 0;
-  DGOP_CUDA_B(cudaGetDevice(&dev));
-  DGOP_CUDA_B(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  int max_smem = 0;
-  DGOP_CUDA_B(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   for (auto& g : b->groups) {
     g.first.push_back(0);
     for (int i : g.members) {
@@ -105,14 +126,7 @@ int setup(dgop_batch* b) {
     DGOP_CUDA_B(cudaMallocHost(&g.h_pinned, tb));
     DGOP_CUDA_B(cudaMalloc(&g.d_first, sizeof(int64_t) * g.first.size()));
     DGOP_CUDA_B(cudaMemcpy(g.d_first, g.first.data(), sizeof(int64_t) * g.first.size(), cudaMemcpyHostToDevice));
-    cudaFuncAttributes fa{};
-    const void* fn = g.entry->func_batch[g.variant];
-    DGOP_CUDA_B(cudaFuncGetAttributes(&fa, fn));
-    DGOP_CUDA_B(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     max_smem - (int)fa.sharedSizeBytes));
-    int per_sm = 0;
-    DGOP_CUDA_B(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)g.block.x, g.smem));
-    if (per_sm < 1) per_sm = 1;
+    const int per_sm = per_sm_of[g.entry->func_batch[g.variant]];
     g.grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(g.first.back(), (int64_t)sms * per_sm)));
   }
   DGOP_CUDA_B(cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming));

@@ -219,10 +219,12 @@ __device__ __forceinline__ void nd_faces(const KronNDParams<Real>& P, Real* base
 // first to reach Y and stores (Y is not zeroed beforehand); bit 1 set, the term is the last and
 // writes y = alpha (Y + block) + beta y to global memory instead of Y (no separate output pass).
 enum : int { kYAdd = 0, kYStore = 1, kYOut = 2 };
+// alpha and beta_y come in registers: the persistent batch kernel reads its parameters from a
+// global table, which the compiler would load again after every store to y.
 template <typename Real>
-__device__ __forceinline__ void nd_y_write(const KronNDParams<Real>& P, int ymode, Real* yl, Real* yg, Real v) {
+__device__ __forceinline__ void nd_y_write(Real alpha, Real beta_y, int ymode, Real* yl, Real* yg, Real v) {
   const Real t = (ymode & kYStore) ? v : *yl + v;
-  if (ymode & kYOut) *yg = (P.beta_y == Real(0)) ? P.alpha * t : P.alpha * t + P.beta_y * *yg;
+  if (ymode & kYOut) *yg = (beta_y == Real(0)) ? alpha * t : alpha * t + beta_y * *yg;
   else *yl = t;
 }
 
@@ -387,7 +389,7 @@ struct KronGroups {
   }
 };
 
-// Step ST of term TERM (TERM == D: the separate mass term, first pass along D - 1) over the blocks
+// Step ST of term TERM (TERM == D: the separate mass term, first pass along axis 0) over the blocks
 // of its group, for the ne elements of the batch.
 template <int D, int N, int G, int TERM, int ST, typename Real>
 __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const Real* __restrict__ xin, Real* base,
@@ -396,11 +398,12 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
   using S = KronNDShape<D, N>;
   using GR = KronGroups<D, N, G>;
   constexpr bool MASS = TERM == D;
-  constexpr int AX = MASS ? D - 1 : TERM;
+  constexpr int AX = MASS ? 0 : TERM;
   constexpr int g = GR::group(AX, ST);
   constexpr int LO = GR::lo(g), HI = GR::hi(g), GSZ = GR::size(g), INNER = GR::inner(g);
   constexpr int IPE = S::ND / GSZ;  // blocks per element
   constexpr bool FIRST = ST == 0, LAST = ST == GR::NG - 1;
+  const Real alpha = P.alpha, beta_y = P.beta_y;
   const int total = ne * IPE;
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     const int b = it / IPE;
@@ -470,7 +473,8 @@ __device__ __forceinline__ void nd_group_step(const KronNDParams<Real>& P, const
     Real* dst = el + (LAST ? 2 : 1) * S::ND;
 #pragma unroll
     for (int j = 0; j < GSZ; ++j) {
-      if constexpr (LAST) nd_y_write(P, ymode, dst + off + j * INNER, yout + (e0 + b) * S::ND + off + j * INNER, v[j]);
+      if constexpr (LAST)
+        nd_y_write(alpha, beta_y, ymode, dst + off + j * INNER, yout + (e0 + b) * S::ND + off + j * INNER, v[j]);
       else dst[off + j * INNER] = v[j];
     }
   }
@@ -482,14 +486,18 @@ __device__ __forceinline__ void kronnd_grouped_block(const KronNDParams<Real>& P
                                                      Real* __restrict__ yout, int64_t e0, int ne, Real* base,
                                                      int (*ecoord)[kMaxDim]) {
   using GR = KronGroups<D, N, G>;
-  // the first term to reach Y stores its block, the last writes y (nd_y_write): no zeroing of Y
-  // and no output pass
+  // The terms run from D - 1 down to 0, then the separate mass term: the first to reach Y stores
+  // its block (Y is not zeroed).  The last term (0, or the mass term; both start along axis 0)
+  // ends on the highest group, whose blocks put INNER consecutive threads on consecutive values:
+  // when that run is a 32-byte sector or more it writes y itself (nd_y_write), otherwise it
+  // accumulates into Y and the coalesced output pass writes y.
+  constexpr bool YOUT = GR::NG >= 2 && GR::inner(GR::NG - 1) * sizeof(Real) >= 32;
   const bool sep_mass = P.has_mass && !(P.has_adv && P.mass_merged);
   nd_setup<D, N>(P, xin, e0, ne, base, ecoord, false);
   if (P.has_adv) {
     static_for<0, D>([&](auto ac) {
-      constexpr int a = decltype(ac)::value;
-      const int ymode = (a == 0 ? kYStore : kYAdd) | ((a == D - 1 && !sep_mass) ? kYOut : kYAdd);
+      constexpr int a = D - 1 - decltype(ac)::value;
+      const int ymode = (a == D - 1 ? kYStore : kYAdd) | ((YOUT && a == 0 && !sep_mass) ? kYOut : kYAdd);
       static_for<0, GR::NG>([&](auto sc) {
         nd_group_step<D, N, G, a, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
         __syncthreads();
@@ -497,12 +505,13 @@ __device__ __forceinline__ void kronnd_grouped_block(const KronNDParams<Real>& P
     });
   }
   if (sep_mass) {
-    const int ymode = (P.has_adv ? kYAdd : kYStore) | kYOut;
+    const int ymode = (P.has_adv ? kYAdd : kYStore) | (YOUT ? kYOut : kYAdd);
     static_for<0, GR::NG>([&](auto sc) {
       nd_group_step<D, N, G, D, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
       __syncthreads();
     });
   }
+  if constexpr (!YOUT) nd_output<D, N>(P, yout, e0, ne, base);
 }
 
 template <int D, int N, int G, typename Real>
@@ -542,8 +551,10 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
   constexpr int SA = kpow(N, A), SB = kpow(N, B);
   constexpr int IPE = S::ND / (N * N);  // blocks per element
   constexpr bool OWN = ST == 0, LAST = ST == H - 1;
-  constexpr bool WITH_MASS = PG == H - 1;  // the separate mass term runs with the last pair
+  constexpr bool WITH_MASS = PG == H - 1;  // the separate mass term runs with pair H - 1
   const bool mass = WITH_MASS && P.has_mass && !(P.has_adv && P.mass_merged);
+  const Real alpha = P.alpha, beta_y = P.beta_y;
+  const int t0 = P.has_adv ? PG : D;  // factors of the other pairs' steps (the mass term alone: its own)
   const int total = ne * IPE;
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     const int b = it / IPE;
@@ -662,7 +673,6 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
       }
     } else {
       // the pair's shared factors along A and B (term PG's; equal to term PG + H's)
-      const int t0 = P.has_adv ? PG : D;  // the mass term alone: its own factors
       const SlotMat<N, Real> fa(mats + (t0 < D ? t0 * D + A : D * D + A) * S::MATP);
       const SlotMat<N, Real> fbm(mats + (t0 < D ? t0 * D + B : D * D + B) * S::MATP);
       Real w[N][N];
@@ -691,7 +701,7 @@ __device__ __forceinline__ void nd_pair_step(const KronNDParams<Real>& P, const 
 #pragma unroll
       for (int j = 0; j < N; ++j) {
         const int q = off + i * SA + j * SB;
-        if constexpr (LAST) nd_y_write(P, ymode, dst + q, yout + (e0 + b) * S::ND + q, acc[i][j]);
+        if constexpr (LAST) nd_y_write(alpha, beta_y, ymode, dst + q, yout + (e0 + b) * S::ND + q, acc[i][j]);
         else dst[q] = acc[i][j];
       }
   }
@@ -703,19 +713,31 @@ __device__ __forceinline__ void kronnd_paired_block(const KronNDParams<Real>& P,
                                                     Real* __restrict__ yout, int64_t e0, int ne, Real* base,
                                                     int (*ecoord)[kMaxDim]) {
   constexpr int H = D / 2;
+  // The pairs run from H - 1 down to 0: pair H - 1 (with the mass term) reaches Y first and stores
+  // its blocks (Y is not zeroed).  The last step of pair PG runs on pair glast(PG), whose blocks
+  // put N^glast consecutive threads on consecutive values (the axes below the pair): when that run
+  // is a 32-byte sector or more the last pair writes y itself (nd_y_write), otherwise it
+  // accumulates into Y and the coalesced output pass writes y.
+  constexpr int GLAST_ADV = H == 1 ? 0 : H - 1;   // glast(0): pair 0 runs last
+  constexpr int GLAST_MASS = H == 1 ? 0 : H - 2;  // glast(H - 1): the mass term alone
+  constexpr bool YOUT_ADV = kpow(N, GLAST_ADV) * sizeof(Real) >= 32;
+  constexpr bool YOUT_MASS = kpow(N, GLAST_MASS) * sizeof(Real) >= 32;
+  const bool yout_ok = P.has_adv ? YOUT_ADV : YOUT_MASS;
   nd_setup<D, N>(P, xin, e0, ne, base, ecoord, false);
   static_for<0, H>([&](auto pc) {
-    constexpr int PG = decltype(pc)::value;
+    constexpr int PG = H - 1 - decltype(pc)::value;
     // a pair runs when it has advection terms, or the mass term alone (operators without
-    // advection: the last pair carries it); the first pair to reach Y stores, the last writes y
+    // advection: the last pair carries it)
     if (P.has_adv || (PG == H - 1 && P.has_mass)) {
-      const int ymode = ((PG == 0 || !P.has_adv) ? kYStore : kYAdd) | (PG == H - 1 ? kYOut : kYAdd);
+      const bool last = PG == 0 || !P.has_adv;
+      const int ymode = (PG == H - 1 ? kYStore : kYAdd) | ((last && yout_ok) ? kYOut : kYAdd);
       static_for<0, H>([&](auto sc) {
         nd_pair_step<D, N, PG, decltype(sc)::value>(P, xin, base, ne, e0, ecoord, ymode, yout);
         __syncthreads();
       });
     }
   });
+  if (!yout_ok) nd_output<D, N>(P, yout, e0, ne, base);
 }
 
 template <int D, int N, typename Real>
@@ -932,9 +954,12 @@ __global__ void __launch_bounds__(kKronNDThreads) kronnd_mass_kernel(const __gri
 // Many operators of one (D, N) and kernel variant V (0: one pass per axis, 1 / 2: groups of 2 / 3
 // axes, 3: paired axes) in one persistent launch: table[i] holds instance i's parameters (forward operator, x / y
 // set per apply), its element batches are the global batch indices [first[i], first[i + 1]);
-// every CTA walks the global batches.
+// every CTA walks the global batches.  Register caps keep the occupancy of the single-operator
+// kernels (per-axis: 4 CTAs per SM, at most 64 registers; grouped: 2, at most 128): the
+// parameters read from the table, rather than from constant memory, would otherwise take the
+// register count past them.
 template <int D, int N, int V, typename Real>
-__global__ void __launch_bounds__(kKronNDThreads)
+__global__ void __launch_bounds__(kKronNDThreads, V == 0 ? 4 : ((V == 1 || V == 2) ? 2 : 1))
     kronnd_batch_kernel(const KronNDParams<Real>* __restrict__ table, const int64_t* __restrict__ first, int count,
                         int EB) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -44,6 +44,35 @@ def test_batch_apply_equals_individual_applies():
     batch.close()
 
 
+def test_batch_large_instance_keeps_its_own_launch():
+    """An instance whose element batches fill every CTA slot of the GPU twice over (here 10^6
+    elements) is applied by its own launch, outside the groups; the small instances of the same
+    (dimension, order) still form a group, and every result is bit-identical to its own apply."""
+    rng = np.random.default_rng(11)
+    specs = [(2, [1000, 1000], 1), (2, [9, 7], 1), (2, [5, 11], 1)]
+    ops = []
+    for D, n, p in specs:
+        beta = C.velocity_constant(list(rng.uniform(-1, 1, D)))
+        ops.append(g.SystemOperator(_space(D, n, p), p + 2, beta, sigma=1e3, bc=g.BC_INFLOW, g=0.0))
+    for o in ops[1:]:
+        o.set_variant(ops[0].variant)  # one (dimension, order, variant) key for all three
+    assert all(o.kernel == "kronnd" for o in ops)
+    xs = [torch.rand(o.space.num_dofs, dtype=torch.float64, device="cuda") - 0.5 for o in ops]
+    want = []
+    for o, x in zip(ops, xs):
+        y = torch.empty_like(x)
+        o(x, y)
+        want.append(y)
+    batch = g.Batch(ops)
+    assert batch.groups == 1
+    ys = [torch.full_like(x, float("nan")) for x in xs]
+    batch.apply(xs, ys)
+    torch.cuda.synchronize()
+    for y, w in zip(ys, want):
+        assert torch.equal(y, w)
+    batch.close()
+
+
 def _systems(specs, seed=7):
     rng = np.random.default_rng(seed)
     ops, precs, bs = [], [], []
