@@ -77,15 +77,18 @@ void fill(KronNDEntry<Real>& d) {
     d.launch_batch[0] = &launch_kronnd_batch<D, N, 0, Real>;
     d.func_batch[0] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 0, Real>);
     d.per_elem = KronNDShape<D, N>::PER_ELEM;
-    // grouped variants while a block (N^G values) stays a register array
-    if constexpr (D >= 2 && N >= 2 && N * N <= 27) {
+    // grouped variants while a block (N^G values) stays a register array (blocks of 2 axes up to
+    // N = 6: the 2D p = 5 systems, among the slowest to solve, need them most)
+    if constexpr (D >= 2 && N >= 2 && N * N <= 36) {
       d.launch_g[0] = &launch_kronnd_grouped<D, N, 2, Real>;
       d.func_g[0] = reinterpret_cast<const void*>(&kronnd_grouped_kernel<D, N, 2, Real>);
       d.launch_m = &launch_kronnd_mass<D, N, Real>;
       d.func_m = reinterpret_cast<const void*>(&kronnd_mass_kernel<D, N, mass_groups<N>(), Real>);
       d.per_elem_m = KronNDMassShape<D, N>::PER_ELEM;
       d.mass_g = mass_groups<N>();
-      if constexpr (sizeof(Real) == 8) {
+      if constexpr (sizeof(Real) == 8 && N * N <= 27) {
+        // (36-value blocks stay single-operator launches: the persistent batch kernel at that
+        // register count measured slower than one launch per operator)
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);
       }
