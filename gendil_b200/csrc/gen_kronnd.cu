@@ -87,8 +87,8 @@ void fill(KronNDEntry<Real>& d) {
       d.per_elem_m = KronNDMassShape<D, N>::PER_ELEM;
       d.mass_g = mass_groups<N>();
       if constexpr (sizeof(Real) == 8 && N * N <= 27) {
-        // (36-value blocks stay single-operator launches: the persistent batch kernel at that
-        // register count measured slower than one launch per operator)
+        // (36-value blocks stay single-operator launches: the persistent batch kernel needs about
+        // 170 FP64 registers for them, past the 128-register cap that keeps two CTAs per SM)
         d.launch_batch[1] = &launch_kronnd_batch<D, N, 1, Real>;
         d.func_batch[1] = reinterpret_cast<const void*>(&kronnd_batch_kernel<D, N, 1, Real>);
       }

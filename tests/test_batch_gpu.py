@@ -16,6 +16,17 @@ def _space(D, n, p, basis=g.GLL):
     return g.Space(D, sizes, [1.0 / s for s in sizes], [0.0] * D, None, p, basis)
 
 
+def _batched(o):
+    """Whether the persistent batch kernel serves this operator's variant: every any-dimension
+    variant but the mass-only one, with blocks of at most 27 values (N = order + 1; grouped by 2
+    axes up to N = 5, by 3 up to N = 3, paired up to N = 5)."""
+    if o.kernel != "kronnd":
+        return False
+    n = o.space.order + 1
+    return {"nd-passes": True, "nd-grouped2": n * n <= 27, "nd-grouped3": n ** 3 <= 27,
+            "nd-paired": n * n <= 27}.get(o.variant, False)
+
+
 def test_batch_apply_equals_individual_applies():
     rng = np.random.default_rng(7)
     ops = []
@@ -34,7 +45,7 @@ def test_batch_apply_equals_individual_applies():
         o(x, y)
         want.append(y)
     batch = g.Batch(ops)
-    assert batch.groups == len({(o.space.dim, o.space.order, o.variant) for o in ops if o.kernel == "kronnd"})
+    assert batch.groups == len({(o.space.dim, o.space.order, o.variant) for o in ops if _batched(o)})
     for _ in range(2):  # twice: the parameter upload of the previous apply is reused safely
         ys = [torch.full_like(x, float("nan")) for x in xs]
         batch.apply(xs, ys)
@@ -65,6 +76,33 @@ def test_batch_large_instance_keeps_its_own_launch():
         want.append(y)
     batch = g.Batch(ops)
     assert batch.groups == 1
+    ys = [torch.full_like(x, float("nan")) for x in xs]
+    batch.apply(xs, ys)
+    torch.cuda.synchronize()
+    for y, w in zip(ys, want):
+        assert torch.equal(y, w)
+    batch.close()
+
+
+def test_batch_unbatched_variant_runs_one_launch_each():
+    """Operators whose variant has no persistent batch kernel (2D p = 5 on 36-value blocks of 2
+    axes) form no group and are applied one launch each, bit-identical to their own applies."""
+    rng = np.random.default_rng(5)
+    ops = []
+    for n in ([7, 5], [6, 9]):
+        beta = C.velocity_constant(list(rng.uniform(-1, 1, 2)))
+        o = g.SystemOperator(_space(2, n, 5), 7, beta, sigma=1e3, bc=g.BC_INFLOW, g=0.0)
+        o.set_variant("nd-grouped2")
+        ops.append(o)
+    assert not any(_batched(o) for o in ops)
+    xs = [torch.rand(o.space.num_dofs, dtype=torch.float64, device="cuda") - 0.5 for o in ops]
+    want = []
+    for o, x in zip(ops, xs):
+        y = torch.empty_like(x)
+        o(x, y)
+        want.append(y)
+    batch = g.Batch(ops)
+    assert batch.groups == 0
     ys = [torch.full_like(x, float("nan")) for x in xs]
     batch.apply(xs, ys)
     torch.cuda.synchronize()
