@@ -298,6 +298,7 @@ def test_kronnd_variants(cid, case, kind, mode):
     register block; axes a and a + D/2 paired where the terms share their other factors) meets the
     parity bar against the reference's golden outputs, forward, transposed and FP32, and agrees
     with the per-axis variant to rounding."""
+    import torch
     import gendil_b200 as g
     op = make_operator(case, kind, mode)
     try:
@@ -317,6 +318,12 @@ def test_kronnd_variants(cid, case, kind, mode):
         tried += 1
         got = (cuda_apply(op, x), cuda_apply(op, x, transpose=True), cuda_apply(op, x, f32=True))
         assert rel_max(got[0], want) <= APPLY_TOL, name
+        # y = alpha A x + beta y (the last step of the grouped and paired variants writes y itself)
+        y0 = inputs(case, seed=9)
+        yb = torch.from_numpy(y0).cuda()
+        op.apply(torch.from_numpy(x).cuda(), yb, alpha=2.5, beta=-0.5)
+        ab = 2.5 * got[0] - 0.5 * y0
+        assert np.abs(yb.cpu().numpy() - ab).max() <= 1e-14 * max(np.abs(ab).max(), 1e-300), name
         if ref is None:
             ref = got
         else:
