@@ -225,16 +225,22 @@ __device__ __forceinline__ void tma_apply(const KronTmaParams<double>& T, uint32
 // phi_s(e_a) el_a(e) and the inflow term (forward: the same coefficient; transposed: the
 // neighbour's phi at its opposite face times its factor).  nbrow(s, src, d, v) fetches this lane's
 // row of the neighbour trace.
+// ph holds phi_0(e_a), phi_1(e_a): the caller loads it (one 16-byte load) before the D pass of
+// axis a, so the pass covers the load's latency.
+__device__ __forceinline__ double2 tma_phi(const KronParams<double>& P, int a, const uint32_t (&c)[3]) {
+  return __ldg(reinterpret_cast<const double2*>(P.phi[a] + c[a] * 2));
+}
+
 template <bool FIRST, typename NbRow>
 __device__ __forceinline__ void tma_faces(const KronParams<double>& P, int a, const uint32_t (&c)[3], int64_t e,
-                                          uint32_t ef, double el, const double (&U)[4][4], double (&Pm)[4][4],
-                                          NbRow nbrow) {
+                                          uint32_t ef, double el, double2 ph, const double (&U)[4][4],
+                                          double (&Pm)[4][4], NbRow nbrow) {
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
     const int sl = s ? 3 : 0;
     const uint32_t f = (ef >> (5 * (a * 2 + s))) & 31u;
     if (!(f & (kRecCorner | kRecNb | kRecG))) continue;
-    const double k_own = P.phi[a][c[a] * 2 + s] * el;
+    const double k_own = (s ? ph.y : ph.x) * el;
     if (f & kRecCorner) {
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -371,6 +377,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
       tma_plane_z(grp_sa, le, t, u);
       {
         double px[N][N];
+        const double2 phx = tma_phi(P, 0, c);
         tma_apply<kSlotDX, true, false>(T, c[0], mats, u, px);
         const double elx = P.elem[0] ? P.elem[0][e] : 1.0;
         if (P.elem[0]) {
@@ -379,7 +386,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
             for (int j = 0; j < N; ++j) px[i][j] *= elx;
         }
-        tma_faces<true>(P, 0, c, e, ef, elx, u, px, [&](int s, int src, int64_t d, double(&v)[N]) {
+        tma_faces<true>(P, 0, c, e, ef, elx, phx, u, px, [&](int s, int src, int64_t d, double(&v)[N]) {
           const int sl = s ? 0 : N - 1;  // the neighbour's opposite slice
           if (src == (int)kTmaSrcGroup) {
             const int r = 4 * (le + (s ? 1 : -1)) + t;
@@ -393,6 +400,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
         });
         tma_apply<kSlotTXY, false, false>(T, c[1], mats, px, qx);
       }
+      const double2 phy = tma_phi(P, 1, c);
       tma_apply<kSlotDY, false, false>(T, c[1], mats, u, py);
       const double ely = P.elem[1] ? P.elem[1][e] : 1.0;
       if (P.elem[1]) {
@@ -401,7 +409,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
           for (int j = 0; j < N; ++j) py[i][j] *= ely;
       }
-      tma_faces<false>(P, 1, c, e, ef, ely, u, py, [&](int s, int src, int64_t d, double(&v)[N]) {
+      tma_faces<false>(P, 1, c, e, ef, ely, phy, u, py, [&](int s, int src, int64_t d, double(&v)[N]) {
         const int sl = s ? 0 : N - 1;
         if (src == (int)kTmaSrcSlot) {
           const double2 a = *reinterpret_cast<const double2*>(yslot + le * 16 + t * 4);
@@ -436,6 +444,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
       }
       double u[N][N], pz[N][N];
       tma_plane_y(grp_sa, le, t, u);
+      [[maybe_unused]] const double2 phz = adv ? tma_phi(P, 2, c) : make_double2(0.0, 0.0);
       tma_apply<kSlotDZ, false, false>(T, c[2], mats, u, pz);
       if (adv) {
         const double elz = P.elem[2] ? P.elem[2][e] : 1.0;
@@ -445,7 +454,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
             for (int k = 0; k < N; ++k) pz[i][k] *= elz;
         }
-        tma_faces<false>(P, 2, c, e, ef, elz, u, pz, [&](int s, int src, int64_t d, double(&v)[N]) {
+        tma_faces<false>(P, 2, c, e, ef, elz, phz, u, pz, [&](int s, int src, int64_t d, double(&v)[N]) {
           const int sl = s ? 0 : N - 1;
           if (src == (int)kTmaSrcSlot) {
             const double2 a = *reinterpret_cast<const double2*>(zslot + swz(le, 4 * t));
