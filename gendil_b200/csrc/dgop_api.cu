@@ -290,12 +290,12 @@ int encode_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dim
   return DGOP_OK;
 }
 
-// The four maps of the bulk-tensor variants (kron3d_tma_kernel.cuh) for vectors x and y of
+// The five maps of the bulk-tensor variants (kron3d_tma_kernel.cuh) for vectors x and y of
 // `nelem` elements of 4 x 4 x 4 values.
 int encode_tma_maps(KronTmaParams<double>& T, const double* x, double* y, int64_t nelem) {
   const cuuint64_t rows = (cuuint64_t)nelem * 4;
   const cuuint64_t d2[2] = {16, rows}, s2[1] = {128};
-  const cuuint32_t b2[2] = {16, 32};
+  const cuuint32_t b2[2] = {16, 32}, b2e[2] = {16, 4};
   const cuuint64_t d3[3] = {16, 4, (cuuint64_t)nelem}, s3[2] = {128, 512};
   const cuuint32_t b3[3] = {16, 1, 8};
   const cuuint64_t d4[4] = {4, 4, 4, (cuuint64_t)nelem}, s4[3] = {32, 128, 512};
@@ -303,6 +303,7 @@ int encode_tma_maps(KronTmaParams<double>& T, const double* x, double* y, int64_
   int rc = encode_map(&T.win, x, 2, d2, s2, b2, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == DGOP_OK) rc = encode_map(&T.zsl, x, 3, d3, s3, b3, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == DGOP_OK) rc = encode_map(&T.ysl, x, 4, d4, s4, b4, CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (rc == DGOP_OK) rc = encode_map(&T.xel, x, 2, d2, s2, b2e, CU_TENSOR_MAP_SWIZZLE_NONE);
   if (rc == DGOP_OK) rc = encode_map(&T.out, y, 2, d2, s2, b2, CU_TENSOR_MAP_SWIZZLE_128B);
   return rc;
 }
@@ -312,7 +313,7 @@ int encode_tma_maps(KronTmaParams<double>& T, const double* x, double* y, int64_
 // variant without them.
 std::mutex g_map_cache_mutex;
 
-// The four maps for (x, y), from the operator's cache of recent pairs or freshly encoded.
+// The five maps for (x, y), from the operator's cache of recent pairs or freshly encoded.
 int tma_maps_cached(KronCfg<double>& K, KronTmaParams<double>& T, const double* x, double* y, int64_t nelem) {
   static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
   std::lock_guard<std::mutex> lock(g_map_cache_mutex);
@@ -321,7 +322,8 @@ int tma_maps_cached(KronCfg<double>& K, KronTmaParams<double>& T, const double* 
       std::memcpy(&T.win, m.maps[0], 128);
       std::memcpy(&T.zsl, m.maps[1], 128);
       std::memcpy(&T.ysl, m.maps[2], 128);
-      std::memcpy(&T.out, m.maps[3], 128);
+      std::memcpy(&T.xel, m.maps[3], 128);
+      std::memcpy(&T.out, m.maps[4], 128);
       return DGOP_OK;
     }
   }
@@ -332,7 +334,8 @@ int tma_maps_cached(KronCfg<double>& K, KronTmaParams<double>& T, const double* 
   std::memcpy(m.maps[0], &T.win, 128);
   std::memcpy(m.maps[1], &T.zsl, 128);
   std::memcpy(m.maps[2], &T.ysl, 128);
-  std::memcpy(m.maps[3], &T.out, 128);
+  std::memcpy(m.maps[3], &T.xel, 128);
+  std::memcpy(m.maps[4], &T.out, 128);
   m.x = x;
   m.y = y;
   return DGOP_OK;

@@ -58,11 +58,12 @@ struct KronCfg {
   uint32_t* d_eflags[2] = {};
   uint32_t* d_gwords[2] = {};
   int* d_err = nullptr;
-  // tensor maps of recent (x, y) pairs (opaque CUtensorMap bytes: group, z slices, y slices, out)
+  // tensor maps of recent (x, y) pairs (opaque CUtensorMap bytes: group, z slices, y slices,
+  // one element, out)
   struct MapEntry {
     const void* x = nullptr;
     const void* y = nullptr;
-    alignas(64) unsigned char maps[4][128];
+    alignas(64) unsigned char maps[5][128];
   };
   MapEntry map_cache[8];
   int map_next = 0;

@@ -279,6 +279,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
   using S = Kron3DShape<N, double>;
   static_assert(S::EPW == EPW, "eight elements per warp");
   const KronParams<double>& P = T.k;
+  // one stage with the exchange tile: the tile is idle from the end of a group until the x faces
+  // of the next have been read, so the x-slot element is staged there
+  constexpr bool XSLOT = STAGES == 1 && !SHFL;
   extern __shared__ unsigned char tma_smem_raw[];
   __shared__ uint64_t bars[kTmaWarps][2];
   [[maybe_unused]] __shared__ double wsum[kTmaWarps];
@@ -309,12 +312,19 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     const int64_t e0 = P.e_begin + g * EPW;
     unsigned char* sb = area + st * kTmaStageBytes;
     const uint32_t gw = T.gwords[e0 / EPW];
-    const uint32_t ys = gw & 3u, zs = (gw >> 2) & 3u;
+    const uint32_t ys = gw & 3u, zs = (gw >> 2) & 3u, xs = XSLOT ? (gw >> 4) & 3u : 0u;
     uint32_t c[3];
     kron_coords(P, (uint32_t)e0, c);
-    const uint32_t bytes = kTmaGroupBytes + (ys ? kTmaSlotBytes : 0) + (zs ? kTmaSlotBytes : 0) + T.nmat * kTmaMatBytes;
+    const uint32_t bytes = kTmaGroupBytes + (ys ? kTmaSlotBytes : 0) + (zs ? kTmaSlotBytes : 0) +
+                           T.nmat * kTmaMatBytes + (xs ? kTmaElemBytes : 0);
     mbar_arrive_expect_tx(&bars[warp][st], bytes);
     tma_load_2d(sb, &T.win, 0, (int)(4 * e0), &bars[warp][st]);
+    if (xs) {
+      const int s = (int)xs - 1;  // element 0's - side or element 7's + side neighbour
+      const int64_t ee = e0 + (s ? 7 : 0);
+      const int64_t en = ee + neighbour_offset(P, 0, s, c[0] + (s ? 7u : 0u));
+      tma_load_2d(tile, &T.xel, 0, (int)(4 * en), &bars[warp][st]);
+    }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int slot = tma_yz_slot(k);
@@ -392,6 +402,10 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
             const int r = 4 * (le + (s ? 1 : -1)) + t;
 #pragma unroll
             for (int q = 0; q < N; ++q) v[q] = grp[swz(r, 4 * q + sl)];
+          } else if (XSLOT && src == (int)kTmaSrcSlot) {
+            // the staged neighbour element, rows of 16 values (plane z = t), unswizzled
+#pragma unroll
+            for (int q = 0; q < N; ++q) v[q] = tile[16 * t + 4 * q + sl];
           } else {
             const double* un = P.x + (e + d) * 64 + 16 * t + sl;
 #pragma unroll
@@ -603,6 +617,13 @@ __global__ void kron_face_words(const KronParams<Real> P, uint32_t* eflags, uint
     const int n1 = __popc(__ballot_sync(0xffffffffu, act && (bits[a * 2 + 1] & kRecNb)));
     side[a] = (n0 == 0 && n1 == 0) ? 0u : (n0 >= n1 ? 1u : 2u);
   }
+  {
+    // x: only element 0's - side and element 7's + side neighbours lie outside the group (its 8
+    // elements are consecutive along x within one row); the x slot takes one of them
+    const bool x0 = __ballot_sync(0xffffffffu, act && lane == 0 && (bits[0] & kRecNb)) != 0u;
+    const bool x1 = __ballot_sync(0xffffffffu, act && lane == 7 && (bits[1] & kRecNb)) != 0u;
+    side[0] = x0 ? 1u : (x1 ? 2u : 0u);
+  }
   if (act) {
     uint32_t w = 0;
     const int le = lane;
@@ -615,7 +636,7 @@ __global__ void kron_face_words(const KronParams<Real> P, uint32_t* eflags, uint
           uint32_t src;
           if (a == 0) {
             const bool inside = s ? (le < 7 && (int64_t)c[0] + 1 < P.sizes[0]) : (le > 0 && c[0] > 0);
-            src = inside ? kTmaSrcGroup : kTmaSrcGlobal;
+            src = inside ? kTmaSrcGroup : (side[0] == (uint32_t)(s + 1) ? kTmaSrcSlot : kTmaSrcGlobal);
           } else {
             src = (side[a] == (uint32_t)(s + 1)) ? kTmaSrcSlot : kTmaSrcGlobal;
           }
@@ -625,7 +646,7 @@ __global__ void kron_face_words(const KronParams<Real> P, uint32_t* eflags, uint
       }
     eflags[e] = w;
   }
-  if (lane == 0) gwords[grp] = side[1] | (side[2] << 2);
+  if (lane == 0) gwords[grp] = side[1] | (side[2] << 2) | (side[0] << 4);
 }
 
 }  // namespace dgop
