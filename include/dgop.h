@@ -170,10 +170,12 @@ int dgop_apply_transpose(dgop_operator* op, const double* x, double* y, void* st
 int dgop_apply_f32(dgop_operator* op, const float* x, float* y, void* stream);
 
 /* Batches of independent operators (no reference counterpart; configuration 5 of the benchmark
- * plan): operators on the any-dimension Kronecker kernel are grouped by (dimension, order) and
- * each group is applied by ONE persistent launch over all its operators' elements; the others are
- * applied one launch each.  y[i] = A_i x[i] (device pointers), bit-identical to dgop_apply.  The
- * operators must outlive the batch.  dgop_batch_groups gives the number of grouped launches. */
+ * plan): operators on the any-dimension Kronecker kernel are grouped by (dimension, order, kernel
+ * variant) and each group is applied by ONE persistent launch over all its operators' elements;
+ * the others (other kernels, variants without a persistent form, and operators large enough to
+ * fill every CTA slot of the GPU twice on their own) are applied one launch each.
+ * y[i] = A_i x[i] (device pointers), bit-identical to dgop_apply.  The operators must outlive the
+ * batch.  dgop_batch_groups gives the number of grouped launches. */
 typedef struct dgop_batch dgop_batch;
 int dgop_batch_create(dgop_operator* const* ops, int count, dgop_batch** out);
 int dgop_batch_groups(const dgop_batch* batch);
