@@ -569,8 +569,10 @@ class GMRESIRSolver(_Solver):
 
 
 class Batch:
-    """Independent operators applied together: one persistent launch per (dimension, order) group
-    of any-dimension Kronecker operators, one launch each for the rest (dgop_batch_apply)."""
+    """Independent operators applied together: one persistent launch per (dimension, order,
+    variant) group of any-dimension Kronecker operators, one launch each for the rest (other
+    kernels, variants without a persistent form, operators that fill the GPU on their own)
+    (dgop_batch_apply)."""
 
     def __init__(self, ops):
         self.ops = list(ops)
