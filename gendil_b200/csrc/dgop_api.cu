@@ -536,6 +536,8 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
     if (arc == DGOP_OK) arc = allow_dynamic_smem(kv.func_sep, max_smem);
     for (const void* f : kv.func_dot)
       if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
+    for (const void* f : kv.func_masked)
+      if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
     if (arc != DGOP_OK) return arc;
     int per_sm = 0;
     DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? kv.func_sep : kv.func, threads, L.smem));

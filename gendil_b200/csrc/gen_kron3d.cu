@@ -41,15 +41,42 @@ void fill_variant(KronVariant<Real>& v) {
   v.threads = kKronThreads;
 }
 
+// The operator's element-dependent slots as a mask (bit k: slot k varies).
+uint32_t vary_mask(const KronParams<double>& k) {
+  uint32_t m = 0;
+  for (int i = 0; i < kNumSlots; ++i)
+    if (k.vary[i]) m |= 1u << i;
+  return m;
+}
+
+// The one-stage tile variant (the fastest on the 3D p=3 workloads) is also compiled for the
+// masks kVaryNone and kVarySheared; an operator whose mask is exactly one of them runs that
+// kernel, every other operator the run-time-mask kernel (same arithmetic, same results).
+template <bool SEP, int STAGES, bool SHFL, bool DOT>
+void launch_tma_masked(const KronTmaParams<double>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  if constexpr (STAGES == 1 && !SHFL) {
+    const uint32_t m = vary_mask(p.k);
+    if (m == kVaryNone) {
+      kron3d_tma_kernel<SEP, STAGES, SHFL, DOT, kVaryNone><<<grid, block, smem, s>>>(p);
+      return;
+    }
+    if (m == kVarySheared) {
+      kron3d_tma_kernel<SEP, STAGES, SHFL, DOT, kVarySheared><<<grid, block, smem, s>>>(p);
+      return;
+    }
+  }
+  kron3d_tma_kernel<SEP, STAGES, SHFL, DOT><<<grid, block, smem, s>>>(p);
+}
+
 template <int STAGES, bool SHFL>
 void launch_tma(const KronTmaParams<double>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   const bool sep = p.k.has_adv && p.k.has_mass && !p.k.mass_merged;
   if (p.k.dot_partials) {
-    if (sep) kron3d_tma_kernel<true, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
-    else kron3d_tma_kernel<false, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+    if (sep) launch_tma_masked<true, STAGES, SHFL, true>(p, grid, block, smem, s);
+    else launch_tma_masked<false, STAGES, SHFL, true>(p, grid, block, smem, s);
   } else {
-    if (sep) kron3d_tma_kernel<true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
-    else kron3d_tma_kernel<false, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+    if (sep) launch_tma_masked<true, STAGES, SHFL, false>(p, grid, block, smem, s);
+    else launch_tma_masked<false, STAGES, SHFL, false>(p, grid, block, smem, s);
   }
 }
 
@@ -60,6 +87,18 @@ void fill_tma(KronVariant<double>& v) {
   v.func_sep = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, STAGES, SHFL>);
   v.func_dot[0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, STAGES, SHFL, true>);
   v.func_dot[1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, STAGES, SHFL, true>);
+  if constexpr (STAGES == 1 && !SHFL) {
+    int k = 0;
+    for (const void* f : {reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVaryNone>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVaryNone>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVaryNone>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVaryNone>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVarySheared>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVarySheared>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVarySheared>),
+                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVarySheared>)})
+      v.func_masked[k++] = f;
+  }
   v.warp_smem = kTmaWarps * tma_warp_bytes(STAGES, SHFL) + 1024;  // bytes per CTA, with the alignment slack
   v.threads = kTmaWarps * 32;
 }

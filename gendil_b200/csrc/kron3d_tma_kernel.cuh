@@ -177,15 +177,27 @@ __device__ __forceinline__ void pass_acc(const Mat& A, const double (&X)[4][4], 
     }
 }
 
+// Which slots have element-dependent matrices: a compile-time mask (bit k: slot k varies) or
+// kVaryRuntime (read P.vary).  A kernel compiled for one mask carries one code path per pass
+// instead of two, half the instructions to fetch (the run-time form measured 7 % slower on the
+// 64^3 p=3 advection apply); the launcher takes such a kernel only for operators whose mask
+// matches.  kVarySheared: beta_x depends on y and beta_y on z (beta_z constant).
+constexpr uint32_t kVaryRuntime = 0xFFFFFFFFu;
+constexpr uint32_t kVaryNone = 0u;
+constexpr uint32_t kVarySheared = (1u << kSlotTXY) | (1u << kSlotTYZ);
+
 // Slot SLOT's matrix applied along the first (FIRST) or second plane index, Y = A X or, with
 // ACC, Y += A X.  Constant matrices come from kernel-parameter space; element-dependent ones from
 // the stage's matrix area when the group staged them (slots along y or z), otherwise from global
 // memory (slots along x, whose coordinate differs between the group's elements).
-template <int SLOT, bool FIRST, bool ACC>
+template <uint32_t VM, int SLOT, bool FIRST, bool ACC>
 __device__ __forceinline__ void tma_apply(const KronTmaParams<double>& T, uint32_t coord, const double* mats,
                                           const double (&X)[4][4], double (&Y)[4][4]) {
   const KronParams<double>& P = T.k;
-  if (P.vary[SLOT]) {
+  bool vary;
+  if constexpr (VM == kVaryRuntime) vary = P.vary[SLOT] != 0;
+  else vary = ((VM >> SLOT) & 1u) != 0;
+  if (vary) {
     RegMat<4, double> A;
     const int mi = T.mat_index[SLOT];
     if (mi >= 0) {
@@ -272,7 +284,7 @@ __device__ __forceinline__ void tma_faces(const KronParams<double>& P, int a, co
   }
 }
 
-template <bool SEP, int STAGES, bool SHFL, bool DOT = false>
+template <bool SEP, int STAGES, bool SHFL, bool DOT = false, uint32_t VM = kVaryRuntime>
 __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     kron3d_tma_kernel(const __grid_constant__ KronTmaParams<double> T) {
   constexpr int N = 4, EPW = 8;
@@ -388,7 +400,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
       {
         double px[N][N];
         const double2 phx = tma_phi(P, 0, c);
-        tma_apply<kSlotDX, true, false>(T, c[0], mats, u, px);
+        tma_apply<VM, kSlotDX, true, false>(T, c[0], mats, u, px);
         const double elx = P.elem[0] ? P.elem[0][e] : 1.0;
         if (P.elem[0]) {
 #pragma unroll
@@ -412,10 +424,10 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
             for (int q = 0; q < N; ++q) v[q] = un[4 * q];
           }
         });
-        tma_apply<kSlotTXY, false, false>(T, c[1], mats, px, qx);
+        tma_apply<VM, kSlotTXY, false, false>(T, c[1], mats, px, qx);
       }
       const double2 phy = tma_phi(P, 1, c);
-      tma_apply<kSlotDY, false, false>(T, c[1], mats, u, py);
+      tma_apply<VM, kSlotDY, false, false>(T, c[1], mats, u, py);
       const double ely = P.elem[1] ? P.elem[1][e] : 1.0;
       if (P.elem[1]) {
 #pragma unroll
@@ -452,14 +464,14 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     [[maybe_unused]] double qm[N][N];
     {
       if (adv) {
-        tma_apply<kSlotTXZ, false, false>(T, c[2], mats, qx, out);
-        tma_apply<kSlotTYZ, false, false>(T, c[2], mats, py, qx);  // qx reused as scratch
-        tma_apply<kSlotTYX, true, true>(T, c[0], mats, qx, out);   // out += Tyx (Tyz py)
+        tma_apply<VM, kSlotTXZ, false, false>(T, c[2], mats, qx, out);
+        tma_apply<VM, kSlotTYZ, false, false>(T, c[2], mats, py, qx);  // qx reused as scratch
+        tma_apply<VM, kSlotTYX, true, true>(T, c[0], mats, qx, out);   // out += Tyx (Tyz py)
       }
       double u[N][N], pz[N][N];
       tma_plane_y(grp_sa, le, t, u);
       [[maybe_unused]] const double2 phz = adv ? tma_phi(P, 2, c) : make_double2(0.0, 0.0);
-      tma_apply<kSlotDZ, false, false>(T, c[2], mats, u, pz);
+      tma_apply<VM, kSlotDZ, false, false>(T, c[2], mats, u, pz);
       if (adv) {
         const double elz = P.elem[2] ? P.elem[2][e] : 1.0;
         if (P.elem[2]) {
@@ -490,9 +502,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
           for (int k = 0; k < N; ++k) pz[i][k] *= em;
       }
-      tma_apply<kSlotTZX, true, false>(T, c[0], mats, pz, qz);
+      tma_apply<VM, kSlotTZX, true, false>(T, c[0], mats, pz, qz);
       if constexpr (SEP) {
-        tma_apply<kSlotMD, false, false>(T, c[2], mats, u, pz);
+        tma_apply<VM, kSlotMD, false, false>(T, c[2], mats, u, pz);
         if (P.elem_mass) {
           const double em = P.elem_mass[e];
 #pragma unroll
@@ -500,7 +512,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
 #pragma unroll
             for (int k = 0; k < N; ++k) pz[i][k] *= em;
         }
-        tma_apply<kSlotMX, true, false>(T, c[0], mats, pz, qm);
+        tma_apply<VM, kSlotMX, true, false>(T, c[0], mats, pz, qm);
       }
     }
     // layout Y -> Z for the terms still missing their y pass, and for `out`
@@ -516,9 +528,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 16 / kTmaWarps)
     // ------------------------------------------------------------ layout Z, output
     // res = out + Tzy qz (+ My qm): the last passes accumulate onto the x and y terms
     double (&res)[N][N] = out;
-    if (adv) tma_apply<kSlotTZY, false, true>(T, c[1], mats, qz, res);
-    else tma_apply<kSlotTZY, false, false>(T, c[1], mats, qz, res);
-    if constexpr (SEP) tma_apply<kSlotMY, false, true>(T, c[1], mats, qm, res);
+    if (adv) tma_apply<VM, kSlotTZY, false, true>(T, c[1], mats, qz, res);
+    else tma_apply<VM, kSlotTZY, false, false>(T, c[1], mats, qz, res);
+    if constexpr (SEP) tma_apply<VM, kSlotMY, false, true>(T, c[1], mats, qm, res);
     const double alpha = P.alpha, by = P.beta_y;
     if (alpha != 1.0) {
 #pragma unroll
