@@ -362,10 +362,10 @@ int launch_kron(const dgop_operator* op, KronCfg<Real>& K, int v, const KronPara
       T.nmat = 0;
       for (int k = 0; k < 8; ++k)
         if (p.vary[tma_yz_slot(k)]) T.mat_index[tma_yz_slot(k)] = T.nmat++;
-      kv.launch_tma(T, L.grid, L.block, L.smem, s);
+      kv.launch_tma(T, p.dot_partials ? L.grid_dot : L.grid, L.block, L.smem, s);
     }
   } else {
-    kv.launch(p, L.grid, L.block, L.smem, s);
+    kv.launch(p, p.dot_partials ? L.grid_dot : L.grid, L.block, L.smem, s);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "operator kernel launch");
@@ -536,14 +536,25 @@ int setup_kron(dgop_operator* op, KronCfg<Real>& K, const KronPlanHost& plan, co
     if (arc == DGOP_OK) arc = allow_dynamic_smem(kv.func_sep, max_smem);
     for (const void* f : kv.func_dot)
       if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
-    for (const void* f : kv.func_masked)
-      if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
+    for (const auto& by_dot : kv.func_masked)
+      for (const auto& by_sep : by_dot)
+        for (const void* f : by_sep)
+          if (arc == DGOP_OK && f) arc = allow_dynamic_smem(f, max_smem);
     if (arc != DGOP_OK) return arc;
-    int per_sm = 0;
-    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sep ? kv.func_sep : kv.func, threads, L.smem));
+    // resident CTAs per SM of the kernels this operator launches (the slot-mask form when its
+    // mask has one), plain and with the inner-product epilogue: each gets a grid of that many
+    const int mi = kron_mask_index(p);
+    const void* kern[2] = {sep ? kv.func_sep : kv.func, kv.func_dot[sep ? 1 : 0]};
+    for (int dot = 0; dot < 2; ++dot)
+      if (mi >= 0 && kv.func_masked[mi][dot][sep ? 1 : 0]) kern[dot] = kv.func_masked[mi][dot][sep ? 1 : 0];
+    int per_sm = 0, per_sm_dot = 0;
+    DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[0], threads, L.smem));
     if (per_sm < 1) continue;
-    const int64_t ctas = std::min<int64_t>((groups + warps - 1) / warps, (int64_t)device_sm_count(op->device) * per_sm);
-    L.grid = dim3((unsigned)std::max<int64_t>(ctas, 1));
+    if (kern[1]) DGOP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_dot, kern[1], threads, L.smem));
+    if (per_sm_dot < 1) per_sm_dot = per_sm;
+    const int64_t need = (groups + warps - 1) / warps, sms = device_sm_count(op->device);
+    L.grid = dim3((unsigned)std::max<int64_t>(std::min<int64_t>(need, sms * per_sm), 1));
+    L.grid_dot = dim3((unsigned)std::max<int64_t>(std::min<int64_t>(need, sms * per_sm_dot), 1));
     L.ok = true;
     ++usable;
   }
@@ -1357,7 +1368,7 @@ static int launch_impl(dgop_operator* op, LaunchCfg<Real>& L, KronCfg<Real>& K, 
       const bool whole = e_begin % 8 == 0 && e_end % 8 == 0;
       const int v = (K.entry->v[K.variant].launch_tma && !whole) ? K.fallback : K.variant;
       if (dot && dot->z && dot->partials && reinterpret_cast<uintptr_t>(dot->z) % 16 == 0 &&
-          (int64_t)K.launch[v].grid.x <= dot->count) {
+          (int64_t)K.launch[v].grid_dot.x <= dot->count) {
         p.dot_z = dot->z;
         p.dot_partials = dot->partials;
         p.dot_count = dot->count;

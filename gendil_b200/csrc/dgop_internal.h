@@ -44,6 +44,7 @@ struct KronCfg {
   struct Launch {
     bool ok = false;
     dim3 grid, block;
+    dim3 grid_dot;  // launches with the inner-product epilogue (that kernel's residency)
     size_t smem = 0;
     float ms = 0.0f;  // autotuner timing (0: not timed)
   } launch[kKronVariants];

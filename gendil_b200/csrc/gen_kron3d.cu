@@ -14,18 +14,48 @@ const char* const kKronNDVariantNames[kKronNDVariants] = {"nd-passes", "nd-group
                                                           "nd-mass"};
 
 namespace {
+// The one-stage tile variant at N = 4 (p = 3) is also compiled for the masks kVaryNone and
+// kVarySheared; an operator whose mask is exactly one of them runs that kernel, every other
+// operator the run-time-mask kernel (same arithmetic, same results).
+template <int N, typename Real, bool SEP, int STAGES, bool SHFL, bool DOT>
+void launch_kron3d_masked(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
+  if constexpr (N == 4 && STAGES == 1 && !SHFL) {
+    const int mi = kron_mask_index(p);
+    if constexpr (std::is_same<Real, double>::value && !SEP) {
+      if (mi == 0) {
+        kron3d_kernel_capped<N, STAGES, SHFL, DOT, kVaryNone><<<grid, block, smem, s>>>(p);
+        return;
+      }
+      if (mi == 1) {
+        kron3d_kernel_capped<N, STAGES, SHFL, DOT, kVarySheared><<<grid, block, smem, s>>>(p);
+        return;
+      }
+    } else {
+      if (mi == 0) {
+        kron3d_kernel<N, Real, SEP, STAGES, SHFL, DOT, kVaryNone><<<grid, block, smem, s>>>(p);
+        return;
+      }
+      if (mi == 1) {
+        kron3d_kernel<N, Real, SEP, STAGES, SHFL, DOT, kVarySheared><<<grid, block, smem, s>>>(p);
+        return;
+      }
+    }
+  }
+  kron3d_kernel<N, Real, SEP, STAGES, SHFL, DOT><<<grid, block, smem, s>>>(p);
+}
+
 template <int N, typename Real, int STAGES, bool SHFL>
 void launch_kron3d(const KronParams<Real>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   const bool sep = p.has_adv && p.has_mass && !p.mass_merged;
   if constexpr (std::is_same<Real, double>::value) {
     if (p.dot_partials) {
-      if (sep) kron3d_kernel<N, Real, true, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
-      else kron3d_kernel<N, Real, false, STAGES, SHFL, true><<<grid, block, smem, s>>>(p);
+      if (sep) launch_kron3d_masked<N, Real, true, STAGES, SHFL, true>(p, grid, block, smem, s);
+      else launch_kron3d_masked<N, Real, false, STAGES, SHFL, true>(p, grid, block, smem, s);
       return;
     }
   }
-  if (sep) kron3d_kernel<N, Real, true, STAGES, SHFL><<<grid, block, smem, s>>>(p);
-  else kron3d_kernel<N, Real, false, STAGES, SHFL><<<grid, block, smem, s>>>(p);
+  if (sep) launch_kron3d_masked<N, Real, true, STAGES, SHFL, false>(p, grid, block, smem, s);
+  else launch_kron3d_masked<N, Real, false, STAGES, SHFL, false>(p, grid, block, smem, s);
 }
 
 template <int N, typename Real, int STAGES, bool SHFL>
@@ -37,30 +67,39 @@ void fill_variant(KronVariant<Real>& v) {
     v.func_dot[0] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, STAGES, SHFL, true>);
     v.func_dot[1] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, STAGES, SHFL, true>);
   }
+  if constexpr (N == 4 && STAGES == 1 && !SHFL) {
+    v.func_masked[0][0][1] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, 1, false, false, kVaryNone>);
+    v.func_masked[1][0][1] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, 1, false, false, kVarySheared>);
+    if constexpr (std::is_same<Real, double>::value) {
+      v.func_masked[0][0][0] = reinterpret_cast<const void*>(&kron3d_kernel_capped<N, 1, false, false, kVaryNone>);
+      v.func_masked[1][0][0] = reinterpret_cast<const void*>(&kron3d_kernel_capped<N, 1, false, false, kVarySheared>);
+      v.func_masked[0][1][0] = reinterpret_cast<const void*>(&kron3d_kernel_capped<N, 1, false, true, kVaryNone>);
+      v.func_masked[1][1][0] = reinterpret_cast<const void*>(&kron3d_kernel_capped<N, 1, false, true, kVarySheared>);
+      v.func_masked[0][1][1] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, 1, false, true, kVaryNone>);
+      v.func_masked[1][1][1] =
+          reinterpret_cast<const void*>(&kron3d_kernel<N, Real, true, 1, false, true, kVarySheared>);
+    } else {
+      v.func_masked[0][0][0] = reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, 1, false, false, kVaryNone>);
+      v.func_masked[1][0][0] =
+          reinterpret_cast<const void*>(&kron3d_kernel<N, Real, false, 1, false, false, kVarySheared>);
+    }
+  }
   v.warp_smem = Kron3DShape<N, Real>::warp_smem(STAGES, SHFL);
   v.threads = kKronThreads;
 }
 
-// The operator's element-dependent slots as a mask (bit k: slot k varies).
-uint32_t vary_mask(const KronParams<double>& k) {
-  uint32_t m = 0;
-  for (int i = 0; i < kNumSlots; ++i)
-    if (k.vary[i]) m |= 1u << i;
-  return m;
-}
-
 // The one-stage tile variant (the fastest on the 3D p=3 workloads) is also compiled for the
-// masks kVaryNone and kVarySheared; an operator whose mask is exactly one of them runs that
-// kernel, every other operator the run-time-mask kernel (same arithmetic, same results).
+// masks kVaryNone and kVarySheared (kron.h); an operator whose mask is exactly one of them runs
+// that kernel, every other operator the run-time-mask kernel (same arithmetic, same results).
 template <bool SEP, int STAGES, bool SHFL, bool DOT>
 void launch_tma_masked(const KronTmaParams<double>& p, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
   if constexpr (STAGES == 1 && !SHFL) {
-    const uint32_t m = vary_mask(p.k);
-    if (m == kVaryNone) {
+    const int mi = kron_mask_index(p.k);
+    if (mi == 0) {
       kron3d_tma_kernel<SEP, STAGES, SHFL, DOT, kVaryNone><<<grid, block, smem, s>>>(p);
       return;
     }
-    if (m == kVarySheared) {
+    if (mi == 1) {
       kron3d_tma_kernel<SEP, STAGES, SHFL, DOT, kVarySheared><<<grid, block, smem, s>>>(p);
       return;
     }
@@ -88,16 +127,14 @@ void fill_tma(KronVariant<double>& v) {
   v.func_dot[0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, STAGES, SHFL, true>);
   v.func_dot[1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, STAGES, SHFL, true>);
   if constexpr (STAGES == 1 && !SHFL) {
-    int k = 0;
-    for (const void* f : {reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVaryNone>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVaryNone>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVaryNone>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVaryNone>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVarySheared>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVarySheared>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVarySheared>),
-                          reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVarySheared>)})
-      v.func_masked[k++] = f;
+    v.func_masked[0][0][0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVaryNone>);
+    v.func_masked[0][0][1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVaryNone>);
+    v.func_masked[0][1][0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVaryNone>);
+    v.func_masked[0][1][1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVaryNone>);
+    v.func_masked[1][0][0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, false, kVarySheared>);
+    v.func_masked[1][0][1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, false, kVarySheared>);
+    v.func_masked[1][1][0] = reinterpret_cast<const void*>(&kron3d_tma_kernel<false, 1, false, true, kVarySheared>);
+    v.func_masked[1][1][1] = reinterpret_cast<const void*>(&kron3d_tma_kernel<true, 1, false, true, kVarySheared>);
   }
   v.warp_smem = kTmaWarps * tma_warp_bytes(STAGES, SHFL) + 1024;  // bytes per CTA, with the alignment slack
   v.threads = kTmaWarps * 32;

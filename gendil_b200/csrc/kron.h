@@ -84,6 +84,29 @@ struct KronParams {
   int dot_count;
 };
 
+// Which slots have element-dependent matrices: a compile-time mask of the 3D kernels (bit k:
+// slot k varies) or kVaryRuntime (read P.vary).  A kernel compiled for one mask carries one code
+// path per pass instead of two, half the instructions to fetch (the run-time form of the
+// bulk-tensor kernel measured 7 % slower on the 64^3 p=3 advection apply); the launchers take
+// such a kernel only for operators whose mask matches.  kVarySheared: beta_x depends on y and
+// beta_y on z (beta_z constant).  kron_mask_index: 0 for kVaryNone, 1 for kVarySheared, -1 else.
+constexpr uint32_t kVaryRuntime = 0xFFFFFFFFu;
+constexpr uint32_t kVaryNone = 0u;
+constexpr uint32_t kVarySheared = (1u << kSlotTXY) | (1u << kSlotTYZ);
+
+template <typename Real>
+inline uint32_t kron_vary_mask(const KronParams<Real>& k) {
+  uint32_t m = 0;
+  for (int i = 0; i < kNumSlots; ++i)
+    if (k.vary[i]) m |= 1u << i;
+  return m;
+}
+template <typename Real>
+inline int kron_mask_index(const KronParams<Real>& k) {
+  const uint32_t m = kron_vary_mask(k);
+  return m == kVaryNone ? 0 : (m == kVarySheared ? 1 : -1);
+}
+
 // Launch parameters of the any-dimension kernel (kronnd_kernel.cuh).
 template <typename Real>
 struct KronNDParams {

@@ -253,11 +253,15 @@ struct ParamMat {
 };
 
 // Apply slot SLOT's matrix (for element coordinate `coord` along its axis) along the first or
-// second plane index: constant matrices come from kernel-parameter space.
-template <int N, typename Real, int SLOT, bool FIRST>
+// second plane index: constant matrices come from kernel-parameter space.  VM: the slot mask the
+// kernel is compiled for (kron.h).
+template <int N, typename Real, int SLOT, bool FIRST, uint32_t VM = kVaryRuntime>
 __device__ __forceinline__ void kron_apply(const KronParams<Real>& P, uint32_t coord, const Real (&X)[N][N],
                                            Real (&Y)[N][N]) {
-  if (P.vary[SLOT]) {
+  bool vary;
+  if constexpr (VM == kVaryRuntime) vary = P.vary[SLOT] != 0;
+  else vary = ((VM >> SLOT) & 1u) != 0;
+  if (vary) {
     RegMat<N, Real> A;
     const Real* p = P.mats + P.vm[SLOT].off + (int64_t)coord * P.vm[SLOT].stride;
     // N x N blocks at offsets that are multiples of the vector width (checked at setup)
@@ -608,8 +612,9 @@ constexpr int kron_max_warps = 4;  // warps per CTA of kron3d_kernel (128 thread
 //   less shared memory per warp and so more warps per SM
 //   SHFL:    layout exchanges by shuffle butterflies (even N) instead of the shared tile
 //   DOT:     the inner-product epilogue (P.dot_partials; FP64 solvers) is compiled in
-template <int N, typename Real, bool SEP, int STAGES, bool SHFL, bool DOT = false>
-__global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ KronParams<Real> P) {
+//   VM:      the slot mask the kernel is compiled for (kVaryRuntime: read P.vary)
+template <int N, typename Real, bool SEP, int STAGES, bool SHFL, bool DOT, uint32_t VM>
+__device__ __forceinline__ void kron3d_body(const KronParams<Real>& P) {
   using S = Kron3DShape<N, Real>;
   constexpr int NN = S::NN, NNN = S::NNN, EPW = S::EPW;
   constexpr bool BFLY = SHFL && S::BUTTERFLY;
@@ -663,7 +668,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
       load_plane_z<N>(ub, t, active, u);
       {
         Real px[N][N];
-        kron_apply<N, Real, kSlotDX, true>(P, c[0], u, px);
+        kron_apply<N, Real, kSlotDX, true, VM>(P, c[0], u, px);
         if (P.elem[0]) {
           const Real elx = active ? P.elem[0][e] : Real(1);
 #pragma unroll
@@ -683,9 +688,9 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
                                           : P.x[en * NNN + sl + N * r + NN * t];
             }
           });
-        kron_apply<N, Real, kSlotTXY, false>(P, c[1], px, qx);
+        kron_apply<N, Real, kSlotTXY, false, VM>(P, c[1], px, qx);
       }
-      kron_apply<N, Real, kSlotDY, false>(P, c[1], u, py);
+      kron_apply<N, Real, kSlotDY, false, VM>(P, c[1], u, py);
       if (P.elem[1]) {
         const Real ely = active ? P.elem[1][e] : Real(1);
 #pragma unroll
@@ -717,9 +722,9 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
     {
       // x and y terms first, so their inputs die before u is loaded
       if (adv) {
-        kron_apply<N, Real, kSlotTXZ, false>(P, c[2], qx, out);
-        kron_apply<N, Real, kSlotTYZ, false>(P, c[2], py, qx);  // qx reused as scratch
-        kron_apply<N, Real, kSlotTYX, true>(P, c[0], qx, py);
+        kron_apply<N, Real, kSlotTXZ, false, VM>(P, c[2], qx, out);
+        kron_apply<N, Real, kSlotTYZ, false, VM>(P, c[2], py, qx);  // qx reused as scratch
+        kron_apply<N, Real, kSlotTYX, true, VM>(P, c[0], qx, py);
 #pragma unroll
         for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -732,7 +737,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
       }
       Real u[N][N], pz[N][N];
       load_plane_y<N>(ub, t, active, u);
-      kron_apply<N, Real, kSlotDZ, false>(P, c[2], u, pz);
+      kron_apply<N, Real, kSlotDZ, false, VM>(P, c[2], u, pz);
       if (adv) {
         if (P.elem[2]) {
           const Real elz = active ? P.elem[2][e] : Real(1);
@@ -757,9 +762,9 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
 #pragma unroll
           for (int k = 0; k < N; ++k) pz[i][k] *= em;
       }
-      kron_apply<N, Real, kSlotTZX, true>(P, c[0], pz, qz);
+      kron_apply<N, Real, kSlotTZX, true, VM>(P, c[0], pz, qz);
       if constexpr (SEP) {
-        kron_apply<N, Real, kSlotMD, false>(P, c[2], u, pz);
+        kron_apply<N, Real, kSlotMD, false, VM>(P, c[2], u, pz);
         if (P.elem_mass) {
           const Real em = active ? P.elem_mass[e] : Real(1);
 #pragma unroll
@@ -767,7 +772,7 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
 #pragma unroll
             for (int k = 0; k < N; ++k) pz[i][k] *= em;
         }
-        kron_apply<N, Real, kSlotMX, true>(P, c[0], pz, qm);
+        kron_apply<N, Real, kSlotMX, true, VM>(P, c[0], pz, qm);
       }
     }
     __syncwarp();  // every lane is done reading the staged input of this group
@@ -795,9 +800,9 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
     }
 
     // ------------------------------------------------------------ layout Z, output
-    kron_apply<N, Real, kSlotTZY, false>(P, c[1], qz, py);
+    kron_apply<N, Real, kSlotTZY, false, VM>(P, c[1], qz, py);
     if constexpr (SEP) {
-      kron_apply<N, Real, kSlotMY, false>(P, c[1], qm, qx);
+      kron_apply<N, Real, kSlotMY, false, VM>(P, c[1], qm, qx);
 #pragma unroll
       for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -869,6 +874,18 @@ __global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ Kro
       for (int i = blockIdx.x + gridDim.x; i < P.dot_count; i += gridDim.x) P.dot_partials[i] = 0.0;
     }
   }
+}
+
+template <int N, typename Real, bool SEP, int STAGES, bool SHFL, bool DOT = false, uint32_t VM = kVaryRuntime>
+__global__ void __launch_bounds__(128) kron3d_kernel(const __grid_constant__ KronParams<Real> P) {
+  kron3d_body<N, Real, SEP, STAGES, SHFL, DOT, VM>(P);
+}
+
+// The FP64 slot-mask forms without a separate mass term, held to the run-time form's 4 CTAs per
+// SM (at most 128 registers; left to itself the compiler takes 138 for kVarySheared).
+template <int N, int STAGES, bool SHFL, bool DOT, uint32_t VM>
+__global__ void __launch_bounds__(128, 4) kron3d_kernel_capped(const __grid_constant__ KronParams<double> P) {
+  kron3d_body<N, double, false, STAGES, SHFL, DOT, VM>(P);
 }
 
 }  // namespace dgop

@@ -177,15 +177,6 @@ __device__ __forceinline__ void pass_acc(const Mat& A, const double (&X)[4][4], 
     }
 }
 
-// Which slots have element-dependent matrices: a compile-time mask (bit k: slot k varies) or
-// kVaryRuntime (read P.vary).  A kernel compiled for one mask carries one code path per pass
-// instead of two, half the instructions to fetch (the run-time form measured 7 % slower on the
-// 64^3 p=3 advection apply); the launcher takes such a kernel only for operators whose mask
-// matches.  kVarySheared: beta_x depends on y and beta_y on z (beta_z constant).
-constexpr uint32_t kVaryRuntime = 0xFFFFFFFFu;
-constexpr uint32_t kVaryNone = 0u;
-constexpr uint32_t kVarySheared = (1u << kSlotTXY) | (1u << kSlotTYZ);
-
 // Slot SLOT's matrix applied along the first (FIRST) or second plane index, Y = A X or, with
 // ACC, Y += A X.  Constant matrices come from kernel-parameter space; element-dependent ones from
 // the stage's matrix area when the group staged them (slots along y or z), otherwise from global

@@ -31,7 +31,9 @@ struct KronVariant {
   const void* func = nullptr;      // kernel symbol (mass merged or absent)
   const void* func_sep = nullptr;  // kernel symbol with a separate mass term
   const void* func_dot[2] = {};    // with the inner-product epilogue (mass merged / separate; FP64)
-  const void* func_masked[8] = {}; // compile-time slot-mask forms of the above (bulk-tensor, one stage)
+  // compile-time slot-mask forms of the above (one-stage tile variants): [mask index, kron.h]
+  // [with the inner-product epilogue][separate mass term]
+  const void* func_masked[2][2][2] = {};
   int warp_smem = 0;               // Real values of shared memory per warp (bytes per CTA for bulk-tensor variants)
   int threads = 0;                 // threads per CTA
 };
